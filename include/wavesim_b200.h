@@ -1,0 +1,182 @@
+/*
+ * wavesim_b200 - C ABI of the B200 modified Born series (MBS) iteration loop.
+ *
+ * This library replaces the iteration loop of IvoVellekoop/wavesim
+ * (WaveSimBase.run_algorithm, WaveSimBase.m:157-197, and its native
+ * counterpart RunWaveSimAlgorithmMex, called at WaveSimBase.m:145-146) with
+ * hand-written sm_100a CUDA kernels.  Everything the MATLAB side computes
+ * before the loop (gamma, wiggle descriptors, epsilon, k02e, roi, the cropped
+ * source) is passed in unchanged; everything it does after the loop
+ * (E ./ gamma and the ROI crop, WaveSimBase.m:150-153) is done by the caller,
+ * or by the library on request (WS_OUTPUT_FIELD).
+ *
+ * Memory layout: every array is MATLAB's column-major layout.  A field of
+ * size N = [Ny, Nx, Nz, Nc] has element (y, x, z, c) (0-based) at
+ * y + Ny*(x + Nx*(z + Nz*c)); complex values are interleaved (re, im) single
+ * precision, as in a complex single gpuArray.
+ *
+ * Errors: functions return a ws_status; ws_last_error() gives a message for
+ * the calling thread.  No C++ exception crosses this interface.
+ * Threading: a ws_solver owns one CUDA stream and is not thread safe; distinct
+ * solvers may be used from distinct threads.
+ */
+#ifndef WAVESIM_B200_H
+#define WAVESIM_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum ws_status {
+  WS_OK = 0,
+  WS_ERR_INVALID_ARGUMENT = 1, /* bad size, pointer, roi, option */
+  WS_ERR_UNSUPPORTED = 2,      /* grid size the FFT kernels do not handle */
+  WS_ERR_CUDA = 3,             /* a CUDA runtime call failed */
+  WS_ERR_OUT_OF_MEMORY = 4,
+  WS_ERR_NO_SOURCE = 5,        /* no source energy inside the grid (Simulation.m:157-161) */
+  WS_ERR_DIVERGED = 6,         /* residual energy became NaN or Inf */
+  WS_ERR_NO_DEVICE = 7
+} ws_status;
+
+/* Where a pointer argument lives. */
+enum { WS_HOST = 0, WS_DEVICE = 1 };
+
+/* Stop rules.
+ * WS_STOP_REFERENCE: Simulation.next (Simulation.m:193-217) exactly: the
+ *   energy is refreshed at iterations 1, 2, 2+k*interval, the ratio to the
+ *   first energy is tested only when it % Nwiggles == 0.
+ * WS_STOP_FRESH: the same test at the same iterations, but with the energy of
+ *   the current iteration (computed by every fused iteration at no cost). */
+enum { WS_STOP_REFERENCE = 0, WS_STOP_FRESH = 1 };
+
+/* What ws_solver_solve writes to E_out.
+ * WS_OUTPUT_EPRIME: the full-grid accumulated field E' (what
+ *   RunWaveSimAlgorithmMex returns; the caller divides by gamma and crops).
+ * WS_OUTPUT_FIELD: E = E' ./ gamma cropped to the roi (Simulation.m:254-261),
+ *   size (y1-y0+1)*(x1-x0+1)*(z1-z0+1)*(c1-c0+1). */
+enum { WS_OUTPUT_EPRIME = 0, WS_OUTPUT_FIELD = 1 };
+
+typedef struct ws_complex {
+  float re;
+  float im;
+} ws_complex;
+
+/* One wiggle descriptor (WaveSimBase.m:300-316): shifted Fourier coordinates
+ * pre-divided by sqrt(epsilon) and the real-space phase ramps.
+ * Lengths: pxe, gx: Nx; pye, gy: Ny; pze, gz: Nz. */
+typedef struct ws_wiggle {
+  const float* pxe;
+  const float* pye;
+  const float* pze;
+  const ws_complex* gx;
+  const ws_complex* gy;
+  const ws_complex* gz;
+} ws_wiggle;
+
+/* One block of a Source object (Source.m:18-21) after Simulation.exec has
+ * shifted and cropped it to the grid (Simulation.m:154-156): 1-based corner
+ * position (y, x, z, polarization) in grid coordinates and the block size;
+ * values are column-major. */
+typedef struct ws_source_block {
+  int64_t position[4];
+  int64_t size[4];
+  const ws_complex* values;
+} ws_source_block;
+
+/* Progress callback, the counterpart of SimulationCallback.m:1
+ * (callbackType, diff_energy, ..., energy_threshold).  Called on the host
+ * every callback_interval iterations and once at the end. */
+typedef void (*ws_callback_fn)(const char* callback_type, const double* diff_energy, int64_t n_iterations,
+                               double energy_threshold, void* user_data);
+
+typedef struct ws_solve_options {
+  int64_t max_iterations;        /* >= 1; the MEX call uses max_iterations or 100000 (WaveSimBase.m:127-131) */
+  double energy_threshold;       /* Simulation.energy_threshold (Simulation.m:53) */
+  int64_t energy_interval;       /* Simulation.energy_calculation_interval (default 8, Simulation.m:61,135) */
+  int stop_rule;                 /* WS_STOP_REFERENCE or WS_STOP_FRESH */
+  int output;                    /* WS_OUTPUT_EPRIME or WS_OUTPUT_FIELD */
+  int stop_on_nonfinite;         /* 1: stop with WS_ERR_DIVERGED when the energy is NaN/Inf */
+  int use_graph;                 /* 1: run the loop as one CUDA graph with a device-side while node */
+  const char* callback_type;     /* "NoCallback" (default when NULL), "EnergyAdded", "EnergyAddedDisp", ... */
+  int64_t callback_interval;     /* Simulation.callback_interval (default 50) */
+  ws_callback_fn callback;       /* may be NULL */
+  void* user_data;
+} ws_solve_options;
+
+typedef struct ws_solver_s* ws_solver;
+
+/* Fill opts with the reference defaults. */
+void ws_default_options(ws_solve_options* opts);
+
+/* Library version string. */
+const char* ws_version(void);
+
+/* Message of the last failed call on this thread ("" if none). */
+const char* ws_last_error(void);
+
+/* 1 if a grid of this size is supported by the FFT kernels. */
+int ws_size_supported(const int64_t N[4]);
+
+/*
+ * ws_run_algorithm - one solve, the argument list of RunWaveSimAlgorithmMex
+ * (WaveSimBase.m:145-146):
+ *   [E, diff_energy] = RunWaveSimAlgorithmMex(N, gamma, Nwiggles, wiggles, source,
+ *       epsilon, k02e, roi, maxIter, energy_threshold, callbackString, callback_interval)
+ * N      : [Ny, Nx, Nz, Nc] (Nc = 1 scalar, 3 vector)
+ * gamma  : Ny*Nx*Nz complex (shared by the Nc components)
+ * roi    : MATLAB's 2x4 roi matrix in column-major order
+ *          {y0, y1, x0, x1, z0, z1, c0, c1}, 1-based inclusive
+ * memory : WS_HOST or WS_DEVICE for every array argument (gamma, wiggles,
+ *          source values, E_out)
+ * E_out  : Ny*Nx*Nz*Nc complex, receives E' (the caller divides by gamma)
+ * diff_energy_out : capacity >= max_iterations doubles; receives the
+ *          per-iteration energy history; *n_iterations its length.
+ * callback / user_data: may be NULL.
+ */
+int ws_run_algorithm(const int64_t N[4], const ws_complex* gamma, int64_t n_wiggles, const ws_wiggle* wiggles,
+                     int64_t n_blocks, const ws_source_block* source, float epsilon, ws_complex k02e,
+                     const int64_t roi[8], int64_t max_iterations, double energy_threshold,
+                     const char* callback_string, int64_t callback_interval, ws_callback_fn callback,
+                     void* user_data, int memory, ws_complex* E_out, double* diff_energy_out,
+                     int64_t* n_iterations);
+
+/* ws_solver_create - uploads (or references, for WS_DEVICE) the medium and
+ * wiggle data once, plans the FFTs and allocates the iteration buffers, so
+ * that repeated solves on one medium (sources, angles) pay set-up once.
+ * Same meaning of arguments as ws_run_algorithm.  device: CUDA ordinal. */
+int ws_solver_create(const int64_t N[4], const ws_complex* gamma, int64_t n_wiggles, const ws_wiggle* wiggles,
+                     float epsilon, ws_complex k02e, const int64_t roi[8], int memory, int device,
+                     ws_solver* out);
+
+/* ws_solver_solve - runs the loop for one source.  source values live in
+ * source_memory; E_out in out_memory.  diff_energy_out (host) may be NULL.
+ * converged (may be NULL) receives 1 if the energy test stopped the loop. */
+int ws_solver_solve(ws_solver s, int64_t n_blocks, const ws_source_block* source, int source_memory,
+                    const ws_solve_options* opts, ws_complex* E_out, int out_memory, double* diff_energy_out,
+                    int64_t* n_iterations, int* converged);
+
+/* Device pointer of the solver's current E' buffer and the CUDA stream it
+ * works on (both valid until ws_solver_destroy). */
+int ws_solver_buffers(ws_solver s, void** E_prime, void** stream);
+
+/* ws_solver_time_kernels - runs n_iterations further iterations on the
+ * current state, one kernel launch at a time, and returns the mean device
+ * time of each fused kernel in ms (CUDA events on the solver's stream):
+ * ms_out[0] forward inner (wiggle + source + inner FFT),
+ * ms_out[1] outer (FFT, Green's function, inverse FFT),
+ * ms_out[2] inverse inner (inverse FFT, unwiggle, mix, accumulate, energy).
+ * bytes_out[3] (may be NULL): algorithmic bytes each launch moves. */
+int ws_solver_time_kernels(ws_solver s, int n_iterations, float ms_out[3], double bytes_out[3]);
+
+/* Number of kernel launches one iteration makes. */
+int ws_solver_launches_per_iteration(ws_solver s);
+
+int ws_solver_destroy(ws_solver s);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* WAVESIM_B200_H */

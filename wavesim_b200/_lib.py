@@ -1,0 +1,122 @@
+"""ctypes binding of the C ABI in include/wavesim_b200.h.
+
+The shared library ``libwavesim_b200.so`` is built in-tree next to this file
+(``python -m wavesim_b200.build`` or ``__graft_entry__.build()``).  There is
+no fallback: if the library is missing, importing this module raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libwavesim_b200.so")
+
+WS_OK = 0
+WS_ERR_INVALID_ARGUMENT = 1
+WS_ERR_UNSUPPORTED = 2
+WS_ERR_CUDA = 3
+WS_ERR_OUT_OF_MEMORY = 4
+WS_ERR_NO_SOURCE = 5
+WS_ERR_DIVERGED = 6
+WS_ERR_NO_DEVICE = 7
+
+WS_HOST = 0
+WS_DEVICE = 1
+WS_STOP_REFERENCE = 0
+WS_STOP_FRESH = 1
+WS_OUTPUT_EPRIME = 0
+WS_OUTPUT_FIELD = 1
+
+STATUS_NAMES = {
+    0: "WS_OK", 1: "WS_ERR_INVALID_ARGUMENT", 2: "WS_ERR_UNSUPPORTED", 3: "WS_ERR_CUDA",
+    4: "WS_ERR_OUT_OF_MEMORY", 5: "WS_ERR_NO_SOURCE", 6: "WS_ERR_DIVERGED", 7: "WS_ERR_NO_DEVICE",
+}
+
+
+class ws_complex(C.Structure):
+    _fields_ = [("re", C.c_float), ("im", C.c_float)]
+
+
+class ws_wiggle(C.Structure):
+    _fields_ = [("pxe", C.c_void_p), ("pye", C.c_void_p), ("pze", C.c_void_p),
+                ("gx", C.c_void_p), ("gy", C.c_void_p), ("gz", C.c_void_p)]
+
+
+class ws_source_block(C.Structure):
+    _fields_ = [("position", C.c_int64 * 4), ("size", C.c_int64 * 4), ("values", C.c_void_p)]
+
+
+CALLBACK = C.CFUNCTYPE(None, C.c_char_p, C.POINTER(C.c_double), C.c_int64, C.c_double, C.c_void_p)
+
+
+class ws_solve_options(C.Structure):
+    _fields_ = [("max_iterations", C.c_int64), ("energy_threshold", C.c_double),
+                ("energy_interval", C.c_int64), ("stop_rule", C.c_int), ("output", C.c_int),
+                ("stop_on_nonfinite", C.c_int), ("use_graph", C.c_int), ("callback_type", C.c_char_p),
+                ("callback_interval", C.c_int64), ("callback", CALLBACK), ("user_data", C.c_void_p)]
+
+
+# every entry point declared in include/wavesim_b200.h
+EXPORTS = [
+    "ws_default_options", "ws_version", "ws_last_error", "ws_size_supported", "ws_run_algorithm",
+    "ws_solver_create", "ws_solver_solve", "ws_solver_buffers", "ws_solver_time_kernels",
+    "ws_solver_launches_per_iteration", "ws_solver_destroy",
+]
+
+
+class WaveSimError(RuntimeError):
+    def __init__(self, status, message):
+        self.status = status
+        super().__init__(f"{STATUS_NAMES.get(status, status)}: {message}")
+
+
+def _load():
+    if not os.path.exists(LIB_PATH):
+        raise ImportError(
+            f"{LIB_PATH} is missing: build the CUDA library first (python -m wavesim_b200.build)")
+    lib = C.CDLL(LIB_PATH)
+    P = C.c_void_p
+    i64p = C.POINTER(C.c_int64)
+    lib.ws_default_options.argtypes = [C.POINTER(ws_solve_options)]
+    lib.ws_default_options.restype = None
+    lib.ws_version.restype = C.c_char_p
+    lib.ws_last_error.restype = C.c_char_p
+    lib.ws_size_supported.argtypes = [i64p]
+    lib.ws_size_supported.restype = C.c_int
+    lib.ws_run_algorithm.argtypes = [i64p, P, C.c_int64, C.POINTER(ws_wiggle), C.c_int64,
+                                     C.POINTER(ws_source_block), C.c_float, ws_complex, i64p, C.c_int64,
+                                     C.c_double, C.c_char_p, C.c_int64, CALLBACK, P, C.c_int, P,
+                                     C.POINTER(C.c_double), i64p]
+    lib.ws_run_algorithm.restype = C.c_int
+    lib.ws_solver_create.argtypes = [i64p, P, C.c_int64, C.POINTER(ws_wiggle), C.c_float, ws_complex, i64p,
+                                     C.c_int, C.c_int, C.POINTER(C.c_void_p)]
+    lib.ws_solver_create.restype = C.c_int
+    lib.ws_solver_solve.argtypes = [P, C.c_int64, C.POINTER(ws_source_block), C.c_int,
+                                    C.POINTER(ws_solve_options), P, C.c_int, C.POINTER(C.c_double), i64p,
+                                    C.POINTER(C.c_int)]
+    lib.ws_solver_solve.restype = C.c_int
+    lib.ws_solver_buffers.argtypes = [P, C.POINTER(C.c_void_p), C.POINTER(C.c_void_p)]
+    lib.ws_solver_buffers.restype = C.c_int
+    lib.ws_solver_time_kernels.argtypes = [P, C.c_int, C.POINTER(C.c_float), C.POINTER(C.c_double)]
+    lib.ws_solver_time_kernels.restype = C.c_int
+    lib.ws_solver_launches_per_iteration.argtypes = [P]
+    lib.ws_solver_launches_per_iteration.restype = C.c_int
+    lib.ws_solver_destroy.argtypes = [P]
+    lib.ws_solver_destroy.restype = C.c_int
+    return lib
+
+
+lib = _load()
+
+
+def check(status):
+    if status != WS_OK:
+        raise WaveSimError(status, lib.ws_last_error().decode(errors="replace"))
+    return status
+
+
+def default_options():
+    o = ws_solve_options()
+    lib.ws_default_options(C.byref(o))
+    return o

@@ -1,0 +1,465 @@
+// Fused MBS iteration kernels (sm_100a).
+//
+// One iteration of WaveSimBase.run_algorithm (WaveSimBase.m:165-189) is three
+// passes over HBM.  "inner" dimensions are the ones a thread block (or a
+// thread-block cluster) holds completely in shared memory; the "outer"
+// dimension is transformed by pencils in the middle pass:
+//   3-D grids (Nz > 1): inner = (y, x) planes, outer = z
+//   2-D grids (Nz == 1): inner = y columns,   outer = x
+//
+// K1 k_fwd_inner : dE (+ i/(eps Nw) S in the first Nw iterations, Source.m:167-169)
+//                  times the wiggle ramps gx gy gz (f_wiggle.m:5), forward FFT
+//                  over the inner dimensions -> T
+// K2 k_outer     : forward FFT over the outer dimension, Green's function
+//                  (f_g0_scalar.m:6 or f_g0_vector.m:4-8, with the 1/N of
+//                  ifftn folded in), inverse FFT over the outer dimension, in place on T
+// K3 k_inv_inner : inverse FFT over the inner dimensions, conj ramps
+//                  (WaveSim.m:55), f_mix (f_mix.m:3-4), E += dE, the ROI energy
+//                  sum(|dE|^2) (Simulation.m:265-273) and, in the last block to
+//                  finish, the stop rule of Simulation.next (Simulation.m:193-217).
+//
+// A 3-D plane that does not fit one block's shared memory is split over a
+// cluster of C blocks along x: the x transform is then one radix-C step across
+// the cluster through distributed shared memory plus a local transform of
+// length Nx/C (forward: X[k1 + C k2] = sum_x' W_{Nx/C}^{x' k2} W_Nx^{k1 x'}
+// sum_c x[x' + c Nx/C] W_C^{c k1}; the inverse mirrors it).
+#pragma once
+#include <cooperative_groups.h>
+#include <cuda_runtime.h>
+#include <math.h>
+#include "ws_fft.cuh"
+
+namespace ws {
+
+namespace cg = cooperative_groups;
+
+constexpr float kAlpha = 0.7f;  // private/f_mix.m:3
+
+struct Geom {
+  int ny, nx, nz, nc;
+  long long npts;  // ny * nx * nz
+  int r0[4], r1[4];  // roi, 0-based, [r0, r1) per (y, x, z, c)
+};
+
+struct Wig {
+  const float* pxe;
+  const float* pye;
+  const float* pze;
+  const float2* gx;
+  const float2* gy;
+  const float2* gz;
+};
+
+// Device-resident loop state (the fields of the reference's `state`).
+struct DevState {
+  int it;           // state.it, 1-based
+  int done;         // !state.has_next
+  int converged;    // state.converged
+  int calc_energy;  // state.calculate_energy
+  int status;       // 0 or WS_ERR_DIVERGED
+  unsigned int blocks_done;
+  int pad0, pad1;
+  double e_acc;             // partial sums of this iteration's ROI energy
+  double last_step_energy;  // state.last_step_energy
+  double diff1;             // state.diff_energy(1)
+};
+
+struct StopRule {
+  int nw;          // numel(wiggles)
+  int fresh;       // 1: WS_STOP_FRESH
+  int nan_stop;    // 1: stop when the energy is not finite
+  int interval;    // energy_calculation_interval
+  long long max_iter;
+  double threshold;
+};
+
+struct Hist {
+  double* diff;   // state.diff_energy
+  double* fresh;  // energy of every iteration
+  long long cap;
+};
+
+struct InnerArgs {
+  Geom g;
+  Wig w;
+  FftPlan py;   // length Ny
+  FftPlan pxl;  // length Nx / csize (3-D only)
+  const float2* twx;  // W_Nx^k table (cluster step)
+  int csize;    // blocks per plane (cluster size), 3-D only
+  int mode3d;
+  int ncols;    // columns per block, 2-D only
+};
+
+struct OuterArgs {
+  Geom g;
+  Wig w;
+  FftPlan po;   // length of the outer dimension
+  float2 k02e;
+  float norm;   // 1 / (Ny Nx Nz), the normalisation of ifftn
+  int ty;       // consecutive y per block
+  int mode3d;
+};
+
+__device__ __forceinline__ int load_done(const DevState* st) { return __ldcg(&st->done); }
+
+// One radix-C step across the cluster (C = a.csize > 1), in place on the
+// shared tile.  Forward: out[x'] = sum_c u_c[x'] W_Nx^{rank (x' + c M)};
+// inverse: out[x'] = sum_c u_c[x'] conj(W_Nx^{c (x' + rank M)}), M = Nx / C.
+template <int EMAX, bool INV>
+__device__ __forceinline__ void cluster_step(float2* sm, int ny, int LS, int ncol, int C, int rank, int nx,
+                                             const float2* __restrict__ twx, int tid, int nthr) {
+  cg::cluster_group cl = cg::this_cluster();
+  cl.sync();
+  float2 acc[EMAX];
+  const int m = ncol * ny;
+#pragma unroll
+  for (int q = 0; q < EMAX; ++q) {
+    const int e = tid + q * nthr;
+    if (e < m) {
+      const int xl = e / ny, y = e - xl * ny;
+      const int ad = xl * LS + y + (y >> 4);
+      float2 s = make_float2(0.f, 0.f);
+      for (int c = 0; c < C; ++c) {
+        const float2* rs = cl.map_shared_rank(sm, c);
+        const float2 u = rs[ad];
+        long long k = INV ? (long long)c * (xl + rank * ncol) : (long long)rank * (xl + c * ncol);
+        float2 w = __ldg(&twx[k % nx]);
+        if (INV) w.y = -w.y;
+        s = cadd(s, cmul(u, w));
+      }
+      acc[q] = s;
+    }
+  }
+  cl.sync();
+#pragma unroll
+  for (int q = 0; q < EMAX; ++q) {
+    const int e = tid + q * nthr;
+    if (e < m) {
+      const int xl = e / ny, y = e - xl * ny;
+      sm[xl * LS + y + (y >> 4)] = acc[q];
+    }
+  }
+  __syncthreads();
+}
+
+// K1 -------------------------------------------------------------------------
+template <int EMAX, int RSET>
+__global__ void __launch_bounds__(512, 1) k_fwd_inner(InnerArgs a, const float2* __restrict__ dE,
+                                                    const float2* __restrict__ src, float2 A,
+                                                    float2* __restrict__ T, const DevState* __restrict__ st) {
+  if (load_done(st)) return;
+  extern __shared__ float2 sm[];
+  const int tid = threadIdx.x, nthr = blockDim.x;
+  const Geom& g = a.g;
+  const int ny = g.ny, LS = padded(ny);
+  int ncol, plane = 0, rank = 0, x0 = 0, z = 0;
+  long long colbase;
+  if (a.mode3d) {
+    rank = blockIdx.x % a.csize;
+    plane = blockIdx.x / a.csize;
+    ncol = g.nx / a.csize;
+    x0 = rank * ncol;
+    z = plane % g.nz;
+    colbase = (long long)plane * g.nx + x0;
+  } else {
+    colbase = (long long)blockIdx.x * a.ncols;
+    ncol = (int)min((long long)a.ncols, (long long)g.nx * g.nc - colbase);
+  }
+  const int m = ncol * ny;
+  const float2 gzz = a.w.gz[z];
+  for (int e = tid; e < m; e += nthr) {
+    const int xl = e / ny, y = e - xl * ny;
+    const long long col = colbase + xl;
+    const long long gi = col * ny + y;
+    float2 v = dE[gi];
+    if (src) v = cadd(v, cmul(A, src[gi]));
+    const int x = a.mode3d ? x0 + xl : (int)(col % g.nx);
+    v = cmul(cmul(cmul(v, a.w.gx[x]), a.w.gy[y]), gzz);
+    sm[xl * LS + y + (y >> 4)] = v;
+  }
+  __syncthreads();
+  fft_lines<false, EMAX, RSET>(sm, Lines{ncol, LS, 1}, a.py, tid, nthr);
+  if (a.mode3d && g.nx > 1) {
+    if (a.csize > 1) cluster_step<EMAX, false>(sm, ny, LS, ncol, a.csize, rank, g.nx, a.twx, tid, nthr);
+    fft_lines<false, EMAX, RSET>(sm, Lines{ny, LS, 0}, a.pxl, tid, nthr);
+  }
+  for (int e = tid; e < m; e += nthr) {
+    const int xl = e / ny, y = e - xl * ny;
+    long long col;
+    if (a.mode3d) {
+      const int kx = a.csize > 1 ? rank + a.csize * xl : xl;
+      col = (long long)plane * g.nx + kx;
+    } else {
+      col = colbase + xl;
+    }
+    T[col * ny + y] = sm[xl * LS + y + (y >> 4)];
+  }
+}
+
+// K2 -------------------------------------------------------------------------
+template <int EMAX, int RSET>
+__global__ void __launch_bounds__(512, 1) k_outer(OuterArgs a, float2* __restrict__ T, const DevState* __restrict__ st) {
+  if (load_done(st)) return;
+  extern __shared__ float2 sm[];
+  const int tid = threadIdx.x, nthr = blockDim.x;
+  const Geom& g = a.g;
+  const int ty = a.ty, nc = g.nc;
+  const int nyt = (g.ny + ty - 1) / ty;
+  const int yt = blockIdx.x % nyt;
+  const int mid = a.mode3d ? blockIdx.x / nyt : 0;
+  const int y0 = yt * ty;
+  const int no = a.mode3d ? g.nz : g.nx;
+  const long long ps = a.mode3d ? (long long)g.ny * g.nx : (long long)g.ny;
+  const long long base = y0 + (long long)g.ny * mid;
+  const int L = nc * ty;
+  const int RS = padded(L);
+  const int m = no * L;
+  for (int e = tid; e < m; e += nthr) {
+    const int yl = e % ty, r = e / ty;
+    const int c = r % nc, o = r / nc;
+    const int l = c * ty + yl;
+    float2 v = make_float2(0.f, 0.f);
+    if (y0 + yl < g.ny) v = T[base + yl + ps * o + g.npts * c];
+    sm[o * RS + l + (l >> 4)] = v;
+  }
+  __syncthreads();
+  fft_lines<false, EMAX, RSET>(sm, Lines{L, RS, 0}, a.po, tid, nthr);
+  // Green's function in the fully transformed (ky, kx, kz) space
+  for (int e = tid; e < no * ty; e += nthr) {
+    const int yl = e % ty, o = e / ty;
+    const int ky = y0 + yl;
+    if (ky >= g.ny) continue;
+    const int kx = a.mode3d ? mid : o;
+    const int kz = a.mode3d ? o : 0;
+    const float px = a.w.pxe[kx], py = a.w.pye[ky], pz = a.w.pze[kz];
+    if (nc == 1) {
+      // f_g0_scalar: E ./ (px^2 + py^2 + (pz^2 - k02e))
+      const float dr = fmaf(px, px, fmaf(py, py, pz * pz)) - a.k02e.x;
+      const float di = -a.k02e.y;
+      const float inv = a.norm / fmaf(dr, dr, di * di);
+      const int ad = o * RS + yl + (yl >> 4);
+      sm[ad] = cmul(sm[ad], make_float2(dr * inv, -di * inv));
+    } else {
+      // f_g0_vector: div = (p . E) / k02e; E_i <- (E_i - p_i div) / (|p|^2 - k02e)
+      const int l0 = yl, l1 = ty + yl, l2 = 2 * ty + yl;
+      const int a0 = o * RS + l0 + (l0 >> 4), a1 = o * RS + l1 + (l1 >> 4), a2 = o * RS + l2 + (l2 >> 4);
+      const float2 ex = sm[a0], ey = sm[a1], ez = sm[a2];
+      const float2 pe = make_float2(fmaf(px, ex.x, fmaf(py, ey.x, pz * ez.x)), fmaf(px, ex.y, fmaf(py, ey.y, pz * ez.y)));
+      const float kk = fmaf(a.k02e.x, a.k02e.x, a.k02e.y * a.k02e.y);
+      const float2 div = make_float2((pe.x * a.k02e.x + pe.y * a.k02e.y) / kk, (pe.y * a.k02e.x - pe.x * a.k02e.y) / kk);
+      const float dr = fmaf(px, px, fmaf(py, py, pz * pz)) - a.k02e.x;
+      const float di = -a.k02e.y;
+      const float inv = a.norm / fmaf(dr, dr, di * di);
+      const float2 g0 = make_float2(dr * inv, -di * inv);
+      sm[a0] = cmul(g0, make_float2(ex.x - px * div.x, ex.y - px * div.y));
+      sm[a1] = cmul(g0, make_float2(ey.x - py * div.x, ey.y - py * div.y));
+      sm[a2] = cmul(g0, make_float2(ez.x - pz * div.x, ez.y - pz * div.y));
+    }
+  }
+  __syncthreads();
+  fft_lines<true, EMAX, RSET>(sm, Lines{L, RS, 0}, a.po, tid, nthr);
+  for (int e = tid; e < m; e += nthr) {
+    const int yl = e % ty, r = e / ty;
+    const int c = r % nc, o = r / nc;
+    const int l = c * ty + yl;
+    if (y0 + yl < g.ny) T[base + yl + ps * o + g.npts * c] = sm[o * RS + l + (l >> 4)];
+  }
+}
+
+// Simulation.next (Simulation.m:193-217), run by one thread after the energy
+// of iteration st->it is complete.
+__device__ __forceinline__ void finish_iteration(DevState* st, const StopRule& rule, const Hist& h,
+                                                 cudaGraphConditionalHandle cond, int set_cond) {
+  const double e = atomicAdd(&st->e_acc, 0.0);
+  st->e_acc = 0.0;
+  const int it = st->it;
+  if (h.fresh && it - 1 < h.cap) h.fresh[it - 1] = e;
+  if (st->calc_energy || rule.fresh) st->last_step_energy = e;
+  const double d = st->last_step_energy;
+  if (it - 1 < h.cap) h.diff[it - 1] = d;
+  if (it == 1) st->diff1 = d;
+  const bool can_terminate = (it % rule.nw) == 0;
+  if (can_terminate && d / st->diff1 < rule.threshold) {
+    st->done = 1;
+    st->converged = 1;
+  } else if (can_terminate && it >= rule.max_iter) {
+    st->done = 1;
+    st->converged = 0;
+  }
+  if (rule.nan_stop && !isfinite(e)) {
+    st->done = 1;
+    st->converged = 0;
+    st->status = 6;  // WS_ERR_DIVERGED
+  }
+  st->calc_energy = ((it - 1) % rule.interval) == 0;
+  st->it = it + 1;
+  st->blocks_done = 0;
+  __threadfence();
+  if (set_cond) cudaGraphSetConditional(cond, st->done ? 0u : 1u);
+}
+
+// K3 -------------------------------------------------------------------------
+template <int EMAX, int RSET>
+__global__ void __launch_bounds__(512, 1) k_inv_inner(InnerArgs a, const float2* __restrict__ T, float2* __restrict__ dE,
+                                                    float2* __restrict__ E, const float2* __restrict__ gamma,
+                                                    DevState* st, StopRule rule, Hist h,
+                                                    cudaGraphConditionalHandle cond, int set_cond) {
+  if (load_done(st)) {
+    if (set_cond && blockIdx.x == 0 && threadIdx.x == 0) cudaGraphSetConditional(cond, 0u);
+    return;
+  }
+  extern __shared__ float2 sm[];
+  __shared__ float red[32];
+  __shared__ unsigned int ticket;
+  const int tid = threadIdx.x, nthr = blockDim.x;
+  const Geom& g = a.g;
+  const int ny = g.ny, LS = padded(ny);
+  int ncol, plane = 0, rank = 0, x0 = 0, z = 0, comp = 0;
+  long long colbase;
+  if (a.mode3d) {
+    rank = blockIdx.x % a.csize;
+    plane = blockIdx.x / a.csize;
+    ncol = g.nx / a.csize;
+    x0 = rank * ncol;
+    z = plane % g.nz;
+    comp = plane / g.nz;
+    colbase = (long long)plane * g.nx + x0;
+  } else {
+    colbase = (long long)blockIdx.x * a.ncols;
+    ncol = (int)min((long long)a.ncols, (long long)g.nx * g.nc - colbase);
+  }
+  const int m = ncol * ny;
+  for (int e = tid; e < m; e += nthr) {
+    const int xl = e / ny, y = e - xl * ny;
+    long long col;
+    if (a.mode3d) {
+      const int kx = a.csize > 1 ? rank + a.csize * xl : xl;
+      col = (long long)plane * g.nx + kx;
+    } else {
+      col = colbase + xl;
+    }
+    sm[xl * LS + y + (y >> 4)] = T[col * ny + y];
+  }
+  __syncthreads();
+  if (a.mode3d && g.nx > 1) {
+    fft_lines<true, EMAX, RSET>(sm, Lines{ny, LS, 0}, a.pxl, tid, nthr);
+    if (a.csize > 1) cluster_step<EMAX, true>(sm, ny, LS, ncol, a.csize, rank, g.nx, a.twx, tid, nthr);
+  }
+  fft_lines<true, EMAX, RSET>(sm, Lines{ncol, LS, 1}, a.py, tid, nthr);
+  const float2 gzz = a.w.gz[z];
+  float esum = 0.f;
+  for (int e = tid; e < m; e += nthr) {
+    const int xl = e / ny, y = e - xl * ny;
+    const long long col = colbase + xl;
+    const long long gi = col * ny + y;
+    int x, c;
+    if (a.mode3d) {
+      x = x0 + xl;
+      c = comp;
+    } else {
+      x = (int)(col % g.nx);
+      c = (int)(col / g.nx);
+    }
+    // Eprop after the inverse transform and the conjugate ramps (WaveSim.m:53-55)
+    const float2 ep = cmul_conj(cmul_conj(cmul_conj(sm[xl * LS + y + (y >> 4)], a.w.gx[x]), a.w.gy[y]), gzz);
+    const float2 gm = gamma[gi - (long long)c * g.npts];
+    const float2 d0 = dE[gi];
+    // f_mix: (1 - a gamma) dE - i a gamma^2 Eprop
+    const float2 one_m = make_float2(1.f - kAlpha * gm.x, -kAlpha * gm.y);
+    const float2 g2 = cmul(gm, gm);
+    const float2 t = cmul(g2, ep);
+    const float2 dn = cadd(cmul(one_m, d0), make_float2(kAlpha * t.y, -kAlpha * t.x));
+    dE[gi] = dn;
+    const float2 e0 = E[gi];
+    E[gi] = cadd(e0, dn);
+    if (y >= g.r0[0] && y < g.r1[0] && x >= g.r0[1] && x < g.r1[1] && z >= g.r0[2] && z < g.r1[2] &&
+        c >= g.r0[3] && c < g.r1[3])
+      esum = fmaf(dn.x, dn.x, fmaf(dn.y, dn.y, esum));
+  }
+  // block reduction of the ROI energy, then one atomic per block
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) esum += __shfl_xor_sync(0xffffffffu, esum, o);
+  if ((tid & 31) == 0) red[tid >> 5] = esum;
+  __syncthreads();
+  if (tid < 32) {
+    float v = tid < (nthr + 31) / 32 ? red[tid] : 0.f;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    if (tid == 0) {
+      atomicAdd(&st->e_acc, (double)v);
+      __threadfence();
+      ticket = atomicAdd(&st->blocks_done, 1u);
+    }
+  }
+  __syncthreads();
+  if (tid == 0 && ticket == gridDim.x - 1) {
+    __threadfence();
+    finish_iteration(st, rule, h, cond, set_cond);
+  }
+}
+
+// Helpers --------------------------------------------------------------------
+__global__ void k_reset_state(DevState* st) {
+  if (threadIdx.x == 0 && blockIdx.x == 0) {
+    st->it = 1;
+    st->done = 0;
+    st->converged = 0;
+    st->calc_energy = 1;
+    st->status = 0;
+    st->blocks_done = 0;
+    st->e_acc = 0.0;
+    st->last_step_energy = __longlong_as_double(0x7ff0000000000000LL);  // inf (Simulation.m:169)
+    st->diff1 = 0.0;
+  }
+}
+
+__global__ void k_resume_state(DevState* st) {
+  if (threadIdx.x == 0 && blockIdx.x == 0) {
+    st->done = 0;
+    st->blocks_done = 0;
+    st->e_acc = 0.0;
+  }
+}
+
+// Source.add_to for one block (values at 0-based corner p, size s), into the
+// dense source buffer; also accumulates the block energy (Source.m:57-67).
+__global__ void k_scatter_source(float2* __restrict__ dst, const float2* __restrict__ vals, Geom g, int p0, int p1,
+                                 int p2, int p3, int s0, int s1, int s2, int s3, double* energy) {
+  const long long n = (long long)s0 * s1 * s2 * s3;
+  float esum = 0.f;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    long long r = i;
+    const int a0 = (int)(r % s0); r /= s0;
+    const int a1 = (int)(r % s1); r /= s1;
+    const int a2 = (int)(r % s2); r /= s2;
+    const int a3 = (int)r;
+    const long long gi = (p0 + a0) + (long long)g.ny * ((p1 + a1) + (long long)g.nx * ((p2 + a2) + (long long)g.nz * (p3 + a3)));
+    const float2 v = vals[i];
+    dst[gi] = cadd(dst[gi], v);
+    esum = fmaf(v.x, v.x, fmaf(v.y, v.y, esum));
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) esum += __shfl_xor_sync(0xffffffffu, esum, o);
+  if ((threadIdx.x & 31) == 0) atomicAdd(energy, (double)esum);
+}
+
+// E = E' ./ gamma on the roi (WaveSimBase.m:193,196), column-major output.
+__global__ void k_finalize(const float2* __restrict__ Ep, const float2* __restrict__ gamma, Geom g,
+                           float2* __restrict__ out) {
+  const int ry = g.r1[0] - g.r0[0], rx = g.r1[1] - g.r0[1], rz = g.r1[2] - g.r0[2], rc = g.r1[3] - g.r0[3];
+  const long long n = (long long)ry * rx * rz * rc;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    long long r = i;
+    const int y = (int)(r % ry) + g.r0[0]; r /= ry;
+    const int x = (int)(r % rx) + g.r0[1]; r /= rx;
+    const int z = (int)(r % rz) + g.r0[2]; r /= rz;
+    const int c = (int)r + g.r0[3];
+    const long long gi0 = y + (long long)g.ny * (x + (long long)g.nx * z);
+    const float2 e = Ep[gi0 + (long long)c * g.npts];
+    const float2 d = gamma[gi0];
+    const float dd = fmaf(d.x, d.x, d.y * d.y);
+    out[i] = make_float2((e.x * d.x + e.y * d.y) / dd, (e.y * d.x - e.x * d.y) / dd);
+  }
+}
+
+}  // namespace ws

@@ -1,0 +1,841 @@
+// C ABI of the B200 MBS loop (declared in include/wavesim_b200.h).
+//
+// Host runtime: FFT planning (radix schedules, twiddle tables, tile and
+// cluster shapes), device buffers, the per-solver CUDA stream, and the loop
+// driver.  The loop runs either as one CUDA graph (first wiggle cycle with the
+// source, then a device-side while node over the steady cycle whose condition
+// the last block of the cycle's final K3 sets) or, when a host callback needs
+// the history, as launches from a host loop.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "wavesim_b200.h"
+#include "ws_kernels.cuh"
+
+namespace ws {
+
+constexpr int kEmax = 16;           // max elements per thread per FFT stage
+constexpr int kMaxThreadsPow2 = 512;
+constexpr int kMaxThreadsMixed = 512;
+constexpr size_t kSmemBudget = 150 * 1024;  // per-block tile budget (bytes)
+constexpr int kNumSms = 148;
+
+thread_local std::string g_last_error;
+
+static int fail(int code, const std::string& msg) {
+  g_last_error = msg;
+  return code;
+}
+
+#define WS_CUDA(call)                                                                          \
+  do {                                                                                         \
+    cudaError_t err__ = (call);                                                                \
+    if (err__ != cudaSuccess) {                                                                \
+      return fail(err__ == cudaErrorMemoryAllocation ? WS_ERR_OUT_OF_MEMORY : WS_ERR_CUDA,     \
+                  std::string(#call) + ": " + cudaGetErrorString(err__));                      \
+    }                                                                                          \
+  } while (0)
+
+// ---------------------------------------------------------------------------
+// planning
+// ---------------------------------------------------------------------------
+static bool plan_radices(int n, std::vector<int>& out) {
+  out.clear();
+  static const int pref[] = {16, 12, 13, 11, 10, 9, 8, 7, 6, 5, 4, 3, 2};
+  while (n > 1) {
+    bool found = false;
+    for (int r : pref) {
+      if (n % r == 0) {
+        out.push_back(r);
+        n /= r;
+        found = true;
+        break;
+      }
+    }
+    if (!found) return false;
+  }
+  return (int)out.size() <= kMaxStages;
+}
+
+static bool length_supported(int n) {
+  std::vector<int> r;
+  return n >= 1 && n <= 65536 && plan_radices(n, r);
+}
+
+struct Layout {
+  int rset = kPow2;  // radix set of every plan of the solver
+  int mode3d = 0;
+  int csize = 1;     // 3-D: blocks (cluster) per plane
+  int ncols = 1;     // 2-D: columns per block
+  int ty = 16;       // outer pass: consecutive y per block
+  int th_inner = 256, th_outer = 256;
+  size_t smem_inner = 0, smem_outer = 0;
+  long long grid_inner = 0, grid_outer = 0;
+};
+
+static bool is_pow2(long long n) { return n >= 1 && (n & (n - 1)) == 0; }
+
+static int make_layout(const Geom& g, Layout& L, std::string& why) {
+  L.mode3d = g.nz > 1;
+  L.rset = kPow2;
+  for (long long n : {(long long)g.ny, (long long)g.nx, (long long)g.nz})
+    if (!is_pow2(n)) L.rset = kMixed;
+  const int kMaxThreads = L.rset == kPow2 ? kMaxThreadsPow2 : kMaxThreadsMixed;
+  auto threads_for = [&](long long elems) {
+    long long t = (elems + kEmax - 1) / kEmax;
+    t = ((t + 31) / 32) * 32;
+    return (int)std::max(32LL, std::min((long long)kMaxThreads, t));
+  };
+  const int ny = g.ny;
+  const size_t col_bytes = (size_t)padded(ny) * sizeof(float2);
+  if (L.mode3d) {
+    // smallest divisor C of Nx (<= 16) whose tile fits
+    int best = 0;
+    for (int c = 1; c <= 16; ++c) {
+      if (g.nx % c) continue;
+      const long long cols = g.nx / c;
+      const long long elems = cols * ny;
+      if (elems > (long long)kMaxThreads * kEmax) continue;
+      if (cols * col_bytes > kSmemBudget) continue;
+      if (c > 1 && !length_supported((int)cols)) continue;
+      best = c;
+      break;
+    }
+    if (!best) {
+      why = "an Ny x Nx plane of this size does not fit a cluster of 16 blocks";
+      return WS_ERR_UNSUPPORTED;
+    }
+    L.csize = best;
+    const long long cols = g.nx / best;
+    L.th_inner = threads_for(cols * ny);
+    L.smem_inner = cols * col_bytes;
+    L.grid_inner = (long long)g.nz * g.nc * best;
+  } else {
+    const long long total_cols = (long long)g.nx * g.nc;
+    const long long max_cols_fit = std::max(1LL, std::min((long long)(kSmemBudget / col_bytes),
+                                                          (long long)kMaxThreads * kEmax / (long long)ny));
+    if ((long long)ny > (long long)kMaxThreads * kEmax || col_bytes > kSmemBudget) {
+      why = "Ny too large for one block";
+      return WS_ERR_UNSUPPORTED;
+    }
+    // aim for >= 2 blocks per SM, at most ~8K elements per block
+    long long want = std::max(1LL, std::min(max_cols_fit, (8192LL + ny - 1) / ny));
+    while (want > 1 && (total_cols + want - 1) / want < 2 * kNumSms) want /= 2;
+    L.ncols = (int)want;
+    L.th_inner = threads_for((long long)want * ny);
+    L.smem_inner = want * col_bytes;
+    L.grid_inner = (total_cols + want - 1) / want;
+  }
+  // outer pass
+  const int no = L.mode3d ? g.nz : g.nx;
+  const long long mids = L.mode3d ? g.nx : 1;
+  int ty = 16;
+  while (ty > 1 && ((long long)padded(g.nc * ty) * no * sizeof(float2) > kSmemBudget ||
+                    (long long)g.nc * ty * no > (long long)kMaxThreads * kEmax))
+    ty /= 2;
+  if (ty > g.ny) ty = std::max(1, g.ny);
+  while (ty > 4 && ((g.ny + ty - 1) / ty) * mids < 2 * kNumSms) ty /= 2;
+  if ((long long)padded(g.nc * ty) * no * sizeof(float2) > kSmemBudget ||
+      (long long)g.nc * ty * no > (long long)kMaxThreads * kEmax) {
+    why = "outer dimension too long for one block";
+    return WS_ERR_UNSUPPORTED;
+  }
+  L.ty = ty;
+  L.th_outer = threads_for((long long)g.nc * ty * no);
+  L.smem_outer = (size_t)padded(g.nc * ty) * no * sizeof(float2);
+  L.grid_outer = (long long)((g.ny + ty - 1) / ty) * mids;
+  return WS_OK;
+}
+
+// ---------------------------------------------------------------------------
+// solver object
+// ---------------------------------------------------------------------------
+struct GraphKey {
+  double threshold = -1;
+  long long max_iter = -1;
+  int interval = -1, stop_rule = -1, nan_stop = -1;
+  bool operator==(const GraphKey& o) const {
+    return threshold == o.threshold && max_iter == o.max_iter && interval == o.interval &&
+           stop_rule == o.stop_rule && nan_stop == o.nan_stop;
+  }
+};
+
+struct Solver {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  Geom g{};
+  Layout lay;
+  int nw = 0;
+  float eps = 0.f;
+  float2 k02e{};
+  std::vector<Wig> wig;
+  float* d_wigf = nullptr;   // all pxe/pye/pze
+  float2* d_wigc = nullptr;  // all gx/gy/gz
+  float2* d_gamma = nullptr;
+  float2 *d_E = nullptr, *d_dE = nullptr, *d_T = nullptr, *d_src = nullptr;
+  float2* d_stage = nullptr;
+  size_t stage_cap = 0;
+  float2* d_out = nullptr;
+  size_t out_cap = 0;
+  DevState* d_state = nullptr;
+  double* d_hist = nullptr;  // diff | fresh
+  long long hist_cap = 0;
+  double* d_energy = nullptr;
+  float2* d_tw = nullptr;
+  FftPlan py{}, pxl{}, po{};
+  const float2* twx = nullptr;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t gexec = nullptr;
+  GraphKey gkey;
+  cudaEvent_t ev[8] = {};
+};
+
+static void free_graph(Solver* s) {
+  if (s->gexec) cudaGraphExecDestroy(s->gexec);
+  if (s->graph) cudaGraphDestroy(s->graph);
+  s->gexec = nullptr;
+  s->graph = nullptr;
+}
+
+static void destroy_solver(Solver* s) {
+  if (!s) return;
+  cudaSetDevice(s->device);
+  free_graph(s);
+  void* ptrs[] = {s->d_wigf, s->d_wigc, s->d_gamma, s->d_E,     s->d_dE,     s->d_T,  s->d_src,
+                  s->d_stage, s->d_out, s->d_state, s->d_hist, s->d_energy, s->d_tw};
+  for (void* p : ptrs)
+    if (p) cudaFree(p);
+  for (auto& e : s->ev)
+    if (e) cudaEventDestroy(e);
+  if (s->stream) cudaStreamDestroy(s->stream);
+  delete s;
+}
+
+static int build_plan(int n, const std::vector<float2>& tw_all_offset_dummy, FftPlan& p) {
+  (void)tw_all_offset_dummy;
+  std::vector<int> r;
+  if (!plan_radices(n, r)) return WS_ERR_UNSUPPORTED;
+  p.n = n;
+  p.nst = (int)r.size();
+  for (int i = 0; i < kMaxStages; ++i) p.radix[i] = i < (int)r.size() ? r[i] : 1;
+  return WS_OK;
+}
+
+static void push_twiddles(std::vector<float2>& all, int n, size_t& off) {
+  off = all.size();
+  for (int k = 0; k < n; ++k) {
+    const double a = -2.0 * M_PI * (double)k / (double)n;
+    all.push_back(make_float2((float)std::cos(a), (float)std::sin(a)));
+  }
+}
+
+template <int RS>
+static cudaError_t set_attributes_for() {
+  const int maxsm = 227 * 1024;
+  cudaError_t e;
+  if ((e = cudaFuncSetAttribute(k_fwd_inner<kEmax, RS>, cudaFuncAttributeMaxDynamicSharedMemorySize, maxsm))) return e;
+  if ((e = cudaFuncSetAttribute(k_inv_inner<kEmax, RS>, cudaFuncAttributeMaxDynamicSharedMemorySize, maxsm))) return e;
+  if ((e = cudaFuncSetAttribute(k_outer<kEmax, RS>, cudaFuncAttributeMaxDynamicSharedMemorySize, maxsm))) return e;
+  if ((e = cudaFuncSetAttribute(k_fwd_inner<kEmax, RS>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1))) return e;
+  return cudaFuncSetAttribute(k_inv_inner<kEmax, RS>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+}
+
+static int set_kernel_attributes() {
+  // per device: attributes are per-context
+  static int done_mask = 0;
+  int dev = 0;
+  WS_CUDA(cudaGetDevice(&dev));
+  if (dev < 31 && (done_mask >> dev) & 1) return WS_OK;
+  WS_CUDA(set_attributes_for<kPow2>());
+  WS_CUDA(set_attributes_for<kMixed>());
+  if (dev < 31) done_mask |= 1 << dev;
+  return WS_OK;
+}
+
+static int check_args(const int64_t N[4], int64_t n_wiggles, const ws_wiggle* wiggles, const ws_complex* gamma,
+                      const int64_t roi[8], Geom& g) {
+  if (!N || !gamma || !wiggles || !roi) return fail(WS_ERR_INVALID_ARGUMENT, "null argument");
+  for (int i = 0; i < 4; ++i)
+    if (N[i] < 1) return fail(WS_ERR_INVALID_ARGUMENT, "N must be positive");
+  if (N[3] != 1 && N[3] != 3) return fail(WS_ERR_INVALID_ARGUMENT, "N(4) must be 1 (scalar) or 3 (vector)");
+  if (N[0] > 65536 || N[1] > 65536 || N[2] > 65536)
+    return fail(WS_ERR_UNSUPPORTED, "grid dimension larger than 65536");
+  if (n_wiggles < 1 || n_wiggles > 64) return fail(WS_ERR_INVALID_ARGUMENT, "Nwiggles must be in [1, 64]");
+  g.ny = (int)N[0];
+  g.nx = (int)N[1];
+  g.nz = (int)N[2];
+  g.nc = (int)N[3];
+  g.npts = (long long)g.ny * g.nx * g.nz;
+  if (g.npts * g.nc > (1LL << 31)) return fail(WS_ERR_UNSUPPORTED, "grid larger than 2^31 elements");
+  for (int d = 0; d < 4; ++d) {
+    const int64_t a = roi[2 * d], b = roi[2 * d + 1];
+    if (a < 1 || b < a || b > N[d]) return fail(WS_ERR_INVALID_ARGUMENT, "roi outside the grid");
+    g.r0[d] = (int)(a - 1);
+    g.r1[d] = (int)b;
+  }
+  for (int d = 0; d < 3; ++d)
+    if (!length_supported((int)N[d]))
+      return fail(WS_ERR_UNSUPPORTED, "grid dimension " + std::to_string(N[d]) +
+                                          " has a prime factor above 13 (use an efficient size)");
+  return WS_OK;
+}
+
+static cudaMemcpyKind kind_from(int memory) { return memory == WS_DEVICE ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice; }
+
+static int create_solver(const int64_t N[4], const ws_complex* gamma, int64_t n_wiggles, const ws_wiggle* wiggles,
+                         float epsilon, ws_complex k02e, const int64_t roi[8], int memory, int device, Solver** out) {
+  Geom g{};
+  int rc = check_args(N, n_wiggles, wiggles, gamma, roi, g);
+  if (rc) return rc;
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return fail(WS_ERR_NO_DEVICE, "no CUDA device");
+  if (device < 0 || device >= ndev) return fail(WS_ERR_INVALID_ARGUMENT, "bad device ordinal");
+  WS_CUDA(cudaSetDevice(device));
+  rc = set_kernel_attributes();
+  if (rc) return rc;
+  Solver* s = new Solver();
+  s->device = device;
+  s->g = g;
+  s->nw = (int)n_wiggles;
+  s->eps = epsilon;
+  s->k02e = make_float2(k02e.re, k02e.im);
+  std::string why;
+  rc = make_layout(g, s->lay, why);
+  if (rc) {
+    destroy_solver(s);
+    return fail(rc, why);
+  }
+#define WS_TRY(call)                 \
+  do {                               \
+    cudaError_t e__ = (call);        \
+    if (e__ != cudaSuccess) {        \
+      destroy_solver(s);             \
+      return fail(e__ == cudaErrorMemoryAllocation ? WS_ERR_OUT_OF_MEMORY : WS_ERR_CUDA, \
+                  std::string(#call) + ": " + cudaGetErrorString(e__)); \
+    }                                \
+  } while (0)
+  WS_TRY(cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking));
+  for (auto& e : s->ev) WS_TRY(cudaEventCreate(&e));
+  // plans and twiddle tables
+  std::vector<float2> tw;
+  size_t off_y, off_x, off_xl, off_o;
+  const int no = s->lay.mode3d ? g.nz : g.nx;
+  const int nxl = s->lay.mode3d ? g.nx / s->lay.csize : 1;
+  push_twiddles(tw, g.ny, off_y);
+  push_twiddles(tw, g.nx, off_x);
+  push_twiddles(tw, nxl, off_xl);
+  push_twiddles(tw, no, off_o);
+  WS_TRY(cudaMalloc(&s->d_tw, tw.size() * sizeof(float2)));
+  WS_TRY(cudaMemcpy(s->d_tw, tw.data(), tw.size() * sizeof(float2), cudaMemcpyHostToDevice));
+  build_plan(g.ny, tw, s->py);
+  s->py.tw = s->d_tw + off_y;
+  build_plan(nxl, tw, s->pxl);
+  s->pxl.tw = s->d_tw + off_xl;
+  build_plan(no, tw, s->po);
+  s->po.tw = s->d_tw + off_o;
+  s->twx = s->d_tw + off_x;
+  // wiggles
+  const size_t nf = (size_t)g.nx + g.ny + g.nz;
+  WS_TRY(cudaMalloc(&s->d_wigf, nf * n_wiggles * sizeof(float)));
+  WS_TRY(cudaMalloc(&s->d_wigc, nf * n_wiggles * sizeof(float2)));
+  const cudaMemcpyKind kind = kind_from(memory);
+  for (int w = 0; w < n_wiggles; ++w) {
+    const ws_wiggle& W = wiggles[w];
+    if (!W.pxe || !W.pye || !W.pze || !W.gx || !W.gy || !W.gz) {
+      destroy_solver(s);
+      return fail(WS_ERR_INVALID_ARGUMENT, "null wiggle array");
+    }
+    float* f = s->d_wigf + nf * w;
+    float2* c = s->d_wigc + nf * w;
+    WS_TRY(cudaMemcpy(f, W.pxe, g.nx * sizeof(float), kind));
+    WS_TRY(cudaMemcpy(f + g.nx, W.pye, g.ny * sizeof(float), kind));
+    WS_TRY(cudaMemcpy(f + g.nx + g.ny, W.pze, g.nz * sizeof(float), kind));
+    WS_TRY(cudaMemcpy(c, W.gx, g.nx * sizeof(float2), kind));
+    WS_TRY(cudaMemcpy(c + g.nx, W.gy, g.ny * sizeof(float2), kind));
+    WS_TRY(cudaMemcpy(c + g.nx + g.ny, W.gz, g.nz * sizeof(float2), kind));
+    s->wig.push_back(Wig{f, f + g.nx, f + g.nx + g.ny, c, c + g.nx, c + g.nx + g.ny});
+  }
+  const size_t nbytes = (size_t)g.npts * g.nc * sizeof(float2);
+  WS_TRY(cudaMalloc(&s->d_gamma, (size_t)g.npts * sizeof(float2)));
+  WS_TRY(cudaMemcpy(s->d_gamma, gamma, (size_t)g.npts * sizeof(float2), kind));
+  WS_TRY(cudaMalloc(&s->d_E, nbytes));
+  WS_TRY(cudaMalloc(&s->d_dE, nbytes));
+  WS_TRY(cudaMalloc(&s->d_T, nbytes));
+  WS_TRY(cudaMalloc(&s->d_src, nbytes));
+  WS_TRY(cudaMalloc(&s->d_state, sizeof(DevState)));
+  WS_TRY(cudaMalloc(&s->d_energy, sizeof(double)));
+  WS_TRY(cudaMemset(s->d_E, 0, nbytes));
+  WS_TRY(cudaMemset(s->d_dE, 0, nbytes));
+#undef WS_TRY
+  *out = s;
+  return WS_OK;
+}
+
+static InnerArgs inner_args(const Solver* s, int w) {
+  InnerArgs a{};
+  a.g = s->g;
+  a.w = s->wig[w];
+  a.py = s->py;
+  a.pxl = s->pxl;
+  a.twx = s->twx;
+  a.csize = s->lay.csize;
+  a.mode3d = s->lay.mode3d;
+  a.ncols = s->lay.ncols;
+  return a;
+}
+
+static OuterArgs outer_args(const Solver* s, int w) {
+  OuterArgs a{};
+  a.g = s->g;
+  a.w = s->wig[w];
+  a.po = s->po;
+  a.k02e = s->k02e;
+  a.norm = (float)(1.0 / ((double)s->g.npts));
+  a.ty = s->lay.ty;
+  a.mode3d = s->lay.mode3d;
+  return a;
+}
+
+template <int RS>
+static cudaError_t launch_k1_t(const Solver* s, int w, bool with_source) {
+  const float2 A = make_float2(0.f, (float)(1.0f / s->eps / (float)s->nw));  // 1i/epsilon/Nwiggles
+  cudaLaunchConfig_t cfg{};
+  cfg.gridDim = dim3((unsigned)s->lay.grid_inner);
+  cfg.blockDim = dim3(s->lay.th_inner);
+  cfg.dynamicSmemBytes = s->lay.smem_inner;
+  cfg.stream = s->stream;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeClusterDimension;
+  attr[0].val.clusterDim.x = s->lay.mode3d ? s->lay.csize : 1;
+  attr[0].val.clusterDim.y = 1;
+  attr[0].val.clusterDim.z = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelEx(&cfg, k_fwd_inner<kEmax, RS>, inner_args(s, w), (const float2*)s->d_dE,
+                            (const float2*)(with_source ? s->d_src : nullptr), A, s->d_T,
+                            (const DevState*)s->d_state);
+}
+
+template <int RS>
+static cudaError_t launch_k2_t(const Solver* s, int w) {
+  k_outer<kEmax, RS><<<(unsigned)s->lay.grid_outer, s->lay.th_outer, s->lay.smem_outer, s->stream>>>(
+      outer_args(s, w), s->d_T, s->d_state);
+  return cudaGetLastError();
+}
+
+template <int RS>
+static cudaError_t launch_k3_t(const Solver* s, int w, const StopRule& rule, const Hist& h,
+                               cudaGraphConditionalHandle cond, int set_cond) {
+  cudaLaunchConfig_t cfg{};
+  cfg.gridDim = dim3((unsigned)s->lay.grid_inner);
+  cfg.blockDim = dim3(s->lay.th_inner);
+  cfg.dynamicSmemBytes = s->lay.smem_inner;
+  cfg.stream = s->stream;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeClusterDimension;
+  attr[0].val.clusterDim.x = s->lay.mode3d ? s->lay.csize : 1;
+  attr[0].val.clusterDim.y = 1;
+  attr[0].val.clusterDim.z = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelEx(&cfg, k_inv_inner<kEmax, RS>, inner_args(s, w), (const float2*)s->d_T, s->d_dE,
+                            s->d_E, (const float2*)s->d_gamma, s->d_state, rule, h, cond, set_cond);
+}
+
+static cudaError_t launch_k1(const Solver* s, int w, bool with_source) {
+  return s->lay.rset == kPow2 ? launch_k1_t<kPow2>(s, w, with_source) : launch_k1_t<kMixed>(s, w, with_source);
+}
+static cudaError_t launch_k2(const Solver* s, int w) {
+  return s->lay.rset == kPow2 ? launch_k2_t<kPow2>(s, w) : launch_k2_t<kMixed>(s, w);
+}
+static cudaError_t launch_k3(const Solver* s, int w, const StopRule& rule, const Hist& h,
+                             cudaGraphConditionalHandle cond, int set_cond) {
+  return s->lay.rset == kPow2 ? launch_k3_t<kPow2>(s, w, rule, h, cond, set_cond)
+                              : launch_k3_t<kMixed>(s, w, rule, h, cond, set_cond);
+}
+
+static cudaError_t launch_iteration(const Solver* s, int it0, bool with_source, const StopRule& rule, const Hist& h,
+                                    cudaGraphConditionalHandle cond, int set_cond) {
+  const int w = it0 % s->nw;
+  cudaError_t e = launch_k1(s, w, with_source);
+  if (e != cudaSuccess) return e;
+  e = launch_k2(s, w);
+  if (e != cudaSuccess) return e;
+  return launch_k3(s, w, rule, h, cond, set_cond);
+}
+
+static int ensure_hist(Solver* s, long long cap) {
+  if (s->hist_cap >= cap) return WS_OK;
+  if (s->d_hist) cudaFree(s->d_hist);
+  s->d_hist = nullptr;
+  s->hist_cap = 0;
+  free_graph(s);  // graphs hold the old pointer
+  WS_CUDA(cudaMalloc(&s->d_hist, 2 * cap * sizeof(double)));
+  s->hist_cap = cap;
+  return WS_OK;
+}
+
+static int build_graph(Solver* s, const StopRule& rule, const Hist& h) {
+  free_graph(s);
+  cudaGraph_t graph;
+  WS_CUDA(cudaGraphCreate(&graph, 0));
+  cudaGraphConditionalHandle cond;
+  cudaError_t e = cudaGraphConditionalHandleCreate(&cond, graph, 1, cudaGraphCondAssignDefault);
+  if (e != cudaSuccess) {
+    cudaGraphDestroy(graph);
+    return fail(WS_ERR_CUDA, std::string("cudaGraphConditionalHandleCreate: ") + cudaGetErrorString(e));
+  }
+  // prologue + first cycle (with the source)
+  e = cudaStreamBeginCaptureToGraph(s->stream, graph, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal);
+  if (e == cudaSuccess) {
+    const size_t nbytes = (size_t)s->g.npts * s->g.nc * sizeof(float2);
+    cudaMemsetAsync(s->d_E, 0, nbytes, s->stream);
+    cudaMemsetAsync(s->d_dE, 0, nbytes, s->stream);
+    k_reset_state<<<1, 32, 0, s->stream>>>(s->d_state);
+    for (int i = 0; i < s->nw && e == cudaSuccess; ++i)
+      e = launch_iteration(s, i, true, rule, h, cond, i == s->nw - 1);
+    cudaGraph_t g2 = graph;
+    cudaError_t e2 = cudaStreamEndCapture(s->stream, &g2);
+    if (e == cudaSuccess) e = e2;
+  }
+  if (e != cudaSuccess) {
+    cudaGraphDestroy(graph);
+    return fail(WS_ERR_CUDA, std::string("graph capture (first cycle): ") + cudaGetErrorString(e));
+  }
+  // sink node of the captured chain
+  size_t nn = 0;
+  cudaGraphGetNodes(graph, nullptr, &nn);
+  std::vector<cudaGraphNode_t> nodes(nn);
+  cudaGraphGetNodes(graph, nodes.data(), &nn);
+  std::vector<cudaGraphNode_t> sinks;
+  for (auto n : nodes) {
+    size_t nd = 0;
+    cudaGraphNodeGetDependentNodes(n, nullptr, &nd);
+    if (nd == 0) sinks.push_back(n);
+  }
+  cudaGraphNodeParams cp{};
+  cp.type = cudaGraphNodeTypeConditional;
+  cp.conditional.handle = cond;
+  cp.conditional.type = cudaGraphCondTypeWhile;
+  cp.conditional.size = 1;
+  cudaGraphNode_t cnode;
+  e = cudaGraphAddNode(&cnode, graph, sinks.data(), sinks.size(), &cp);
+  if (e != cudaSuccess) {
+    cudaGraphDestroy(graph);
+    return fail(WS_ERR_CUDA, std::string("cudaGraphAddNode(while): ") + cudaGetErrorString(e));
+  }
+  cudaGraph_t body = cp.conditional.phGraph_out[0];
+  e = cudaStreamBeginCaptureToGraph(s->stream, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal);
+  if (e == cudaSuccess) {
+    for (int i = 0; i < s->nw && e == cudaSuccess; ++i)
+      e = launch_iteration(s, i, false, rule, h, cond, i == s->nw - 1);
+    cudaGraph_t b2 = body;
+    cudaError_t e2 = cudaStreamEndCapture(s->stream, &b2);
+    if (e == cudaSuccess) e = e2;
+  }
+  if (e != cudaSuccess) {
+    cudaGraphDestroy(graph);
+    return fail(WS_ERR_CUDA, std::string("graph capture (while body): ") + cudaGetErrorString(e));
+  }
+  e = cudaGraphInstantiate(&s->gexec, graph, 0);
+  if (e != cudaSuccess) {
+    cudaGraphDestroy(graph);
+    s->gexec = nullptr;
+    return fail(WS_ERR_CUDA, std::string("cudaGraphInstantiate: ") + cudaGetErrorString(e));
+  }
+  s->graph = graph;
+  return WS_OK;
+}
+
+static int upload_source(Solver* s, int64_t n_blocks, const ws_source_block* src, int memory, double* energy) {
+  const Geom& g = s->g;
+  const size_t nbytes = (size_t)g.npts * g.nc * sizeof(float2);
+  WS_CUDA(cudaMemsetAsync(s->d_src, 0, nbytes, s->stream));
+  WS_CUDA(cudaMemsetAsync(s->d_energy, 0, sizeof(double), s->stream));
+  size_t need = 0;
+  for (int64_t b = 0; b < n_blocks; ++b) {
+    const ws_source_block& B = src[b];
+    size_t n = 1;
+    for (int d = 0; d < 4; ++d) {
+      const int64_t lim = d == 0 ? g.ny : d == 1 ? g.nx : d == 2 ? g.nz : g.nc;
+      if (B.size[d] < 1 || B.position[d] < 1 || B.position[d] + B.size[d] - 1 > lim)
+        return fail(WS_ERR_INVALID_ARGUMENT, "source block outside the grid (crop it first, Source.m:81-103)");
+      n *= (size_t)B.size[d];
+    }
+    if (!B.values) return fail(WS_ERR_INVALID_ARGUMENT, "null source values");
+    need = std::max(need, n);
+  }
+  if (need > s->stage_cap && memory != WS_DEVICE) {
+    if (s->d_stage) cudaFree(s->d_stage);
+    s->d_stage = nullptr;
+    s->stage_cap = 0;
+    WS_CUDA(cudaMalloc(&s->d_stage, need * sizeof(float2)));
+    s->stage_cap = need;
+  }
+  for (int64_t b = 0; b < n_blocks; ++b) {
+    const ws_source_block& B = src[b];
+    const size_t n = (size_t)(B.size[0] * B.size[1] * B.size[2] * B.size[3]);
+    const float2* vals = (const float2*)B.values;
+    if (memory != WS_DEVICE) {
+      WS_CUDA(cudaMemcpyAsync(s->d_stage, B.values, n * sizeof(float2), cudaMemcpyHostToDevice, s->stream));
+      vals = s->d_stage;
+    }
+    const int th = 256;
+    const long long blocks = std::min<long long>((n + th - 1) / th, 4096);
+    k_scatter_source<<<(unsigned)std::max(1LL, blocks), th, 0, s->stream>>>(
+        s->d_src, vals, g, (int)B.position[0] - 1, (int)B.position[1] - 1, (int)B.position[2] - 1,
+        (int)B.position[3] - 1, (int)B.size[0], (int)B.size[1], (int)B.size[2], (int)B.size[3], s->d_energy);
+    WS_CUDA(cudaGetLastError());
+    if (memory != WS_DEVICE) WS_CUDA(cudaStreamSynchronize(s->stream));  // staging buffer reuse
+  }
+  WS_CUDA(cudaMemcpyAsync(energy, s->d_energy, sizeof(double), cudaMemcpyDeviceToHost, s->stream));
+  WS_CUDA(cudaStreamSynchronize(s->stream));
+  return WS_OK;
+}
+
+static int solve(Solver* s, int64_t n_blocks, const ws_source_block* src, int source_memory,
+                 const ws_solve_options* o, ws_complex* E_out, int out_memory, double* diff_out, int64_t* n_it,
+                 int* converged) {
+  WS_CUDA(cudaSetDevice(s->device));
+  ws_solve_options opt;
+  ws_default_options(&opt);
+  if (o) opt = *o;
+  if (opt.max_iterations < 1 || opt.max_iterations > 100000000LL)
+    return fail(WS_ERR_INVALID_ARGUMENT, "max_iterations must be in [1, 1e8]");
+  if (opt.energy_interval < 1) return fail(WS_ERR_INVALID_ARGUMENT, "energy_interval must be >= 1");
+  if (n_blocks < 1 || !src) return fail(WS_ERR_NO_SOURCE, "no source blocks");
+  double src_energy = 0;
+  int rc = upload_source(s, n_blocks, src, source_memory, &src_energy);
+  if (rc) return rc;
+  if (!(src_energy > 0)) return fail(WS_ERR_NO_SOURCE, "There is no source inside the grid boundaries");
+  // the loop can run at most max_iterations + Nw - 1 iterations
+  const long long cap = opt.max_iterations + s->nw;
+  rc = ensure_hist(s, cap);
+  if (rc) return rc;
+  StopRule rule{};
+  rule.nw = s->nw;
+  rule.fresh = opt.stop_rule == WS_STOP_FRESH;
+  rule.nan_stop = opt.stop_on_nonfinite ? 1 : 0;
+  rule.interval = (int)std::min<int64_t>(opt.energy_interval, 1 << 30);
+  rule.max_iter = opt.max_iterations;
+  rule.threshold = opt.energy_threshold;
+  Hist h{s->d_hist, s->d_hist + cap, cap};
+  const bool want_cb = opt.callback && opt.callback_type && std::strcmp(opt.callback_type, "NoCallback") != 0;
+  if (opt.use_graph && !want_cb) {
+    GraphKey key{rule.threshold, rule.max_iter, rule.interval, opt.stop_rule, rule.nan_stop};
+    if (!s->gexec || !(key == s->gkey)) {
+      rc = build_graph(s, rule, h);
+      if (rc) return rc;
+      s->gkey = key;
+    }
+    WS_CUDA(cudaGraphLaunch(s->gexec, s->stream));
+  } else {
+    const size_t nbytes = (size_t)s->g.npts * s->g.nc * sizeof(float2);
+    WS_CUDA(cudaMemsetAsync(s->d_E, 0, nbytes, s->stream));
+    WS_CUDA(cudaMemsetAsync(s->d_dE, 0, nbytes, s->stream));
+    k_reset_state<<<1, 32, 0, s->stream>>>(s->d_state);
+    std::vector<double> hist;
+    long long it = 0;
+    const long long cb_int = std::max<int64_t>(1, opt.callback_interval);
+    DevState hs{};
+    for (;;) {
+      for (int i = 0; i < s->nw; ++i) {
+        WS_CUDA(launch_iteration(s, (int)(it % s->nw), it < s->nw, rule, h, 0, 0));
+        ++it;
+      }
+      WS_CUDA(cudaMemcpyAsync(&hs, s->d_state, sizeof(DevState), cudaMemcpyDeviceToHost, s->stream));
+      WS_CUDA(cudaStreamSynchronize(s->stream));
+      const long long done_it = hs.it - 1;
+      if (want_cb) {
+        hist.resize(done_it);
+        WS_CUDA(cudaMemcpy(hist.data(), s->d_hist, done_it * sizeof(double), cudaMemcpyDeviceToHost));
+        for (long long k = done_it - s->nw + 1; k <= done_it; ++k)
+          if (k >= 1 && (k % cb_int == 0 || (hs.done && k == done_it)))
+            opt.callback(opt.callback_type, hist.data(), k, opt.energy_threshold, opt.user_data);
+      }
+      if (hs.done) break;
+    }
+  }
+  DevState hs{};
+  WS_CUDA(cudaMemcpyAsync(&hs, s->d_state, sizeof(DevState), cudaMemcpyDeviceToHost, s->stream));
+  WS_CUDA(cudaStreamSynchronize(s->stream));
+  const long long n_iter = hs.it - 1;
+  if (n_it) *n_it = n_iter;
+  if (converged) *converged = hs.converged;
+  if (diff_out && n_iter > 0)
+    WS_CUDA(cudaMemcpy(diff_out, s->d_hist, std::min(n_iter, cap) * sizeof(double), cudaMemcpyDeviceToHost));
+  if (E_out) {
+    const Geom& g = s->g;
+    const cudaMemcpyKind k = out_memory == WS_DEVICE ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost;
+    if (opt.output == WS_OUTPUT_FIELD) {
+      const size_t n = (size_t)(g.r1[0] - g.r0[0]) * (g.r1[1] - g.r0[1]) * (g.r1[2] - g.r0[2]) * (g.r1[3] - g.r0[3]);
+      float2* dst = (float2*)E_out;
+      if (out_memory != WS_DEVICE) {
+        if (n > s->out_cap) {
+          if (s->d_out) cudaFree(s->d_out);
+          s->d_out = nullptr;
+          s->out_cap = 0;
+          WS_CUDA(cudaMalloc(&s->d_out, n * sizeof(float2)));
+          s->out_cap = n;
+        }
+        dst = s->d_out;
+      }
+      const long long blocks = std::min<long long>(((long long)n + 255) / 256, 8 * kNumSms);
+      k_finalize<<<(unsigned)blocks, 256, 0, s->stream>>>(s->d_E, s->d_gamma, g, dst);
+      WS_CUDA(cudaGetLastError());
+      if (out_memory != WS_DEVICE) WS_CUDA(cudaMemcpyAsync(E_out, s->d_out, n * sizeof(float2), k, s->stream));
+    } else {
+      WS_CUDA(cudaMemcpyAsync(E_out, s->d_E, (size_t)g.npts * g.nc * sizeof(float2), k, s->stream));
+    }
+    WS_CUDA(cudaStreamSynchronize(s->stream));
+  }
+  if (!want_cb && opt.callback && opt.callback_type && std::strcmp(opt.callback_type, "NoCallback") != 0) {
+    // unreachable (want_cb covers it); kept for clarity of the contract
+  }
+  if (hs.status == WS_ERR_DIVERGED) return fail(WS_ERR_DIVERGED, "residual energy is not finite");
+  return WS_OK;
+}
+
+}  // namespace ws
+
+using namespace ws;
+
+extern "C" {
+
+void ws_default_options(ws_solve_options* o) {
+  if (!o) return;
+  std::memset(o, 0, sizeof(*o));
+  o->max_iterations = 100000;
+  o->energy_threshold = 1e-2;
+  o->energy_interval = 8;
+  o->stop_rule = WS_STOP_REFERENCE;
+  o->output = WS_OUTPUT_EPRIME;
+  o->stop_on_nonfinite = 1;
+  o->use_graph = 1;
+  o->callback_type = "NoCallback";
+  o->callback_interval = 50;
+}
+
+const char* ws_version(void) { return "wavesim_b200 0.1.0 (sm_100a)"; }
+
+const char* ws_last_error(void) { return g_last_error.c_str(); }
+
+int ws_size_supported(const int64_t N[4]) {
+  if (!N || (N[3] != 1 && N[3] != 3)) return 0;
+  Geom g{};
+  g.ny = (int)N[0];
+  g.nx = (int)N[1];
+  g.nz = (int)N[2];
+  g.nc = (int)N[3];
+  for (int d = 0; d < 3; ++d)
+    if (N[d] < 1 || !length_supported((int)N[d])) return 0;
+  Layout L;
+  std::string why;
+  return make_layout(g, L, why) == WS_OK;
+}
+
+int ws_solver_create(const int64_t N[4], const ws_complex* gamma, int64_t n_wiggles, const ws_wiggle* wiggles,
+                     float epsilon, ws_complex k02e, const int64_t roi[8], int memory, int device, ws_solver* out) {
+  if (!out) return fail(WS_ERR_INVALID_ARGUMENT, "null output handle");
+  *out = nullptr;
+  Solver* s = nullptr;
+  const int rc = create_solver(N, gamma, n_wiggles, wiggles, epsilon, k02e, roi, memory, device, &s);
+  if (rc) return rc;
+  *out = reinterpret_cast<ws_solver>(s);
+  return WS_OK;
+}
+
+int ws_solver_solve(ws_solver h, int64_t n_blocks, const ws_source_block* source, int source_memory,
+                    const ws_solve_options* opts, ws_complex* E_out, int out_memory, double* diff_energy_out,
+                    int64_t* n_iterations, int* converged) {
+  if (!h) return fail(WS_ERR_INVALID_ARGUMENT, "null solver");
+  return solve(reinterpret_cast<Solver*>(h), n_blocks, source, source_memory, opts, E_out, out_memory,
+               diff_energy_out, n_iterations, converged);
+}
+
+int ws_solver_buffers(ws_solver h, void** E_prime, void** stream) {
+  if (!h) return fail(WS_ERR_INVALID_ARGUMENT, "null solver");
+  Solver* s = reinterpret_cast<Solver*>(h);
+  if (E_prime) *E_prime = s->d_E;
+  if (stream) *stream = s->stream;
+  return WS_OK;
+}
+
+int ws_solver_launches_per_iteration(ws_solver h) { return h ? 3 : 0; }
+
+int ws_solver_time_kernels(ws_solver h, int n_iterations, float ms_out[3], double bytes_out[3]) {
+  if (!h || !ms_out || n_iterations < 1) return fail(WS_ERR_INVALID_ARGUMENT, "bad argument");
+  Solver* s = reinterpret_cast<Solver*>(h);
+  WS_CUDA(cudaSetDevice(s->device));
+  const long long cap = n_iterations + 1;
+  if (s->hist_cap < cap) {
+    const int rc = ensure_hist(s, cap);
+    if (rc) return rc;
+  }
+  StopRule rule{s->nw, 1, 0, 1, (long long)1 << 62, -1.0};
+  Hist hh{s->d_hist, s->d_hist + s->hist_cap, 0};  // cap 0: history untouched
+  k_resume_state<<<1, 32, 0, s->stream>>>(s->d_state);
+  float acc[3] = {0, 0, 0};
+  for (int i = 0; i < n_iterations; ++i) {
+    const int w = i % s->nw;
+    WS_CUDA(cudaEventRecord(s->ev[0], s->stream));
+    WS_CUDA(launch_k1(s, w, false));
+    WS_CUDA(cudaEventRecord(s->ev[1], s->stream));
+    WS_CUDA(launch_k2(s, w));
+    WS_CUDA(cudaEventRecord(s->ev[2], s->stream));
+    WS_CUDA(launch_k3(s, w, rule, hh, 0, 0));
+    WS_CUDA(cudaEventRecord(s->ev[3], s->stream));
+    WS_CUDA(cudaEventSynchronize(s->ev[3]));
+    float t;
+    for (int k = 0; k < 3; ++k) {
+      WS_CUDA(cudaEventElapsedTime(&t, s->ev[k], s->ev[k + 1]));
+      acc[k] += t;
+    }
+  }
+  for (int k = 0; k < 3; ++k) ms_out[k] = acc[k] / n_iterations;
+  if (bytes_out) {
+    const double n = (double)s->g.npts * s->g.nc;
+    bytes_out[0] = 16.0 * n;                                // read dE, write T
+    bytes_out[1] = 16.0 * n;                                // read T, write T
+    bytes_out[2] = 40.0 * n + 8.0 * (double)s->g.npts;      // read T, dE, E, gamma; write dE, E
+  }
+  return WS_OK;
+}
+
+int ws_solver_destroy(ws_solver h) {
+  destroy_solver(reinterpret_cast<Solver*>(h));
+  return WS_OK;
+}
+
+int ws_run_algorithm(const int64_t N[4], const ws_complex* gamma, int64_t n_wiggles, const ws_wiggle* wiggles,
+                     int64_t n_blocks, const ws_source_block* source, float epsilon, ws_complex k02e,
+                     const int64_t roi[8], int64_t max_iterations, double energy_threshold,
+                     const char* callback_string, int64_t callback_interval, ws_callback_fn callback,
+                     void* user_data, int memory, ws_complex* E_out, double* diff_energy_out,
+                     int64_t* n_iterations) {
+  int dev = 0;
+  cudaGetDevice(&dev);
+  Solver* s = nullptr;
+  int rc = create_solver(N, gamma, n_wiggles, wiggles, epsilon, k02e, roi, memory, dev, &s);
+  if (rc) return rc;
+  ws_solve_options o;
+  ws_default_options(&o);
+  o.max_iterations = max_iterations;
+  o.energy_threshold = energy_threshold;
+  o.callback_type = callback_string ? callback_string : "NoCallback";
+  o.callback_interval = callback_interval > 0 ? callback_interval : 50;
+  o.energy_interval = std::min<int64_t>(8, o.callback_interval);  // Simulation.m:135
+  o.callback = callback;
+  o.user_data = user_data;
+  rc = solve(s, n_blocks, source, memory, &o, E_out, memory, diff_energy_out, n_iterations, nullptr);
+  destroy_solver(s);
+  return rc;
+}
+
+}  // extern "C"

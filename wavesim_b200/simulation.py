@@ -1,0 +1,271 @@
+"""WaveSim / WaveSimVector: the reference's solver classes over the CUDA loop.
+
+Mirrors the MATLAB API of the reference (Simulation.m, WaveSimBase.m,
+WaveSim.m, WaveSimVector.m): construct with a refractive-index map and an
+options dict, then ``E, state = sim.exec(source)``.  Everything before the
+loop (epsilon, V, gamma, ARL filters, wiggle descriptors, ROI, source shift
+and crop) is computed here on the host exactly as the reference does; the
+loop itself (WaveSimBase.m:157-197, the part RunWaveSimAlgorithmMex replaces)
+runs in libwavesim_b200.so through ``ws_solver_solve``.
+
+Options (names as in the reference): lambda, pixel_size, boundary_widths,
+boundary_type, boundary_strength, energy_threshold, energy_calculation_interval,
+max_cycles, callback, callback_interval, roi, epsilon, ACC / wiggle,
+single_precision (must be true: the loop is complex FP32), gpu_enabled and
+usemex (accepted and ignored).  Added: ``stop_rule`` ('reference' | 'fresh'),
+``device`` (CUDA ordinal), ``max_iterations`` (overrides max_cycles),
+``use_graph``.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import math
+import time
+import warnings
+from types import SimpleNamespace
+
+import numpy as np
+
+from . import _lib
+from .problem import Medium, Source, _pad4
+
+ALPHA = 0.7  # private/f_mix.m:3
+
+
+def nuttallwin(n):
+    """Symmetric 4-term Blackman-Nuttall window (MATLAB nuttallwin)."""
+    if n == 1:
+        return np.ones(1)
+    t = 2 * np.pi * np.arange(n) / (n - 1)
+    return 0.3635819 - 0.4891775 * np.cos(t) + 0.1365995 * np.cos(2 * t) - 0.0106411 * np.cos(3 * t)
+
+
+def wiggle_perm(flags):
+    """private/wiggle_perm.m: sign combinations of the enabled directions, in
+    the column order the reference uses to limit wrap-around artefacts."""
+    flags = np.asarray(flags, dtype=bool).ravel()
+    k = int(flags.sum())
+    cols = 2 ** k
+    out = np.zeros((flags.size, cols))
+    rows = np.flatnonzero(flags)
+    for r_i, d in enumerate(rows):
+        period = 2 ** r_i
+        out[d] = [1.0 if ((c // period) % 2 == 0) else -1.0 for c in range(cols)]
+    order = {2: [0, 1, 3, 2], 3: [0, 1, 2, 4, 3, 5, 6, 7]}.get(k, list(range(cols)))
+    return out[:, order]
+
+
+class WaveSim:
+    """Scalar modified Born series (WaveSim.m + WaveSimBase.m + Simulation.m)."""
+
+    vector = False
+
+    def __init__(self, refractive_index, options):
+        o = dict(options)
+        if "wiggle" in o:  # WaveSimBase.m:48-50
+            o["ACC"] = o["wiggle"]
+        if not o.get("single_precision", True):
+            raise ValueError("the B200 loop runs in complex single precision; single_precision must be true")
+        self.options = o
+        self.lambda_ = float(o.get("lambda", 1.0))
+        self.energy_threshold = float(o.get("energy_threshold", 1e-2))
+        self.callback_interval = int(o.get("callback_interval", 50))
+        self.energy_calculation_interval = min(int(o.get("energy_calculation_interval", 8)),
+                                               self.callback_interval)  # Simulation.m:135
+        self.max_cycles = o.get("max_cycles", math.inf)
+        self.callback = o.get("callback", None)
+        self.stop_rule = o.get("stop_rule", "reference")
+        self.device = int(o.get("device", 0))
+        self.use_graph = bool(o.get("use_graph", True))
+
+        self.sample = Medium(refractive_index, o)
+        self.grid = self.sample.grid
+        self.N = np.concatenate([self.grid.N, [1]]).astype(np.int64)
+        lo = self.sample.Bl + 1
+        hi = self.grid.N - self.sample.Br
+        if o.get("roi") is None:
+            self.roi = np.stack([_pad4(lo), _pad4(hi)])
+        else:
+            r = np.asarray(o["roi"])
+            self.roi = np.stack([_pad4(r[0]), _pad4(r[1])])
+            self.roi[:, :3] += lo - 1
+
+        k0 = 2 * np.pi / self.lambda_
+        k0c = np.sqrt(self.sample.e_r_center) * k0
+        if "epsilon" in o:
+            eps = float(o["epsilon"])
+        else:  # WaveSimBase.m:201-215
+            eps = max(float(np.abs(self.sample.e_r * k0 ** 2 - k0c ** 2).max()) / 0.95, 3.0)
+        self.iterations_per_cycle = self.lambda_ / (2 * k0c / eps)
+        V = self.sample.e_r * k0 ** 2 - k0c ** 2 - 1.0j * eps
+        V = V * self._edge_filter()
+        self.gamma = (1.0j / eps * V).astype(np.complex64)
+        self.k02e = np.complex64(k0c ** 2 / eps + 1.0j)
+        self.epsilon = np.float32(eps)
+        self.k0, self.k0c = k0, k0c
+        self.wiggles, self.ACC = self._wiggles(o.get("ACC", True))
+        if self.vector:
+            if o.get("roi") is None:
+                self.roi[1, 3] = 3  # WaveSimVector.m:14-16
+            self.N[3] = 3
+        self._solver = None
+
+    # WaveSimBase.apply_edge_filters (WaveSimBase.m:217-258): separable ARL window
+    def _edge_filter(self):
+        F = np.ones(tuple(self.grid.N))
+        if self.sample.boundary_type != "ARL" or (self.sample.Bl == 0).all():
+            return F
+        bw = np.ravel(self.options["boundary_widths"])
+        linear = bool((self.grid.N > 1).all())
+        for d in range(3):
+            bl, br = int(self.sample.Bl[d]), int(self.sample.Br[d])
+            if bl <= 0:
+                continue
+            L = int(bw[d])
+            if linear:
+                win = lambda B: (np.arange(1, B + 1) - 0.21) / (B + 0.66)  # noqa: E731
+            else:
+                nw = nuttallwin(2 * L - 1)
+                win = lambda B, nw=nw: nw[:B]  # noqa: E731
+            step = np.concatenate([[0.0], win(L - 1)]) if bl == br else win(L)
+            core = int(self.grid.N[d]) - bl - br
+            f = np.concatenate([np.zeros(bl - L), step, np.ones(core), step[::-1], np.zeros(br - L)])
+            shape = [1, 1, 1]
+            shape[d] = f.size
+            F = F * f.reshape(shape)
+        return F
+
+    # WaveSimBase.compute_wiggles / wiggle_descriptor (WaveSimBase.m:272-316)
+    def _wiggles(self, acc):
+        acc = np.ravel(np.asarray(acc))
+        if acc.size == 1:
+            acc = ~self.grid.periodic if bool(acc[0]) else np.zeros(3, dtype=bool)
+        acc = acc.astype(bool)
+        g = self.grid
+        se = np.sqrt(self.epsilon)
+        out = []
+        for w in wiggle_perm(acc).T:
+            d = SimpleNamespace(wig=w)
+            d.pye = ((g.py_range - g.dpy * w[0] / 4) / se).astype(np.float32)
+            d.pxe = ((g.px_range - g.dpx * w[1] / 4) / se).astype(np.float32)
+            d.pze = ((g.pz_range - g.dpz * w[2] / 4) / se).astype(np.float32)
+            d.gy = np.exp(0.5j * np.pi * w[0] * np.arange(g.N[0]) / g.N[0]).astype(np.complex64)
+            d.gx = np.exp(0.5j * np.pi * w[1] * np.arange(g.N[1]) / g.N[1]).astype(np.complex64)
+            d.gz = np.exp(0.5j * np.pi * w[2] * np.arange(g.N[2]) / g.N[2]).astype(np.complex64)
+            out.append(d)
+        return out, acc
+
+    # ------------------------------------------------------------------ C ABI
+    def _roi8(self):
+        r = self.roi
+        return (C.c_int64 * 8)(*[int(r[i, d]) for d in range(4) for i in range(2)])
+
+    def _wiggle_structs(self):
+        self._wig_keep = []
+        arr = (_lib.ws_wiggle * len(self.wiggles))()
+        for i, w in enumerate(self.wiggles):
+            parts = [np.ascontiguousarray(a) for a in (w.pxe, w.pye, w.pze, w.gx, w.gy, w.gz)]
+            self._wig_keep.extend(parts)
+            arr[i] = _lib.ws_wiggle(*[p.ctypes.data for p in parts])
+        return arr
+
+    def solver(self):
+        """The ws_solver for this medium (created once; set-up uploaded once)."""
+        if self._solver is None:
+            N = (C.c_int64 * 4)(*[int(v) for v in self.N])
+            gamma = np.asfortranarray(self.gamma)
+            wig = self._wiggle_structs()
+            h = C.c_void_p()
+            _lib.check(_lib.lib.ws_solver_create(
+                N, gamma.ctypes.data, len(self.wiggles), wig, C.c_float(self.epsilon),
+                _lib.ws_complex(self.k02e.real, self.k02e.imag), self._roi8(), _lib.WS_HOST, self.device,
+                C.byref(h)))
+            self._solver = h
+        return self._solver
+
+    def close(self):
+        if self._solver is not None:
+            _lib.lib.ws_solver_destroy(self._solver)
+            self._solver = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def source_blocks(self, source):
+        """Simulation.exec source handling (Simulation.m:151-161): shift to the
+        ROI origin, crop to the grid, cast to complex single (column-major)."""
+        if not isinstance(source, Source):
+            raise TypeError("Expecting a Source object as input parameter")
+        s = source.shift(self.roi[0]).crop(np.ones(4, dtype=np.int64), self.N)
+        blocks = (_lib.ws_source_block * max(1, len(s.values)))()
+        keep = []
+        for i, (p, v) in enumerate(zip(s.positions, s.values)):
+            v = np.asfortranarray(v.astype(np.complex64))
+            keep.append(v)
+            blocks[i] = _lib.ws_source_block((C.c_int64 * 4)(*[int(a) for a in p]),
+                                             (C.c_int64 * 4)(*[int(a) for a in v.shape]), v.ctypes.data)
+        return s, blocks, keep
+
+    def max_iterations(self):
+        if "max_iterations" in self.options:
+            return int(self.options["max_iterations"])
+        if math.isfinite(self.max_cycles):
+            return int(math.ceil(self.max_cycles * self.iterations_per_cycle))
+        return 100000  # WaveSimBase.m:127-131
+
+    def exec(self, source):
+        """Simulation.exec (Simulation.m:138-190) with the loop on the GPU.
+        Returns (E, state): E = E'/gamma on the ROI, indexed [y, x, z] (scalar)
+        or [y, x, z, c] (vector); state.it, state.diff_energy, state.converged,
+        state.time."""
+        t0 = time.perf_counter()
+        s, blocks, keep = self.source_blocks(source)
+        state = SimpleNamespace(source=s, source_energy=s.energy())
+        if state.source_energy == 0:
+            warnings.warn("There is no source inside the grid boundaries, expect to get zero field everywhere.")
+            return None, state
+        h = self.solver()
+        o = _lib.default_options()
+        o.max_iterations = self.max_iterations()
+        o.energy_threshold = self.energy_threshold
+        o.energy_interval = self.energy_calculation_interval
+        o.stop_rule = _lib.WS_STOP_FRESH if self.stop_rule == "fresh" else _lib.WS_STOP_REFERENCE
+        o.output = _lib.WS_OUTPUT_FIELD
+        o.use_graph = 1 if self.use_graph else 0
+        cb_keep = None
+        if self.callback is not None:
+            sim = self
+
+            def _cb(kind, hist, n, thr, user):
+                sim.callback(sim, SimpleNamespace(diff_energy=np.ctypeslib.as_array(hist, (n,)).copy(),
+                                                  it=int(n), energy_threshold=thr))
+            cb_keep = _lib.CALLBACK(_cb)
+            o.callback = cb_keep
+            o.callback_type = b"Custom"
+            o.callback_interval = self.callback_interval
+        r = self.roi
+        shape = tuple(int(r[1, d] - r[0, d] + 1) for d in range(4))
+        E = np.empty(shape, dtype=np.complex64, order="F")
+        hist = np.zeros(o.max_iterations + len(self.wiggles) + 1)
+        n_it = C.c_int64()
+        conv = C.c_int()
+        _lib.check(_lib.lib.ws_solver_solve(
+            h, len(s.values), blocks, _lib.WS_HOST, C.byref(o), E.ctypes.data, _lib.WS_HOST,
+            hist.ctypes.data_as(C.POINTER(C.c_double)), C.byref(n_it), C.byref(conv)))
+        del keep, cb_keep
+        state.it = int(n_it.value) + 1  # Simulation.next leaves it one past the last iteration
+        state.diff_energy = hist[:n_it.value].copy()
+        state.converged = bool(conv.value)
+        state.time = time.perf_counter() - t0
+        if not self.vector:
+            E = E[..., 0]
+        return np.ascontiguousarray(E), state
+
+
+class WaveSimVector(WaveSim):
+    """Vector (Maxwell) MBS with the dyadic Green's function (WaveSimVector.m)."""
+
+    vector = True
