@@ -1,0 +1,388 @@
+#!/usr/bin/env python3
+"""Benchmark: time-to-tolerance of the modified Born series on a 3-D 256^3
+disordered medium (grid incl. 16-px boundary, ROI 224^3, 2000 spheres of
+n = 1.5 in n = 1.33, plane-wave source, energy_threshold 1e-3), on B200.
+
+One step = one complete solve to tolerance (the reference's stop rule,
+Simulation.m:193-217, decided on the device), inputs resident in HBM.
+``value`` is the job-level time per solve in ms (max over ranks of the
+timed region / solves done by all ranks); lower is better.  Multi-GPU runs
+are independent replicas (each rank solves its own copy), ``scaling`` weak.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+``--impl reference`` times the reference algorithm's CPU implementation (the
+FP32 restatement in oracle/, scipy.fft on all host cores) on a bounded sample
+of iterations of the same workload and projects it to the reference's
+iteration count.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import json
+import os
+import re
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "3D 256³ time-to-tol 1e-3: plain vs warm-start+batched MBS; % B200 HBM peak"
+UNIT = "ms"
+WORKLOAD = "c3: 3-D scalar 256^3 grid incl. 16-px boundary (ROI 224^3), 2000 seeded spheres n=1.5 in 1.33, " \
+           "plane wave on z=1, energy_threshold 1e-3, 8 wiggles"
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=5)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    p.add_argument("--config", default="c3", choices=["c1", "c2", "c3", "c4"])
+    p.add_argument("--cpu-iters", type=int, default=3, help="iterations in the CPU baseline sample")
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--no-e2e", action="store_true")
+    return p.parse_args()
+
+
+def dist_setup(backend):
+    import torch
+    import torch.distributed as dist
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if ws > 1:
+        from datetime import timedelta
+        dist.init_process_group(backend, timeout=timedelta(seconds=600))
+    return torch, dist, ws, rank, local
+
+
+def max_over_ranks(dist, ws, value, device=None):
+    if ws == 1:
+        return value
+    import torch
+    t = torch.tensor([value], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+class Clocks:
+    """nvidia-smi sampling during the timed region (SM clock and throttle reasons)."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.path = tempfile.mktemp(suffix=".csv")
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.f = open(self.path, "w")
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), "--query-gpu=" + self.FIELDS,
+                                          "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.f,
+                                         stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+            self.f.close()
+
+    def summary(self):
+        try:
+            rows = [r.split(",") for r in open(self.path).read().strip().splitlines() if r.strip()]
+        except Exception:
+            rows = []
+        rows = [[c.strip() for c in r] for r in rows if len(r) >= 9]
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].lower() == "active"})
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+def measured_peaks():
+    try:
+        return json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json"))), "measured"
+    except Exception:
+        return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0}, "fallback"
+
+
+def profile_traffic(kernel):
+    """DRAM bytes per launch of `kernel` on this workload from the committed ncu
+    summary (profiles/*.md, line 'dram_bytes_per_launch[<kernel>]: N')."""
+    pdir = os.path.join(ROOT, "profiles")
+    if not os.path.isdir(pdir):
+        return None
+    for f in sorted(os.listdir(pdir)):
+        if not f.endswith((".md", ".txt")):
+            continue
+        m = re.search(r"dram_bytes_per_launch\[%s\]:\s*([0-9.eE+]+)" % re.escape(kernel),
+                      open(os.path.join(pdir, f)).read())
+        if m:
+            return float(m.group(1))
+    return None
+
+
+def build_problem(config):
+    from wavesim_b200 import workloads
+    import wavesim_b200 as ws
+    n, opt, val, pos, vector = workloads.CONFIGS[config]()
+    t = time.time()
+    sim = (ws.WaveSimVector if vector else ws.WaveSim)(n, opt)
+    return sim, ws.Source(val, pos), time.time() - t, (n, opt, val, pos, vector)
+
+
+def reference_iterations():
+    try:
+        return json.load(open(os.path.join(ROOT, "tests", "golden", "c3_reference_run.json")))["iterations"]
+    except Exception:
+        return None
+
+
+def cpu_sample(spec, iters):
+    """The FP32 restatement of the reference loop (oracle/) timed for `iters`
+    iterations on all host cores; returns ms per iteration."""
+    from oracle import mbs_oracle as ref
+    n, opt, val, pos, vector = spec
+    sim = (ref.WaveSimVector if vector else ref.WaveSim)(n, dict(opt, single_precision=True))
+    src = ref.Source(val, pos)
+    t = time.perf_counter()
+    sim.exec(src, max_iterations=iters)
+    dt = time.perf_counter() - t
+    nw = len(sim.wiggles)
+    done = ((iters + nw - 1) // nw) * nw  # the loop ends on a multiple of Nw
+    return 1e3 * dt / done, done
+
+
+def run_reference(args):
+    torch, dist, ws, rank, local = dist_setup("gloo")
+    if rank != 0:
+        if ws > 1:
+            dist.barrier()
+            dist.destroy_process_group()
+        return
+    _, _, _, spec = build_problem(args.config)
+    iters_tol = reference_iterations() if args.config == "c3" else None
+    samples = []
+    for i in range(args.warmup + args.steps):
+        ms_it, done = cpu_sample(spec, 1)
+        if i >= args.warmup:
+            samples.append(ms_it)
+    ms_it = float(np.mean(samples))
+    value = ms_it * iters_tol if iters_tol else None
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": value, "higher_is_better": False,
+        "scaling": "weak", "vs_baseline": None, "dtype": "c64 (fp32 complex)", "data": "synthetic (seeded)",
+        "config": {"workload": WORKLOAD if args.config == "c3" else args.config},
+        "ms_per_iteration": ms_it, "iterations_to_tol": iters_tol,
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": os.cpu_count(), "kind": "port",
+                         "sample": f"{args.steps} steps of one MBS iteration each (rounded up to a multiple of "
+                                   f"Nw by the reference stop rule) of the 256^3 workload, FP32 scipy.fft "
+                                   f"restatement on {os.cpu_count()} threads, projected to the reference's "
+                                   f"{iters_tol} iterations to tolerance"},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    if ws > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def run_ours(args):
+    torch, dist, ws, rank, local = dist_setup("nccl")
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    from wavesim_b200 import _lib
+    sim, source, setup_s, spec = build_problem(args.config)
+    sim.device = local
+    h = sim.solver()
+    stream_ptr = C.c_void_p()
+    _lib.check(_lib.lib.ws_solver_buffers(h, None, C.byref(stream_ptr)))
+    stream = torch.cuda.ExternalStream(stream_ptr.value, device=dev)
+
+    # device-resident source blocks and output
+    s, blocks, keep = sim.source_blocks(source)
+    dev_vals = []
+    for i, v in enumerate(keep):
+        t = torch.from_numpy(np.ascontiguousarray(v.ravel(order="F")).view(np.float32)).to(dev)
+        dev_vals.append(t)
+        blocks[i].values = t.data_ptr()
+    r = sim.roi
+    out_n = int(np.prod([r[1, d] - r[0, d] + 1 for d in range(4)]))
+    E_dev = torch.empty(out_n * 2, dtype=torch.float32, device=dev)
+    opts = _lib.default_options()
+    opts.max_iterations = sim.max_iterations()
+    opts.energy_threshold = sim.energy_threshold
+    opts.energy_interval = sim.energy_calculation_interval
+    opts.output = _lib.WS_OUTPUT_FIELD
+    n_it = C.c_int64()
+    conv = C.c_int()
+
+    def solve():
+        _lib.check(_lib.lib.ws_solver_solve(h, len(s.values), blocks, _lib.WS_DEVICE, C.byref(opts),
+                                            E_dev.data_ptr(), _lib.WS_DEVICE, None, C.byref(n_it), C.byref(conv)))
+
+    for _ in range(args.warmup):
+        solve()
+    torch.cuda.synchronize()
+    if ws > 1:
+        dist.barrier()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    iters = []
+    with Clocks(local) as clk:
+        torch.cuda.synchronize()
+        ev0.record(stream)
+        for _ in range(args.steps):
+            solve()
+            iters.append(int(n_it.value))
+        ev1.record(stream)
+        ev1.synchronize()
+        torch.cuda.synchronize()
+    local_ms = ev0.elapsed_time(ev1)
+    if ws > 1:
+        dist.barrier()
+    total_ms = max_over_ranks(dist, ws, local_ms, dev)
+    ms_per_solve_gpu = local_ms / args.steps
+    value = total_ms / (args.steps * ws)
+    n_iter = iters[-1]
+    launches_per_solve = 3 * n_iter + (n_iter // len(sim.wiggles)) + 1 + len(s.values) + 1
+
+    # per-kernel device time (CUDA events on the solver's stream) -> roofline
+    ms3 = (C.c_float * 3)()
+    by3 = (C.c_double * 3)()
+    _lib.check(_lib.lib.ws_solver_time_kernels(h, 24, ms3, by3))
+    names = ["k_fwd_inner", "k_outer", "k_inv_inner"]
+    peaks, peak_kind = measured_peaks()
+    peak = float(peaks.get("hbm_gbs", 6650.0))
+    kern = []
+    for i in range(3):
+        gbs = by3[i] / (ms3[i] * 1e-3) / 1e9
+        kern.append({"kernel": names[i], "ms": ms3[i], "algorithmic_bytes": by3[i], "achieved_gbs": gbs,
+                     "frac": gbs / peak})
+    dom = max(kern, key=lambda k: k["ms"])
+    iter_ms = sum(ms3)
+    bytes_iter = sum(by3)
+
+    # e2e: the reference-facing one-shot call (ws_run_algorithm, the MEX
+    # argument list) with host buffers: set-up upload, solve, E' download
+    e2e = None
+    if not args.no_e2e:
+        e2e = run_e2e(args, sim, s, keep, torch, dev)
+        if ws > 1:
+            e2e["value"] = max_over_ranks(dist, ws, e2e["value"] * args.steps, dev) / (args.steps * ws)
+
+    cpu = None
+    if rank == 0 and ws == 1 and not args.no_cpu_baseline:
+        ms_it, done = cpu_sample(spec, args.cpu_iters)
+        cpu = {"value": ms_it * n_iter, "unit": UNIT, "cores": os.cpu_count(), "kind": "port",
+               "sample": f"{done} MBS iterations of the same 256^3 workload with the FP32 restatement of the "
+                         f"reference loop (oracle/, scipy.fft, {os.cpu_count()} threads): "
+                         f"{ms_it:.1f} ms/iteration, projected to the {n_iter} iterations to tolerance"}
+
+    if rank == 0:
+        ref_it = reference_iterations() if args.config == "c3" else None
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": value, "higher_is_better": False, "scaling": "weak",
+            "vs_baseline": None, "dtype": "c64 (fp32 complex)", "data": "synthetic (seeded)",
+            "config": {"workload": WORKLOAD if args.config == "c3" else args.config,
+                       "grid": [int(v) for v in sim.N], "stop_rule": "reference (Simulation.next), on device",
+                       "l2": "inputs larger than L2 (each 256^3 c64 array is 134 MB > 126 MB L2)",
+                       "parallelism": f"replicas x{ws}"},
+            "iterations_to_tol": n_iter, "reference_iterations_to_tol": ref_it, "converged": bool(conv.value),
+            "ms_per_solve_per_gpu": ms_per_solve_gpu, "ms_per_iteration": ms_per_solve_gpu / n_iter,
+            "iterations_per_s": n_iter / (ms_per_solve_gpu * 1e-3) * ws,
+            "effective_hbm_gbs_per_iteration": bytes_iter / (ms_per_solve_gpu / n_iter * 1e-3) / 1e9,
+            "kernels": kern,
+            "roofline": {"bound": "hbm", "kernel": dom["kernel"], "achieved": dom["achieved_gbs"], "peak": peak,
+                         "peak_kind": peak_kind, "unit": "GB/s", "frac": dom["achieved_gbs"] / peak,
+                         "traffic": profile_traffic(dom["kernel"]),
+                         "algorithmic_bytes_per_launch": dom["algorithmic_bytes"]},
+            "e2e": e2e, "gpu_launches": launches_per_solve * args.steps, "cpu_baseline": cpu,
+            "clocks": clk.summary(), "host_setup_s": setup_s,
+        }
+        print(json.dumps(line), flush=True)
+    sim.close()
+    if ws > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def run_e2e(args, sim, s, keep, torch, dev):
+    """ws_run_algorithm on pinned host buffers: H2D of gamma, wiggles and source,
+    the solve, D2H of E' and the energy history, every step."""
+    from wavesim_b200 import _lib
+    pin = lambda a: torch.from_numpy(np.ascontiguousarray(a)).pin_memory().numpy()  # noqa: E731
+    gamma = pin(np.asfortranarray(sim.gamma).ravel(order="F"))
+    wkeep = []
+    wig = (_lib.ws_wiggle * len(sim.wiggles))()
+    for i, w in enumerate(sim.wiggles):
+        parts = [pin(a) for a in (w.pxe, w.pye, w.pze, w.gx, w.gy, w.gz)]
+        wkeep.extend(parts)
+        wig[i] = _lib.ws_wiggle(*[p.ctypes.data for p in parts])
+    blocks = (_lib.ws_source_block * len(keep))()
+    vkeep = []
+    for i, (p, v) in enumerate(zip(s.positions, keep)):
+        pv = pin(np.asfortranarray(v).ravel(order="F"))
+        vkeep.append(pv)
+        blocks[i] = _lib.ws_source_block((C.c_int64 * 4)(*[int(a) for a in p]),
+                                         (C.c_int64 * 4)(*[int(a) for a in v.shape]), pv.ctypes.data)
+    npts_c = int(np.prod(sim.N))
+    E = pin(np.zeros(npts_c, np.complex64))
+    maxit = sim.max_iterations()
+    hist = pin(np.zeros(maxit + 64))
+    N = (C.c_int64 * 4)(*[int(v) for v in sim.N])
+    n_it = C.c_int64()
+
+    def call():
+        _lib.check(_lib.lib.ws_run_algorithm(
+            N, gamma.ctypes.data, len(sim.wiggles), wig, len(keep), blocks, C.c_float(sim.epsilon),
+            _lib.ws_complex(sim.k02e.real, sim.k02e.imag), sim._roi8(), maxit, sim.energy_threshold,
+            b"NoCallback", sim.callback_interval, _lib.CALLBACK(), None, _lib.WS_HOST, E.ctypes.data,
+            hist.ctypes.data_as(C.POINTER(C.c_double)), C.byref(n_it)))
+
+    call()
+    torch.cuda.synchronize()
+    t = time.perf_counter()
+    for _ in range(args.steps):
+        call()
+    torch.cuda.synchronize()
+    ms = (time.perf_counter() - t) * 1e3 / args.steps
+    h2d = gamma.nbytes + sum(a.nbytes for a in wkeep) + sum(a.nbytes for a in vkeep)
+    d2h = E.nbytes + 8 * int(n_it.value)
+    return {"value": ms, "unit": UNIT, "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
+            "api": "ws_run_algorithm (RunWaveSimAlgorithmMex argument list), host pinned buffers, "
+                   "host wall clock around the blocking call"}
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -58,7 +58,7 @@ struct DevState {
   int calc_energy;  // state.calculate_energy
   int status;       // 0 or WS_ERR_DIVERGED
   unsigned int blocks_done;
-  int pad0, pad1;
+  long long cycles;  // wiggle cycles completed (loop guard)
   double e_acc;             // partial sums of this iteration's ROI energy
   double last_step_energy;  // state.last_step_energy
   double diff1;             // state.diff_energy(1)
@@ -268,8 +268,7 @@ __global__ void __launch_bounds__(512, 1) k_outer(OuterArgs a, float2* __restric
 
 // Simulation.next (Simulation.m:193-217), run by one thread after the energy
 // of iteration st->it is complete.
-__device__ __forceinline__ void finish_iteration(DevState* st, const StopRule& rule, const Hist& h,
-                                                 cudaGraphConditionalHandle cond, int set_cond) {
+__device__ __forceinline__ void finish_iteration(DevState* st, const StopRule& rule, const Hist& h) {
   const double e = atomicAdd(&st->e_acc, 0.0);
   st->e_acc = 0.0;
   const int it = st->it;
@@ -295,19 +294,14 @@ __device__ __forceinline__ void finish_iteration(DevState* st, const StopRule& r
   st->it = it + 1;
   st->blocks_done = 0;
   __threadfence();
-  if (set_cond) cudaGraphSetConditional(cond, st->done ? 0u : 1u);
 }
 
 // K3 -------------------------------------------------------------------------
 template <int EMAX, int RSET>
 __global__ void __launch_bounds__(512, 1) k_inv_inner(InnerArgs a, const float2* __restrict__ T, float2* __restrict__ dE,
                                                     float2* __restrict__ E, const float2* __restrict__ gamma,
-                                                    DevState* st, StopRule rule, Hist h,
-                                                    cudaGraphConditionalHandle cond, int set_cond) {
-  if (load_done(st)) {
-    if (set_cond && blockIdx.x == 0 && threadIdx.x == 0) cudaGraphSetConditional(cond, 0u);
-    return;
-  }
+                                                    DevState* st, StopRule rule, Hist h) {
+  if (load_done(st)) return;
   extern __shared__ float2 sm[];
   __shared__ float red[32];
   __shared__ unsigned int ticket;
@@ -394,7 +388,7 @@ __global__ void __launch_bounds__(512, 1) k_inv_inner(InnerArgs a, const float2*
   __syncthreads();
   if (tid == 0 && ticket == gridDim.x - 1) {
     __threadfence();
-    finish_iteration(st, rule, h, cond, set_cond);
+    finish_iteration(st, rule, h);
   }
 }
 
@@ -407,9 +401,22 @@ __global__ void k_reset_state(DevState* st) {
     st->calc_energy = 1;
     st->status = 0;
     st->blocks_done = 0;
+    st->cycles = 0;
     st->e_acc = 0.0;
     st->last_step_energy = __longlong_as_double(0x7ff0000000000000LL);  // inf (Simulation.m:169)
     st->diff1 = 0.0;
+  }
+}
+
+// Runs after each wiggle cycle of the graph: continues the device-side while
+// loop only if the stop rule has not fired and fewer than max_cycles cycles
+// have run, so the loop ends even if the stop logic were never reached.
+__global__ void k_cycle_guard(DevState* st, cudaGraphConditionalHandle cond, long long max_cycles) {
+  if (threadIdx.x == 0 && blockIdx.x == 0) {
+    const long long c = ++st->cycles;
+    const bool go = !st->done && c < max_cycles;
+    if (!go) st->done = 1;
+    cudaGraphSetConditional(cond, go ? 1u : 0u);
   }
 }
 

@@ -235,13 +235,20 @@ static void push_twiddles(std::vector<float2>& all, int n, size_t& off) {
   }
 }
 
+template <typename K>
+static cudaError_t allow_dynamic_smem(K kernel, int optin) {
+  cudaFuncAttributes fa{};
+  cudaError_t e = cudaFuncGetAttributes(&fa, kernel);
+  if (e != cudaSuccess) return e;
+  return cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, optin - (int)fa.sharedSizeBytes);
+}
+
 template <int RS>
-static cudaError_t set_attributes_for() {
-  const int maxsm = 227 * 1024;
+static cudaError_t set_attributes_for(int optin) {
   cudaError_t e;
-  if ((e = cudaFuncSetAttribute(k_fwd_inner<kEmax, RS>, cudaFuncAttributeMaxDynamicSharedMemorySize, maxsm))) return e;
-  if ((e = cudaFuncSetAttribute(k_inv_inner<kEmax, RS>, cudaFuncAttributeMaxDynamicSharedMemorySize, maxsm))) return e;
-  if ((e = cudaFuncSetAttribute(k_outer<kEmax, RS>, cudaFuncAttributeMaxDynamicSharedMemorySize, maxsm))) return e;
+  if ((e = allow_dynamic_smem(k_fwd_inner<kEmax, RS>, optin))) return e;
+  if ((e = allow_dynamic_smem(k_inv_inner<kEmax, RS>, optin))) return e;
+  if ((e = allow_dynamic_smem(k_outer<kEmax, RS>, optin))) return e;
   if ((e = cudaFuncSetAttribute(k_fwd_inner<kEmax, RS>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1))) return e;
   return cudaFuncSetAttribute(k_inv_inner<kEmax, RS>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
 }
@@ -252,8 +259,10 @@ static int set_kernel_attributes() {
   int dev = 0;
   WS_CUDA(cudaGetDevice(&dev));
   if (dev < 31 && (done_mask >> dev) & 1) return WS_OK;
-  WS_CUDA(set_attributes_for<kPow2>());
-  WS_CUDA(set_attributes_for<kMixed>());
+  int optin = 0;
+  WS_CUDA(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+  WS_CUDA(set_attributes_for<kPow2>(optin));
+  WS_CUDA(set_attributes_for<kMixed>(optin));
   if (dev < 31) done_mask |= 1 << dev;
   return WS_OK;
 }
@@ -430,8 +439,7 @@ static cudaError_t launch_k2_t(const Solver* s, int w) {
 }
 
 template <int RS>
-static cudaError_t launch_k3_t(const Solver* s, int w, const StopRule& rule, const Hist& h,
-                               cudaGraphConditionalHandle cond, int set_cond) {
+static cudaError_t launch_k3_t(const Solver* s, int w, const StopRule& rule, const Hist& h) {
   cudaLaunchConfig_t cfg{};
   cfg.gridDim = dim3((unsigned)s->lay.grid_inner);
   cfg.blockDim = dim3(s->lay.th_inner);
@@ -445,7 +453,7 @@ static cudaError_t launch_k3_t(const Solver* s, int w, const StopRule& rule, con
   cfg.attrs = attr;
   cfg.numAttrs = 1;
   return cudaLaunchKernelEx(&cfg, k_inv_inner<kEmax, RS>, inner_args(s, w), (const float2*)s->d_T, s->d_dE,
-                            s->d_E, (const float2*)s->d_gamma, s->d_state, rule, h, cond, set_cond);
+                            s->d_E, (const float2*)s->d_gamma, s->d_state, rule, h);
 }
 
 static cudaError_t launch_k1(const Solver* s, int w, bool with_source) {
@@ -454,20 +462,18 @@ static cudaError_t launch_k1(const Solver* s, int w, bool with_source) {
 static cudaError_t launch_k2(const Solver* s, int w) {
   return s->lay.rset == kPow2 ? launch_k2_t<kPow2>(s, w) : launch_k2_t<kMixed>(s, w);
 }
-static cudaError_t launch_k3(const Solver* s, int w, const StopRule& rule, const Hist& h,
-                             cudaGraphConditionalHandle cond, int set_cond) {
-  return s->lay.rset == kPow2 ? launch_k3_t<kPow2>(s, w, rule, h, cond, set_cond)
-                              : launch_k3_t<kMixed>(s, w, rule, h, cond, set_cond);
+static cudaError_t launch_k3(const Solver* s, int w, const StopRule& rule, const Hist& h) {
+  return s->lay.rset == kPow2 ? launch_k3_t<kPow2>(s, w, rule, h) : launch_k3_t<kMixed>(s, w, rule, h);
 }
 
-static cudaError_t launch_iteration(const Solver* s, int it0, bool with_source, const StopRule& rule, const Hist& h,
-                                    cudaGraphConditionalHandle cond, int set_cond) {
+static cudaError_t launch_iteration(const Solver* s, int it0, bool with_source, const StopRule& rule,
+                                    const Hist& h) {
   const int w = it0 % s->nw;
   cudaError_t e = launch_k1(s, w, with_source);
   if (e != cudaSuccess) return e;
   e = launch_k2(s, w);
   if (e != cudaSuccess) return e;
-  return launch_k3(s, w, rule, h, cond, set_cond);
+  return launch_k3(s, w, rule, h);
 }
 
 static int ensure_hist(Solver* s, long long cap) {
@@ -483,6 +489,9 @@ static int ensure_hist(Solver* s, long long cap) {
 
 static int build_graph(Solver* s, const StopRule& rule, const Hist& h) {
   free_graph(s);
+  // the stop rule can only end the loop at a multiple of Nw, at the latest at
+  // the first multiple >= max_iter: this many cycles always suffice
+  const long long max_cycles = (rule.max_iter + s->nw - 1) / s->nw + 1;
   cudaGraph_t graph;
   WS_CUDA(cudaGraphCreate(&graph, 0));
   cudaGraphConditionalHandle cond;
@@ -498,8 +507,11 @@ static int build_graph(Solver* s, const StopRule& rule, const Hist& h) {
     cudaMemsetAsync(s->d_E, 0, nbytes, s->stream);
     cudaMemsetAsync(s->d_dE, 0, nbytes, s->stream);
     k_reset_state<<<1, 32, 0, s->stream>>>(s->d_state);
-    for (int i = 0; i < s->nw && e == cudaSuccess; ++i)
-      e = launch_iteration(s, i, true, rule, h, cond, i == s->nw - 1);
+    for (int i = 0; i < s->nw && e == cudaSuccess; ++i) e = launch_iteration(s, i, true, rule, h);
+    if (e == cudaSuccess) {
+      k_cycle_guard<<<1, 32, 0, s->stream>>>(s->d_state, cond, max_cycles);
+      e = cudaGetLastError();
+    }
     cudaGraph_t g2 = graph;
     cudaError_t e2 = cudaStreamEndCapture(s->stream, &g2);
     if (e == cudaSuccess) e = e2;
@@ -533,8 +545,11 @@ static int build_graph(Solver* s, const StopRule& rule, const Hist& h) {
   cudaGraph_t body = cp.conditional.phGraph_out[0];
   e = cudaStreamBeginCaptureToGraph(s->stream, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal);
   if (e == cudaSuccess) {
-    for (int i = 0; i < s->nw && e == cudaSuccess; ++i)
-      e = launch_iteration(s, i, false, rule, h, cond, i == s->nw - 1);
+    for (int i = 0; i < s->nw && e == cudaSuccess; ++i) e = launch_iteration(s, i, false, rule, h);
+    if (e == cudaSuccess) {
+      k_cycle_guard<<<1, 32, 0, s->stream>>>(s->d_state, cond, max_cycles);
+      e = cudaGetLastError();
+    }
     cudaGraph_t b2 = body;
     cudaError_t e2 = cudaStreamEndCapture(s->stream, &b2);
     if (e == cudaSuccess) e = e2;
@@ -644,9 +659,11 @@ static int solve(Solver* s, int64_t n_blocks, const ws_source_block* src, int so
     long long it = 0;
     const long long cb_int = std::max<int64_t>(1, opt.callback_interval);
     DevState hs{};
-    for (;;) {
+    const long long max_cycles = (rule.max_iter + s->nw - 1) / s->nw + 1;
+    for (long long cycle = 0;; ++cycle) {
+      if (cycle >= max_cycles) return fail(WS_ERR_CUDA, "loop did not stop within max_iterations (internal error)");
       for (int i = 0; i < s->nw; ++i) {
-        WS_CUDA(launch_iteration(s, (int)(it % s->nw), it < s->nw, rule, h, 0, 0));
+        WS_CUDA(launch_iteration(s, (int)(it % s->nw), it < s->nw, rule, h));
         ++it;
       }
       WS_CUDA(cudaMemcpyAsync(&hs, s->d_state, sizeof(DevState), cudaMemcpyDeviceToHost, s->stream));
@@ -789,7 +806,7 @@ int ws_solver_time_kernels(ws_solver h, int n_iterations, float ms_out[3], doubl
     WS_CUDA(cudaEventRecord(s->ev[1], s->stream));
     WS_CUDA(launch_k2(s, w));
     WS_CUDA(cudaEventRecord(s->ev[2], s->stream));
-    WS_CUDA(launch_k3(s, w, rule, hh, 0, 0));
+    WS_CUDA(launch_k3(s, w, rule, hh));
     WS_CUDA(cudaEventRecord(s->ev[3], s->stream));
     WS_CUDA(cudaEventSynchronize(s->ev[3]));
     float t;
