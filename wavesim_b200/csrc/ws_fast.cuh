@@ -1,0 +1,442 @@
+// Power-of-two fast path of the fused MBS kernels.
+//
+// Every thread owns 16 elements of one line of length N at a time, so a line
+// has P = N/16 threads, and the radix schedule is fixed at compile time:
+//   N = 16:          [16]
+//   N = 32 ... 256:  [16, N/16]
+//   N = 512 ... 4096:[16, 16, N/256]
+// Thread p enters with v[r] = x[p + P r] (its first-stage inputs, loaded
+// straight from global memory when the line is contiguous there) and leaves
+// with v[m] = X[p + P m]: the same index set, so a forward transform, a
+// pointwise multiply and an inverse transform chain in registers.  Only the
+// exchanges between stages touch shared memory (one write and one read per
+// element for N <= 256).  All index arithmetic is shifts and masks.
+//
+// Kernels (scalar or per-component planes, layout of the generic path):
+//   kf_plane_fwd<N, C, DO_X>  K1: (y, x) planes of N x N (3-D, DO_X) or
+//                              columns of length N (2-D); for C > 1 a plane is
+//                              split over a cluster of C blocks and the x
+//                              transform follows a DSMEM transpose (each
+//                              element crosses once).
+//   kf_pencil<NO, TY>         K2: outer-dimension pencils, Green's function.
+//   kf_plane_inv<N, C, DO_X>  K3: inverse of K1 + unwiggle, mix, accumulate,
+//                              ROI energy, stop rule.
+#pragma once
+#include "ws_kernels.cuh"
+
+namespace ws {
+namespace fast {
+
+constexpr int kThreads = 256;
+
+__host__ __device__ constexpr int ipow16(int e) { return e == 0 ? 1 : 16 * ipow16(e - 1); }
+
+template <int N>
+struct LinePlan {
+  static_assert(N >= 16 && N <= 4096 && (N & (N - 1)) == 0, "power-of-two line of 16..4096");
+  static constexpr int P = N / 16;
+  static constexpr int NST = N <= 16 ? 1 : (N <= 256 ? 2 : 3);
+  __host__ __device__ static constexpr int radix(int s) { return s < NST - 1 ? 16 : N / ipow16(NST - 1); }
+  __host__ __device__ static constexpr int span(int s) { return ipow16(s); }
+};
+
+// line element i at base[i + i/16] (contiguous, padded)
+struct ColLine {
+  float2* base;
+  __device__ __forceinline__ float2& at(int i) const { return base[i + (i >> 4)]; }
+};
+// line element i at base[i * stride] (interleaved lines)
+struct RowLine {
+  float2* base;
+  int stride;
+  __device__ __forceinline__ float2& at(int i) const { return base[i * stride]; }
+};
+
+struct SyncWarp {
+  __device__ __forceinline__ void operator()() const { __syncwarp(); }
+};
+struct SyncBlock {
+  __device__ __forceinline__ void operator()() const { __syncthreads(); }
+};
+
+template <int R, bool INV>
+__device__ __forceinline__ void dft_slice(float2 (&v)[16], int off) {
+  float2 u[R];
+#pragma unroll
+  for (int r = 0; r < R; ++r) u[r] = v[off + r];
+  Dft<R, INV>::run(u);
+#pragma unroll
+  for (int r = 0; r < R; ++r) v[off + r] = u[r];
+}
+
+template <int N, bool INV, int S, class Line, class Sync>
+__device__ __forceinline__ void line_stage(float2 (&v)[16], const Line& L, int p, const float2* __restrict__ tw,
+                                           Sync sync) {
+  using PL = LinePlan<N>;
+  constexpr int R = PL::radix(S), Ns = PL::span(S), B = 16 / R, P = PL::P, NR = N / R;
+  constexpr int TS = N / (Ns * R);
+  if constexpr (S > 0) {
+#pragma unroll
+    for (int q = 0; q < B; ++q) {
+      const int j = p + P * q;
+#pragma unroll
+      for (int r = 0; r < R; ++r) v[q * R + r] = L.at(j + r * NR);
+      const int jm = j & (Ns - 1);
+#pragma unroll
+      for (int r = 1; r < R; ++r) {
+        float2 w = __ldg(&tw[jm * r * TS]);
+        if (INV) w.y = -w.y;
+        v[q * R + r] = cmul(v[q * R + r], w);
+      }
+    }
+  }
+#pragma unroll
+  for (int q = 0; q < B; ++q) dft_slice<R, INV>(v, q * R);
+  if constexpr (S < PL::NST - 1) {
+    sync();
+#pragma unroll
+    for (int q = 0; q < B; ++q) {
+      const int j = p + P * q;
+      const int jm = j & (Ns - 1);
+      const int base = (j - jm) * R + jm;
+#pragma unroll
+      for (int r = 0; r < R; ++r) L.at(base + r * Ns) = v[q * R + r];
+    }
+    sync();
+  } else if constexpr (B > 1) {
+    float2 t[16];
+#pragma unroll
+    for (int q = 0; q < B; ++q)
+#pragma unroll
+      for (int r = 0; r < R; ++r) t[q + B * r] = v[q * R + r];
+#pragma unroll
+    for (int m = 0; m < 16; ++m) v[m] = t[m];
+  }
+}
+
+// In: v[r] = x[p + P r].  Out: v[m] = X[p + P m] (unnormalised; INV: sign +1).
+template <int N, bool INV, class Line, class Sync>
+__device__ __forceinline__ void line_fft(float2 (&v)[16], const Line& L, int p, const float2* __restrict__ tw,
+                                         Sync sync) {
+  line_stage<N, INV, 0>(v, L, p, tw, sync);
+  if constexpr (LinePlan<N>::NST > 1) line_stage<N, INV, 1>(v, L, p, tw, sync);
+  if constexpr (LinePlan<N>::NST > 2) line_stage<N, INV, 2>(v, L, p, tw, sync);
+}
+
+// shared-memory tile geometry of the plane kernels
+template <int N, int C, bool DO_X>
+struct PlaneGeom {
+  static constexpr int M = DO_X ? N / C : 0;   // columns held in phase A (2-D: a.ncols at run time)
+  static constexpr int CS = N + N / 16 + 1;    // padded column stride (odd: row access conflict free)
+  static constexpr int LR = N / C;             // rows held in the x phase (C > 1)
+  static constexpr int CS2 = LR + LR / 16 + 1; // column stride of the transposed tile
+  static constexpr int P = N / 16;
+  static constexpr int LPR = kThreads / P;     // lines per round
+  static constexpr size_t smem_a = (size_t)(M + 1) * CS * sizeof(float2);  // + scratch column
+  static constexpr size_t smem_b = (size_t)N * CS2 * sizeof(float2);
+  static constexpr size_t smem = (C > 1 && DO_X) ? (smem_a > smem_b ? smem_a : smem_b) : smem_a;
+  static_assert(kThreads % P == 0 || P > kThreads, "threads per line");
+};
+
+// ----------------------------------------------------------------------------
+// K1
+// ----------------------------------------------------------------------------
+template <int N, int C, bool DO_X>
+__global__ void __launch_bounds__(kThreads, 2)
+    kf_plane_fwd(InnerArgs a, const float2* __restrict__ dE, const float2* __restrict__ src, float2 A,
+                 float2* __restrict__ T, const DevState* __restrict__ st) {
+  using G = PlaneGeom<N, C, DO_X>;
+  constexpr int P = G::P, LPR = G::LPR;
+  if (load_done(st)) return;
+  extern __shared__ float2 sm[];
+  const int tid = threadIdx.x;
+  const Geom& g = a.g;
+  const int nx = g.nx;
+  const int M = DO_X ? G::M : a.ncols;  // scratch column for idle lanes: index M
+  int rank = 0, plane = 0, x0 = 0, z = 0, ncol;
+  long long colbase;
+  if constexpr (DO_X) {
+    rank = C > 1 ? (int)(blockIdx.x % C) : 0;
+    plane = blockIdx.x / C;
+    x0 = rank * M;
+    z = plane % g.nz;
+    colbase = (long long)plane * nx + x0;
+    ncol = M;
+  } else {
+    colbase = (long long)blockIdx.x * M;
+    ncol = (int)min((long long)M, (long long)nx * g.nc - colbase);
+  }
+  const float2 gzz = a.w.gz[z];
+  // phase A: y transform of each held column, straight from global memory
+  for (int c0 = 0; c0 < ncol; c0 += LPR) {
+    const int cl = c0 + tid / P, p = tid % P;
+    const bool live = cl < ncol;
+    float2 v[16];
+    if (live) {
+      const long long col = colbase + cl;
+      const int x = DO_X ? x0 + cl : (int)(col % nx);
+      const float2 gxz = cmul(a.w.gx[x], gzz);
+      const float2* __restrict__ s = dE + col * N;
+      const float2* __restrict__ sr = src ? src + col * N : nullptr;
+#pragma unroll
+      for (int r = 0; r < 16; ++r) {
+        const int y = p + P * r;
+        float2 e = s[y];
+        if (sr) e = cadd(e, cmul(A, sr[y]));
+        v[r] = cmul(cmul(e, gxz), a.w.gy[y]);
+      }
+    } else {
+#pragma unroll
+      for (int r = 0; r < 16; ++r) v[r] = make_float2(0.f, 0.f);
+    }
+    ColLine L{sm + (live ? cl : M) * G::CS};
+    if constexpr (P <= 32) {
+      line_fft<N, false>(v, L, p, a.py.tw, SyncWarp{});
+    } else {
+      line_fft<N, false>(v, L, p, a.py.tw, SyncBlock{});
+    }
+    if constexpr (DO_X) {
+#pragma unroll
+      for (int m = 0; m < 16; ++m) L.at(p + P * m) = v[m];
+    } else if (live) {
+      float2* __restrict__ d = T + (colbase + cl) * N;
+#pragma unroll
+      for (int m = 0; m < 16; ++m) d[p + P * m] = v[m];
+    }
+  }
+  if constexpr (DO_X) {
+    __syncthreads();
+    // rows of the x transform: C == 1 -> column-major tile as is;
+    // C > 1 -> transpose through the cluster so this block holds rows
+    // [rank*LR, (rank+1)*LR) of all N columns, column-major with stride CS2.
+    int xs = G::CS;
+    if constexpr (C > 1) {
+      cg::cluster_group cl = cg::this_cluster();
+      constexpr int PER = G::LR * N / kThreads;  // elements per thread
+      float2 hold[PER];
+      cl.sync();
+#pragma unroll
+      for (int i = 0; i < PER; ++i) {
+        const int e = tid + kThreads * i;
+        const int kyl = e % G::LR, x = e / G::LR;
+        const float2* rs = cl.map_shared_rank(sm, x / G::M);
+        const int ky = rank * G::LR + kyl;
+        hold[i] = rs[(x % G::M) * G::CS + ky + (ky >> 4)];
+      }
+      cl.sync();
+#pragma unroll
+      for (int i = 0; i < PER; ++i) {
+        const int e = tid + kThreads * i;
+        const int kyl = e % G::LR, x = e / G::LR;
+        sm[x * G::CS2 + kyl + (kyl >> 4)] = hold[i];
+      }
+      __syncthreads();
+      xs = G::CS2;
+    }
+    constexpr int ROWS = C > 1 ? G::LR : N;
+    constexpr int RPR = kThreads / P;  // rows per round
+    for (int r0 = 0; r0 < ROWS; r0 += RPR) {
+      const int rl = r0 + tid % RPR, p = tid / RPR;
+      RowLine L{sm + rl + (rl >> 4), xs};
+      float2 v[16];
+#pragma unroll
+      for (int r = 0; r < 16; ++r) v[r] = L.at(p + P * r);
+      line_fft<N, false>(v, L, p, a.twx, SyncBlock{});
+      const int ky = (C > 1 ? rank * G::LR : 0) + rl;
+      float2* __restrict__ d = T + (long long)plane * nx * N + ky;
+#pragma unroll
+      for (int m = 0; m < 16; ++m) d[(long long)(p + P * m) * N] = v[m];
+    }
+  }
+}
+
+// ----------------------------------------------------------------------------
+// K2: outer-dimension pencils of length NO, TY consecutive y per block
+// ----------------------------------------------------------------------------
+template <int NO, int TY>
+__global__ void __launch_bounds__(TY*(NO / 16) < 1024 ? TY*(NO / 16) : 1024)
+    kf_pencil(OuterArgs a, float2* __restrict__ T, const DevState* __restrict__ st) {
+  constexpr int P = NO / 16;
+  constexpr int TYS = TY + 1;
+  if (load_done(st)) return;
+  extern __shared__ float2 sm[];
+  const Geom& g = a.g;
+  const int tid = threadIdx.x;
+  const int yl = tid % TY, p = tid / TY;
+  const int nyt = g.ny / TY;
+  const int yt = blockIdx.x % nyt;
+  const int mid = a.mode3d ? blockIdx.x / nyt : 0;
+  const int ky = yt * TY + yl;
+  const long long ps = a.mode3d ? (long long)g.ny * g.nx : (long long)g.ny;
+  float2* __restrict__ base = T + ky + (long long)g.ny * mid;
+  float2 v[16];
+#pragma unroll
+  for (int r = 0; r < 16; ++r) v[r] = base[ps * (p + P * r)];
+  RowLine L{sm + yl, TYS};
+  line_fft<NO, false>(v, L, p, a.po.tw, SyncBlock{});
+  // f_g0_scalar with the 1/N of ifftn: E ./ (px^2 + py^2 + (pz^2 - k02e))
+  const float py = a.w.pye[ky];
+  const float pxm = a.mode3d ? a.w.pxe[mid] : 0.f;
+  const float base2 = a.mode3d ? fmaf(pxm, pxm, py * py) : fmaf(py, py, a.w.pze[0] * a.w.pze[0]);
+  const float di = -a.k02e.y;
+#pragma unroll
+  for (int m = 0; m < 16; ++m) {
+    const int ko = p + P * m;
+    const float po = a.mode3d ? a.w.pze[ko] : a.w.pxe[ko];
+    const float dr = fmaf(po, po, base2) - a.k02e.x;
+    const float inv = a.norm / fmaf(dr, dr, di * di);
+    v[m] = cmul(v[m], make_float2(dr * inv, -di * inv));
+  }
+  line_fft<NO, true>(v, L, p, a.po.tw, SyncBlock{});
+#pragma unroll
+  for (int m = 0; m < 16; ++m) base[ps * (p + P * m)] = v[m];
+}
+
+// ----------------------------------------------------------------------------
+// K3
+// ----------------------------------------------------------------------------
+template <int N, int C, bool DO_X>
+__global__ void __launch_bounds__(kThreads, 2)
+    kf_plane_inv(InnerArgs a, const float2* __restrict__ T, float2* __restrict__ dE, float2* __restrict__ E,
+                 const float2* __restrict__ gamma, DevState* st, StopRule rule, Hist h) {
+  using G = PlaneGeom<N, C, DO_X>;
+  constexpr int P = G::P, LPR = G::LPR;
+  if (load_done(st)) return;
+  extern __shared__ float2 sm[];
+  __shared__ float red[kThreads / 32];
+  __shared__ unsigned int ticket;
+  const int tid = threadIdx.x;
+  const Geom& g = a.g;
+  const int nx = g.nx;
+  const int M = DO_X ? G::M : a.ncols;
+  int rank = 0, plane = 0, x0 = 0, z = 0, comp = 0, ncol;
+  long long colbase;
+  if constexpr (DO_X) {
+    rank = C > 1 ? (int)(blockIdx.x % C) : 0;
+    plane = blockIdx.x / C;
+    x0 = rank * M;
+    z = plane % g.nz;
+    comp = plane / g.nz;
+    colbase = (long long)plane * nx + x0;
+    ncol = M;
+  } else {
+    colbase = (long long)blockIdx.x * M;
+    ncol = (int)min((long long)M, (long long)nx * g.nc - colbase);
+  }
+  if constexpr (DO_X) {
+    constexpr int ROWS = C > 1 ? G::LR : N;
+    constexpr int RPR = kThreads / P;
+    const int xs = C > 1 ? G::CS2 : G::CS;
+    for (int r0 = 0; r0 < ROWS; r0 += RPR) {
+      const int rl = r0 + tid % RPR, p = tid / RPR;
+      const int ky = (C > 1 ? rank * G::LR : 0) + rl;
+      const float2* __restrict__ s = T + (long long)plane * nx * N + ky;
+      float2 v[16];
+#pragma unroll
+      for (int r = 0; r < 16; ++r) v[r] = s[(long long)(p + P * r) * N];
+      RowLine L{sm + rl + (rl >> 4), xs};
+      line_fft<N, true>(v, L, p, a.twx, SyncBlock{});
+#pragma unroll
+      for (int m = 0; m < 16; ++m) L.at(p + P * m) = v[m];
+    }
+    __syncthreads();
+    if constexpr (C > 1) {
+      cg::cluster_group cl = cg::this_cluster();
+      constexpr int PER = G::M * N / kThreads;
+      float2 hold[PER];
+      cl.sync();
+#pragma unroll
+      for (int i = 0; i < PER; ++i) {
+        const int e = tid + kThreads * i;
+        const int ky = e % N, c = e / N;
+        const float2* rs = cl.map_shared_rank(sm, ky / G::LR);
+        const int kyl = ky % G::LR;
+        hold[i] = rs[(x0 + c) * G::CS2 + kyl + (kyl >> 4)];
+      }
+      cl.sync();
+#pragma unroll
+      for (int i = 0; i < PER; ++i) {
+        const int e = tid + kThreads * i;
+        const int ky = e % N, c = e / N;
+        sm[c * G::CS + ky + (ky >> 4)] = hold[i];
+      }
+      __syncthreads();
+    }
+  }
+  const float2 gzz = a.w.gz[z];
+  float esum = 0.f;
+  for (int c0 = 0; c0 < ncol; c0 += LPR) {
+    const int cl = c0 + tid / P, p = tid % P;
+    const bool live = cl < ncol;
+    float2 v[16];
+    ColLine L{sm + (live ? cl : M) * G::CS};
+    if constexpr (DO_X) {
+#pragma unroll
+      for (int r = 0; r < 16; ++r) v[r] = L.at(p + P * r);
+    } else {
+      if (live) {
+        const float2* __restrict__ s = T + (colbase + cl) * N;
+#pragma unroll
+        for (int r = 0; r < 16; ++r) v[r] = s[p + P * r];
+      } else {
+#pragma unroll
+        for (int r = 0; r < 16; ++r) v[r] = make_float2(0.f, 0.f);
+      }
+    }
+    if constexpr (P <= 32) {
+      line_fft<N, true>(v, L, p, a.py.tw, SyncWarp{});
+    } else {
+      line_fft<N, true>(v, L, p, a.py.tw, SyncBlock{});
+    }
+    if (live) {
+      const long long col = colbase + cl;
+      int x, c;
+      if constexpr (DO_X) {
+        x = x0 + cl;
+        c = comp;
+      } else {
+        x = (int)(col % nx);
+        c = (int)(col / nx);
+      }
+      const float2 gxz = cmul(a.w.gx[x], gzz);
+      const bool in_xzc = x >= g.r0[1] && x < g.r1[1] && z >= g.r0[2] && z < g.r1[2] && c >= g.r0[3] && c < g.r1[3];
+      const long long gcol = col * N;
+      const long long gam = gcol - (long long)c * g.npts;
+#pragma unroll
+      for (int m = 0; m < 16; ++m) {
+        const int y = p + P * m;
+        const float2 ep = cmul_conj(cmul_conj(v[m], gxz), a.w.gy[y]);
+        const float2 gm = gamma[gam + y];
+        const float2 d0 = dE[gcol + y];
+        const float2 one_m = make_float2(1.f - kAlpha * gm.x, -kAlpha * gm.y);
+        const float2 t = cmul(cmul(gm, gm), ep);
+        const float2 dn = cadd(cmul(one_m, d0), make_float2(kAlpha * t.y, -kAlpha * t.x));
+        dE[gcol + y] = dn;
+        E[gcol + y] = cadd(E[gcol + y], dn);
+        if (in_xzc && y >= g.r0[0] && y < g.r1[0]) esum = fmaf(dn.x, dn.x, fmaf(dn.y, dn.y, esum));
+      }
+    }
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) esum += __shfl_xor_sync(0xffffffffu, esum, o);
+  if ((tid & 31) == 0) red[tid >> 5] = esum;
+  __syncthreads();
+  if (tid < 32) {
+    float v = tid < kThreads / 32 ? red[tid] : 0.f;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    if (tid == 0) {
+      atomicAdd(&st->e_acc, (double)v);
+      __threadfence();
+      ticket = atomicAdd(&st->blocks_done, 1u);
+    }
+  }
+  __syncthreads();
+  if (tid == 0 && ticket == gridDim.x - 1) {
+    __threadfence();
+    finish_iteration(st, rule, h);
+  }
+}
+
+}  // namespace fast
+}  // namespace ws

@@ -11,11 +11,13 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <string>
 #include <vector>
 
 #include "wavesim_b200.h"
+#include "ws_fast.cuh"
 #include "ws_kernels.cuh"
 
 namespace ws {
@@ -68,7 +70,45 @@ static bool length_supported(int n) {
   return n >= 1 && n <= 65536 && plan_radices(n, r);
 }
 
+// Fast power-of-two kernels (ws_fast.cuh), instantiated for these shapes.
+struct FastInner {
+  int n, c, do_x;
+  const void* fwd;
+  const void* inv;
+  size_t smem;      // bytes (3-D); 2-D: bytes per held column, one extra column of scratch
+};
+struct FastPencil {
+  int no, ty;
+  const void* fn;
+};
+
+template <int N, int C, bool DX>
+static FastInner fast_inner() {
+  using G = fast::PlaneGeom<N, C, DX>;
+  return FastInner{N, C, DX ? 1 : 0, (const void*)fast::kf_plane_fwd<N, C, DX>,
+                   (const void*)fast::kf_plane_inv<N, C, DX>, DX ? G::smem : (size_t)G::CS * sizeof(float2)};
+}
+template <int NO, int TY>
+static FastPencil fast_pencil() {
+  return FastPencil{NO, TY, (const void*)fast::kf_pencil<NO, TY>};
+}
+
+static const std::vector<FastInner>& fast_inner_table() {
+  static const std::vector<FastInner> t = {
+      fast_inner<64, 1, true>(),     fast_inner<128, 2, true>(),    fast_inner<256, 8, true>(),
+      fast_inner<64, 1, false>(),    fast_inner<128, 1, false>(),   fast_inner<256, 1, false>(),
+      fast_inner<512, 1, false>(),   fast_inner<1024, 1, false>(),  fast_inner<2048, 1, false>()};
+  return t;
+}
+static const std::vector<FastPencil>& fast_pencil_table() {
+  static const std::vector<FastPencil> t = {fast_pencil<32, 16>(),  fast_pencil<64, 16>(),  fast_pencil<128, 16>(),
+                                            fast_pencil<256, 16>(), fast_pencil<512, 8>(),  fast_pencil<1024, 4>()};
+  return t;
+}
+
 struct Layout {
+  const FastInner* fi = nullptr;   // fast K1/K3, or null (generic)
+  const FastPencil* fp = nullptr;  // fast K2, or null (generic)
   int rset = kPow2;  // radix set of every plan of the solver
   int mode3d = 0;
   int csize = 1;     // 3-D: blocks (cluster) per plane
@@ -150,6 +190,25 @@ static int make_layout(const Geom& g, Layout& L, std::string& why) {
   L.th_outer = threads_for((long long)g.nc * ty * no);
   L.smem_outer = (size_t)padded(g.nc * ty) * no * sizeof(float2);
   L.grid_outer = (long long)((g.ny + ty - 1) / ty) * mids;
+  // fast power-of-two kernels where a shape matches
+  const char* path = std::getenv("WAVESIM_B200_PATH");
+  if (path && std::strcmp(path, "generic") == 0) return WS_OK;
+  for (const FastInner& f : fast_inner_table()) {
+    if (L.mode3d && f.do_x && g.ny == f.n && g.nx == f.n) L.fi = &f;
+    if (!L.mode3d && !f.do_x && g.ny == f.n) L.fi = &f;
+  }
+  if (L.fi && !L.mode3d) {
+    // one round of lines per block: 256 threads, 16 elements each
+    const long long total_cols = (long long)g.nx * g.nc;
+    const long long want = std::max(1, 4096 / g.ny);
+    L.ncols = (int)want;
+    L.grid_inner = (total_cols + want - 1) / want;
+  }
+  if (L.fi && L.mode3d) L.grid_inner = (long long)g.nz * g.nc * L.fi->c;
+  if (g.nc == 1) {
+    for (const FastPencil& f : fast_pencil_table())
+      if (f.no == no && g.ny % f.ty == 0) L.fp = &f;
+  }
   return WS_OK;
 }
 
@@ -238,9 +297,10 @@ static void push_twiddles(std::vector<float2>& all, int n, size_t& off) {
 template <typename K>
 static cudaError_t allow_dynamic_smem(K kernel, int optin) {
   cudaFuncAttributes fa{};
-  cudaError_t e = cudaFuncGetAttributes(&fa, kernel);
+  cudaError_t e = cudaFuncGetAttributes(&fa, (const void*)kernel);
   if (e != cudaSuccess) return e;
-  return cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, optin - (int)fa.sharedSizeBytes);
+  return cudaFuncSetAttribute((const void*)kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              optin - (int)fa.sharedSizeBytes);
 }
 
 template <int RS>
@@ -263,6 +323,11 @@ static int set_kernel_attributes() {
   WS_CUDA(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
   WS_CUDA(set_attributes_for<kPow2>(optin));
   WS_CUDA(set_attributes_for<kMixed>(optin));
+  for (const FastInner& f : fast_inner_table()) {
+    WS_CUDA(allow_dynamic_smem(f.fwd, optin));
+    WS_CUDA(allow_dynamic_smem(f.inv, optin));
+  }
+  for (const FastPencil& f : fast_pencil_table()) WS_CUDA(allow_dynamic_smem(f.fn, optin));
   if (dev < 31) done_mask |= 1 << dev;
   return WS_OK;
 }
@@ -456,13 +521,70 @@ static cudaError_t launch_k3_t(const Solver* s, int w, const StopRule& rule, con
                             s->d_E, (const float2*)s->d_gamma, s->d_state, rule, h);
 }
 
+static size_t fast_inner_smem(const Solver* s) {
+  const FastInner* f = s->lay.fi;
+  return f->do_x ? f->smem : f->smem * (size_t)(s->lay.ncols + 1);
+}
+
+static cudaError_t launch_fast_inner(const Solver* s, const void* fn, void** args) {
+  cudaLaunchConfig_t cfg{};
+  cfg.gridDim = dim3((unsigned)s->lay.grid_inner);
+  cfg.blockDim = dim3(fast::kThreads);
+  cfg.dynamicSmemBytes = fast_inner_smem(s);
+  cfg.stream = s->stream;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeClusterDimension;
+  attr[0].val.clusterDim.x = s->lay.fi->do_x ? s->lay.fi->c : 1;
+  attr[0].val.clusterDim.y = 1;
+  attr[0].val.clusterDim.z = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelExC(&cfg, fn, args);
+}
+
 static cudaError_t launch_k1(const Solver* s, int w, bool with_source) {
+  if (s->lay.fi) {
+    InnerArgs a = inner_args(s, w);
+    a.ncols = s->lay.ncols;
+    const float2* dE = s->d_dE;
+    const float2* src = with_source ? s->d_src : nullptr;
+    float2 A = make_float2(0.f, (float)(1.0f / s->eps / (float)s->nw));
+    float2* T = s->d_T;
+    const DevState* st = s->d_state;
+    void* args[] = {&a, &dE, &src, &A, &T, &st};
+    return launch_fast_inner(s, s->lay.fi->fwd, args);
+  }
   return s->lay.rset == kPow2 ? launch_k1_t<kPow2>(s, w, with_source) : launch_k1_t<kMixed>(s, w, with_source);
 }
 static cudaError_t launch_k2(const Solver* s, int w) {
+  if (s->lay.fp) {
+    OuterArgs a = outer_args(s, w);
+    const FastPencil* f = s->lay.fp;
+    const int th = f->ty * (f->no / 16);
+    const long long mids = s->lay.mode3d ? s->g.nx : 1;
+    const unsigned grid = (unsigned)((s->g.ny / f->ty) * mids);
+    const size_t smem = (size_t)(f->ty + 1) * f->no * sizeof(float2);
+    float2* T = s->d_T;
+    const DevState* st = s->d_state;
+    void* args[] = {&a, &T, &st};
+    return cudaLaunchKernel(f->fn, dim3(grid), dim3(th), args, smem, s->stream);
+  }
   return s->lay.rset == kPow2 ? launch_k2_t<kPow2>(s, w) : launch_k2_t<kMixed>(s, w);
 }
 static cudaError_t launch_k3(const Solver* s, int w, const StopRule& rule, const Hist& h) {
+  if (s->lay.fi) {
+    InnerArgs a = inner_args(s, w);
+    a.ncols = s->lay.ncols;
+    const float2* T = s->d_T;
+    float2* dE = s->d_dE;
+    float2* E = s->d_E;
+    const float2* gamma = s->d_gamma;
+    DevState* st = s->d_state;
+    StopRule r = rule;
+    Hist hh = h;
+    void* args[] = {&a, &T, &dE, &E, &gamma, &st, &r, &hh};
+    return launch_fast_inner(s, s->lay.fi->inv, args);
+  }
   return s->lay.rset == kPow2 ? launch_k3_t<kPow2>(s, w, rule, h) : launch_k3_t<kMixed>(s, w, rule, h);
 }
 
