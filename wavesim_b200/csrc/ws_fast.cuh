@@ -284,7 +284,7 @@ __global__ void __launch_bounds__(TY*(NO / 16) < 1024 ? TY*(NO / 16) : 1024)
     const int ko = p + P * m;
     const float po = a.mode3d ? a.w.pze[ko] : a.w.pxe[ko];
     const float dr = fmaf(po, po, base2) - a.k02e.x;
-    const float inv = a.norm / fmaf(dr, dr, di * di);
+    const float inv = __fdividef(a.norm, fmaf(dr, dr, di * di));
     v[m] = cmul(v[m], make_float2(dr * inv, -di * inv));
   }
   line_fft<NO, true>(v, L, p, a.po.tw, SyncBlock{});
@@ -298,13 +298,12 @@ __global__ void __launch_bounds__(TY*(NO / 16) < 1024 ? TY*(NO / 16) : 1024)
 template <int N, int C, bool DO_X>
 __global__ void __launch_bounds__(kThreads, 2)
     kf_plane_inv(InnerArgs a, const float2* __restrict__ T, float2* __restrict__ dE, float2* __restrict__ E,
-                 const float2* __restrict__ gamma, DevState* st, StopRule rule, Hist h) {
+                 const float2* __restrict__ gamma, const DevState* __restrict__ st, double* __restrict__ partials) {
   using G = PlaneGeom<N, C, DO_X>;
   constexpr int P = G::P, LPR = G::LPR;
   if (load_done(st)) return;
   extern __shared__ float2 sm[];
   __shared__ float red[kThreads / 32];
-  __shared__ unsigned int ticket;
   const int tid = threadIdx.x;
   const Geom& g = a.g;
   const int nx = g.nx;
@@ -401,19 +400,33 @@ __global__ void __launch_bounds__(kThreads, 2)
       const float2 gxz = cmul(a.w.gx[x], gzz);
       const bool in_xzc = x >= g.r0[1] && x < g.r1[1] && z >= g.r0[2] && z < g.r1[2] && c >= g.r0[3] && c < g.r1[3];
       const long long gcol = col * N;
-      const long long gam = gcol - (long long)c * g.npts;
+      const float2* __restrict__ gmc = gamma + (gcol - (long long)c * g.npts);
+      float2* __restrict__ dEc = dE + gcol;
+      float2* __restrict__ Ec = E + gcol;
+      // Eprop after the conjugate ramps (WaveSim.m:55), then f_mix (f_mix.m:3-4)
+      // and E += dE; the loads of a half are issued together.
 #pragma unroll
-      for (int m = 0; m < 16; ++m) {
-        const int y = p + P * m;
-        const float2 ep = cmul_conj(cmul_conj(v[m], gxz), a.w.gy[y]);
-        const float2 gm = gamma[gam + y];
-        const float2 d0 = dE[gcol + y];
-        const float2 one_m = make_float2(1.f - kAlpha * gm.x, -kAlpha * gm.y);
-        const float2 t = cmul(cmul(gm, gm), ep);
-        const float2 dn = cadd(cmul(one_m, d0), make_float2(kAlpha * t.y, -kAlpha * t.x));
-        dE[gcol + y] = dn;
-        E[gcol + y] = cadd(E[gcol + y], dn);
-        if (in_xzc && y >= g.r0[0] && y < g.r1[0]) esum = fmaf(dn.x, dn.x, fmaf(dn.y, dn.y, esum));
+      for (int h = 0; h < 2; ++h) {
+        float2 gm[8], d0[8], e0[8];
+#pragma unroll
+        for (int i = 0; i < 8; ++i) {
+          const int y = p + P * (8 * h + i);
+          gm[i] = gmc[y];
+          d0[i] = dEc[y];
+          e0[i] = Ec[y];
+        }
+#pragma unroll
+        for (int i = 0; i < 8; ++i) {
+          const int m = 8 * h + i;
+          const int y = p + P * m;
+          const float2 ep = cmul_conj(cmul_conj(v[m], gxz), a.w.gy[y]);
+          const float2 one_m = make_float2(1.f - kAlpha * gm[i].x, -kAlpha * gm[i].y);
+          const float2 t = cmul(cmul(gm[i], gm[i]), ep);
+          const float2 dn = cadd(cmul(one_m, d0[i]), make_float2(kAlpha * t.y, -kAlpha * t.x));
+          dEc[y] = dn;
+          Ec[y] = cadd(e0[i], dn);
+          if (in_xzc && y >= g.r0[0] && y < g.r1[0]) esum = fmaf(dn.x, dn.x, fmaf(dn.y, dn.y, esum));
+        }
       }
     }
   }
@@ -425,16 +438,7 @@ __global__ void __launch_bounds__(kThreads, 2)
     float v = tid < kThreads / 32 ? red[tid] : 0.f;
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-    if (tid == 0) {
-      atomicAdd(&st->e_acc, (double)v);
-      __threadfence();
-      ticket = atomicAdd(&st->blocks_done, 1u);
-    }
-  }
-  __syncthreads();
-  if (tid == 0 && ticket == gridDim.x - 1) {
-    __threadfence();
-    finish_iteration(st, rule, h);
+    if (tid == 0) partials[blockIdx.x] = (double)v;
   }
 }
 

@@ -269,7 +269,7 @@ __global__ void __launch_bounds__(512, 1) k_outer(OuterArgs a, float2* __restric
 // Simulation.next (Simulation.m:193-217), run by one thread after the energy
 // of iteration st->it is complete.
 __device__ __forceinline__ void finish_iteration(DevState* st, const StopRule& rule, const Hist& h) {
-  const double e = atomicAdd(&st->e_acc, 0.0);
+  const double e = st->e_acc;
   st->e_acc = 0.0;
   const int it = st->it;
   if (h.fresh && it - 1 < h.cap) h.fresh[it - 1] = e;
@@ -293,18 +293,16 @@ __device__ __forceinline__ void finish_iteration(DevState* st, const StopRule& r
   st->calc_energy = ((it - 1) % rule.interval) == 0;
   st->it = it + 1;
   st->blocks_done = 0;
-  __threadfence();
 }
 
 // K3 -------------------------------------------------------------------------
 template <int EMAX, int RSET>
 __global__ void __launch_bounds__(512, 1) k_inv_inner(InnerArgs a, const float2* __restrict__ T, float2* __restrict__ dE,
                                                     float2* __restrict__ E, const float2* __restrict__ gamma,
-                                                    DevState* st, StopRule rule, Hist h) {
+                                                    const DevState* __restrict__ st, double* __restrict__ partials) {
   if (load_done(st)) return;
   extern __shared__ float2 sm[];
   __shared__ float red[32];
-  __shared__ unsigned int ticket;
   const int tid = threadIdx.x, nthr = blockDim.x;
   const Geom& g = a.g;
   const int ny = g.ny, LS = padded(ny);
@@ -370,7 +368,7 @@ __global__ void __launch_bounds__(512, 1) k_inv_inner(InnerArgs a, const float2*
         c >= g.r0[3] && c < g.r1[3])
       esum = fmaf(dn.x, dn.x, fmaf(dn.y, dn.y, esum));
   }
-  // block reduction of the ROI energy, then one atomic per block
+  // block reduction of the ROI energy into this block's partial sum
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) esum += __shfl_xor_sync(0xffffffffu, esum, o);
   if ((tid & 31) == 0) red[tid >> 5] = esum;
@@ -379,21 +377,33 @@ __global__ void __launch_bounds__(512, 1) k_inv_inner(InnerArgs a, const float2*
     float v = tid < (nthr + 31) / 32 ? red[tid] : 0.f;
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-    if (tid == 0) {
-      atomicAdd(&st->e_acc, (double)v);
-      __threadfence();
-      ticket = atomicAdd(&st->blocks_done, 1u);
-    }
+    if (tid == 0) partials[blockIdx.x] = (double)v;
   }
+}
+
+// The stop rule after each iteration: sums the per-block ROI energies of K3 in
+// a fixed order (so the energy history is reproducible bit for bit) and runs
+// Simulation.next (Simulation.m:193-217).  One block.
+static __global__ void __launch_bounds__(256) k_finish_iteration(DevState* st, StopRule rule, Hist h,
+                                                          const double* __restrict__ partials, int nparts) {
+  if (load_done(st)) return;
+  __shared__ double red[256];
+  double acc = 0.0;
+  for (int i = threadIdx.x; i < nparts; i += blockDim.x) acc += partials[i];
+  red[threadIdx.x] = acc;
   __syncthreads();
-  if (tid == 0 && ticket == gridDim.x - 1) {
-    __threadfence();
+  for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+    if ((int)threadIdx.x < o) red[threadIdx.x] += red[threadIdx.x + o];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    st->e_acc = red[0];
     finish_iteration(st, rule, h);
   }
 }
 
 // Helpers --------------------------------------------------------------------
-__global__ void k_reset_state(DevState* st) {
+static __global__ void k_reset_state(DevState* st) {
   if (threadIdx.x == 0 && blockIdx.x == 0) {
     st->it = 1;
     st->done = 0;
@@ -411,7 +421,7 @@ __global__ void k_reset_state(DevState* st) {
 // Runs after each wiggle cycle of the graph: continues the device-side while
 // loop only if the stop rule has not fired and fewer than max_cycles cycles
 // have run, so the loop ends even if the stop logic were never reached.
-__global__ void k_cycle_guard(DevState* st, cudaGraphConditionalHandle cond, long long max_cycles) {
+static __global__ void k_cycle_guard(DevState* st, cudaGraphConditionalHandle cond, long long max_cycles) {
   if (threadIdx.x == 0 && blockIdx.x == 0) {
     const long long c = ++st->cycles;
     const bool go = !st->done && c < max_cycles;
@@ -420,7 +430,7 @@ __global__ void k_cycle_guard(DevState* st, cudaGraphConditionalHandle cond, lon
   }
 }
 
-__global__ void k_resume_state(DevState* st) {
+static __global__ void k_resume_state(DevState* st) {
   if (threadIdx.x == 0 && blockIdx.x == 0) {
     st->done = 0;
     st->blocks_done = 0;
@@ -430,7 +440,7 @@ __global__ void k_resume_state(DevState* st) {
 
 // Source.add_to for one block (values at 0-based corner p, size s), into the
 // dense source buffer; also accumulates the block energy (Source.m:57-67).
-__global__ void k_scatter_source(float2* __restrict__ dst, const float2* __restrict__ vals, Geom g, int p0, int p1,
+static __global__ void k_scatter_source(float2* __restrict__ dst, const float2* __restrict__ vals, Geom g, int p0, int p1,
                                  int p2, int p3, int s0, int s1, int s2, int s3, double* energy) {
   const long long n = (long long)s0 * s1 * s2 * s3;
   float esum = 0.f;
@@ -451,7 +461,7 @@ __global__ void k_scatter_source(float2* __restrict__ dst, const float2* __restr
 }
 
 // E = E' ./ gamma on the roi (WaveSimBase.m:193,196), column-major output.
-__global__ void k_finalize(const float2* __restrict__ Ep, const float2* __restrict__ gamma, Geom g,
+static __global__ void k_finalize(const float2* __restrict__ Ep, const float2* __restrict__ gamma, Geom g,
                            float2* __restrict__ out) {
   const int ry = g.r1[0] - g.r0[0], rx = g.r1[1] - g.r0[1], rz = g.r1[2] - g.r0[2], rc = g.r1[3] - g.r0[3];
   const long long n = (long long)ry * rx * rz * rc;

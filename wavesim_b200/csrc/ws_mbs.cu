@@ -246,6 +246,7 @@ struct Solver {
   double* d_hist = nullptr;  // diff | fresh
   long long hist_cap = 0;
   double* d_energy = nullptr;
+  double* d_partials = nullptr;  // per-block ROI energy of K3
   float2* d_tw = nullptr;
   FftPlan py{}, pxl{}, po{};
   const float2* twx = nullptr;
@@ -266,8 +267,8 @@ static void destroy_solver(Solver* s) {
   if (!s) return;
   cudaSetDevice(s->device);
   free_graph(s);
-  void* ptrs[] = {s->d_wigf, s->d_wigc, s->d_gamma, s->d_E,     s->d_dE,     s->d_T,  s->d_src,
-                  s->d_stage, s->d_out, s->d_state, s->d_hist, s->d_energy, s->d_tw};
+  void* ptrs[] = {s->d_wigf, s->d_wigc,  s->d_gamma,  s->d_E,        s->d_dE, s->d_T,   s->d_src,
+                  s->d_stage, s->d_out, s->d_state, s->d_hist, s->d_energy, s->d_tw, s->d_partials};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   for (auto& e : s->ev)
@@ -444,6 +445,7 @@ static int create_solver(const int64_t N[4], const ws_complex* gamma, int64_t n_
   WS_TRY(cudaMalloc(&s->d_src, nbytes));
   WS_TRY(cudaMalloc(&s->d_state, sizeof(DevState)));
   WS_TRY(cudaMalloc(&s->d_energy, sizeof(double)));
+  WS_TRY(cudaMalloc(&s->d_partials, (size_t)std::max<long long>(1, s->lay.grid_inner) * sizeof(double)));
   WS_TRY(cudaMemset(s->d_E, 0, nbytes));
   WS_TRY(cudaMemset(s->d_dE, 0, nbytes));
 #undef WS_TRY
@@ -504,7 +506,7 @@ static cudaError_t launch_k2_t(const Solver* s, int w) {
 }
 
 template <int RS>
-static cudaError_t launch_k3_t(const Solver* s, int w, const StopRule& rule, const Hist& h) {
+static cudaError_t launch_k3_t(const Solver* s, int w) {
   cudaLaunchConfig_t cfg{};
   cfg.gridDim = dim3((unsigned)s->lay.grid_inner);
   cfg.blockDim = dim3(s->lay.th_inner);
@@ -518,7 +520,7 @@ static cudaError_t launch_k3_t(const Solver* s, int w, const StopRule& rule, con
   cfg.attrs = attr;
   cfg.numAttrs = 1;
   return cudaLaunchKernelEx(&cfg, k_inv_inner<kEmax, RS>, inner_args(s, w), (const float2*)s->d_T, s->d_dE,
-                            s->d_E, (const float2*)s->d_gamma, s->d_state, rule, h);
+                            s->d_E, (const float2*)s->d_gamma, (const DevState*)s->d_state, s->d_partials);
 }
 
 static size_t fast_inner_smem(const Solver* s) {
@@ -571,7 +573,8 @@ static cudaError_t launch_k2(const Solver* s, int w) {
   }
   return s->lay.rset == kPow2 ? launch_k2_t<kPow2>(s, w) : launch_k2_t<kMixed>(s, w);
 }
-static cudaError_t launch_k3(const Solver* s, int w, const StopRule& rule, const Hist& h) {
+static cudaError_t launch_k3_only(const Solver* s, int w) {
+  cudaError_t e;
   if (s->lay.fi) {
     InnerArgs a = inner_args(s, w);
     a.ncols = s->lay.ncols;
@@ -579,13 +582,25 @@ static cudaError_t launch_k3(const Solver* s, int w, const StopRule& rule, const
     float2* dE = s->d_dE;
     float2* E = s->d_E;
     const float2* gamma = s->d_gamma;
-    DevState* st = s->d_state;
-    StopRule r = rule;
-    Hist hh = h;
-    void* args[] = {&a, &T, &dE, &E, &gamma, &st, &r, &hh};
-    return launch_fast_inner(s, s->lay.fi->inv, args);
+    const DevState* st = s->d_state;
+    double* partials = s->d_partials;
+    void* args[] = {&a, &T, &dE, &E, &gamma, &st, &partials};
+    e = launch_fast_inner(s, s->lay.fi->inv, args);
+  } else {
+    e = s->lay.rset == kPow2 ? launch_k3_t<kPow2>(s, w) : launch_k3_t<kMixed>(s, w);
   }
-  return s->lay.rset == kPow2 ? launch_k3_t<kPow2>(s, w, rule, h) : launch_k3_t<kMixed>(s, w, rule, h);
+  return e;
+}
+
+static cudaError_t launch_finish(const Solver* s, const StopRule& rule, const Hist& h) {
+  k_finish_iteration<<<1, 256, 0, s->stream>>>(s->d_state, rule, h, s->d_partials, (int)s->lay.grid_inner);
+  return cudaGetLastError();
+}
+
+static cudaError_t launch_k3(const Solver* s, int w, const StopRule& rule, const Hist& h) {
+  cudaError_t e = launch_k3_only(s, w);
+  if (e != cudaSuccess) return e;
+  return launch_finish(s, rule, h);
 }
 
 static cudaError_t launch_iteration(const Solver* s, int it0, bool with_source, const StopRule& rule,
@@ -906,7 +921,7 @@ int ws_solver_buffers(ws_solver h, void** E_prime, void** stream) {
   return WS_OK;
 }
 
-int ws_solver_launches_per_iteration(ws_solver h) { return h ? 3 : 0; }
+int ws_solver_launches_per_iteration(ws_solver h) { return h ? 4 : 0; }
 
 int ws_solver_time_kernels(ws_solver h, int n_iterations, float ms_out[3], double bytes_out[3]) {
   if (!h || !ms_out || n_iterations < 1) return fail(WS_ERR_INVALID_ARGUMENT, "bad argument");
@@ -928,8 +943,9 @@ int ws_solver_time_kernels(ws_solver h, int n_iterations, float ms_out[3], doubl
     WS_CUDA(cudaEventRecord(s->ev[1], s->stream));
     WS_CUDA(launch_k2(s, w));
     WS_CUDA(cudaEventRecord(s->ev[2], s->stream));
-    WS_CUDA(launch_k3(s, w, rule, hh));
+    WS_CUDA(launch_k3_only(s, w));
     WS_CUDA(cudaEventRecord(s->ev[3], s->stream));
+    WS_CUDA(launch_finish(s, rule, hh));
     WS_CUDA(cudaEventSynchronize(s->ev[3]));
     float t;
     for (int k = 0; k < 3; ++k) {
