@@ -175,6 +175,41 @@ int ws_solver_launches_per_iteration(ws_solver s);
 
 int ws_solver_destroy(ws_solver s);
 
+/*
+ * ws_run_algorithm_noalloc - the same loop as ws_run_algorithm for callers
+ * that cannot allocate GPU memory (an application that owns the device
+ * through its own memory pool, a real-time loop that forbids allocation after
+ * start-up, a plug-in confined to the buffers it is handed).  No counterpart
+ * in the reference.
+ *
+ * Every pointer is a device pointer except wiggles (a host array of
+ * ws_wiggle whose members are device pointers), N, roi and the scalar outputs.
+ * source_field is the dense source, Ny*Nx*Nz*Nc complex (the blocks summed
+ * into one field, Source.add_to with factor 1).  E_out receives E' (full
+ * grid), diff_energy_out (device, >= max_iterations + n_wiggles doubles) the
+ * energy history.  stream: a cudaStream_t, or NULL for the default stream.
+ *
+ * The working arrays live in one statically allocated device array of
+ * ws_noalloc_scratch_bytes() bytes (40 MiB), shared by all calls and kept by
+ * every GPU that loads it until the process exits.  A grid needs 16 bytes per
+ * field element plus twiddle tables: about 2.6 million elements at most;
+ * larger grids return WS_ERR_INVALID_ARGUMENT.  Calls that overlap on the GPU
+ * race on the shared array.  The first call on each device looks up the
+ * array's address and should come before any stream capture.  Errors:
+ * ws_noalloc_last_error().
+ */
+int ws_run_algorithm_noalloc(const int64_t N[4], const ws_complex* gamma, int64_t n_wiggles,
+                             const ws_wiggle* wiggles, const ws_complex* source_field, float epsilon,
+                             ws_complex k02e, const int64_t roi[8], int64_t max_iterations,
+                             double energy_threshold, int64_t energy_interval, ws_complex* E_out,
+                             double* diff_energy_out, int64_t* n_iterations, int* converged, void* stream);
+
+/* Size in bytes of the static scratch array of ws_run_algorithm_noalloc. */
+int64_t ws_noalloc_scratch_bytes(void);
+
+/* Message of the last failed ws_run_algorithm_noalloc call on this thread. */
+const char* ws_noalloc_last_error(void);
+
 #ifdef __cplusplus
 }
 #endif

@@ -1,7 +1,7 @@
 """ctypes binding of the C ABI in include/wavesim_b200.h.
 
 The shared library ``libwavesim_b200.so`` is built in-tree next to this file
-(``python -m wavesim_b200.build`` or ``__graft_entry__.build()``).  There is
+(``python wavesim_b200/build.py`` or ``__graft_entry__.build()``).  There is
 no fallback: if the library is missing, importing this module raises.
 """
 from __future__ import annotations
@@ -61,7 +61,8 @@ class ws_solve_options(C.Structure):
 EXPORTS = [
     "ws_default_options", "ws_version", "ws_last_error", "ws_size_supported", "ws_run_algorithm",
     "ws_solver_create", "ws_solver_solve", "ws_solver_buffers", "ws_solver_time_kernels",
-    "ws_solver_launches_per_iteration", "ws_solver_destroy",
+    "ws_solver_launches_per_iteration", "ws_solver_destroy", "ws_run_algorithm_noalloc",
+    "ws_noalloc_scratch_bytes", "ws_noalloc_last_error",
 ]
 
 
@@ -74,7 +75,7 @@ class WaveSimError(RuntimeError):
 def _load():
     if not os.path.exists(LIB_PATH):
         raise ImportError(
-            f"{LIB_PATH} is missing: build the CUDA library first (python -m wavesim_b200.build)")
+            f"{LIB_PATH} is missing: build the CUDA library first (python wavesim_b200/build.py)")
     lib = C.CDLL(LIB_PATH)
     P = C.c_void_p
     i64p = C.POINTER(C.c_int64)
@@ -104,6 +105,12 @@ def _load():
     lib.ws_solver_launches_per_iteration.restype = C.c_int
     lib.ws_solver_destroy.argtypes = [P]
     lib.ws_solver_destroy.restype = C.c_int
+    lib.ws_run_algorithm_noalloc.argtypes = [i64p, P, C.c_int64, C.POINTER(ws_wiggle), P, C.c_float, ws_complex,
+                                             i64p, C.c_int64, C.c_double, C.c_int64, P, P, i64p,
+                                             C.POINTER(C.c_int), P]
+    lib.ws_run_algorithm_noalloc.restype = C.c_int
+    lib.ws_noalloc_scratch_bytes.restype = C.c_int64
+    lib.ws_noalloc_last_error.restype = C.c_char_p
     return lib
 
 

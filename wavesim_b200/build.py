@@ -1,4 +1,7 @@
-"""Build libwavesim_b200.so in-tree for sm_100a:  python -m wavesim_b200.build"""
+"""Build libwavesim_b200.so in-tree for sm_100a:  python wavesim_b200/build.py
+
+(Run as a script: importing the package itself needs the built library.)
+"""
 from __future__ import annotations
 
 import os
@@ -13,7 +16,7 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-shared", "-I" + os.path.join(ROOT, "include")]
 
 TARGETS = {
-    "libwavesim_b200.so": ["ws_mbs.cu"],
+    "libwavesim_b200.so": ["ws_mbs.cu", "ws_noalloc.cu"],
 }
 
 
