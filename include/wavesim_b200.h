@@ -131,8 +131,9 @@ int ws_size_supported(const int64_t N[4]);
  * memory : WS_HOST or WS_DEVICE for every array argument (gamma, wiggles,
  *          source values, E_out)
  * E_out  : Ny*Nx*Nz*Nc complex, receives E' (the caller divides by gamma)
- * diff_energy_out : capacity >= max_iterations doubles; receives the
- *          per-iteration energy history; *n_iterations its length.
+ * diff_energy_out : capacity >= max_iterations + Nwiggles doubles (the loop
+ *          stops at the first multiple of Nwiggles >= max_iterations);
+ *          receives the per-iteration energy history; *n_iterations its length.
  * callback / user_data: may be NULL.
  */
 int ws_run_algorithm(const int64_t N[4], const ws_complex* gamma, int64_t n_wiggles, const ws_wiggle* wiggles,
@@ -156,6 +157,21 @@ int ws_solver_create(const int64_t N[4], const ws_complex* gamma, int64_t n_wigg
 int ws_solver_solve(ws_solver s, int64_t n_blocks, const ws_source_block* source, int source_memory,
                     const ws_solve_options* opts, ws_complex* E_out, int out_memory, double* diff_energy_out,
                     int64_t* n_iterations, int* converged);
+
+/* ws_solver_solve_batch - n_rhs right-hand sides (sources) on the solver's
+ * medium in one set of launches: the blocks of right-hand side r are the
+ * block_counts[r] entries that follow those of r-1 in `blocks`.  Each one runs
+ * the reference loop with its own stop rule; one that has converged stops
+ * working while the others go on.  Outputs are consecutive per right-hand
+ * side: E_out (n_rhs fields, E' or the roi field per opts->output),
+ * diff_energy_out (host, may be NULL: n_rhs x diff_capacity doubles),
+ * n_iterations and converged (n_rhs entries each, may be NULL).  The batch
+ * form of ws_solver_solve; no counterpart in the reference, whose callers run
+ * exec once per source (e.g. examples/pulse2d.m:31-40).  Callbacks are not
+ * supported for n_rhs > 1. */
+int ws_solver_solve_batch(ws_solver s, int64_t n_rhs, const int64_t* block_counts, const ws_source_block* blocks,
+                          int source_memory, const ws_solve_options* opts, ws_complex* E_out, int out_memory,
+                          double* diff_energy_out, int64_t diff_capacity, int64_t* n_iterations, int* converged);
 
 /* Device pointer of the solver's current E' buffer and the CUDA stream it
  * works on (both valid until ws_solver_destroy). */

@@ -60,7 +60,7 @@ class ws_solve_options(C.Structure):
 # every entry point declared in include/wavesim_b200.h
 EXPORTS = [
     "ws_default_options", "ws_version", "ws_last_error", "ws_size_supported", "ws_run_algorithm",
-    "ws_solver_create", "ws_solver_solve", "ws_solver_buffers", "ws_solver_time_kernels",
+    "ws_solver_create", "ws_solver_solve", "ws_solver_solve_batch", "ws_solver_buffers", "ws_solver_time_kernels",
     "ws_solver_launches_per_iteration", "ws_solver_destroy", "ws_run_algorithm_noalloc",
     "ws_noalloc_scratch_bytes", "ws_noalloc_last_error",
 ]
@@ -97,6 +97,10 @@ def _load():
                                     C.POINTER(ws_solve_options), P, C.c_int, C.POINTER(C.c_double), i64p,
                                     C.POINTER(C.c_int)]
     lib.ws_solver_solve.restype = C.c_int
+    lib.ws_solver_solve_batch.argtypes = [P, C.c_int64, i64p, C.POINTER(ws_source_block), C.c_int,
+                                          C.POINTER(ws_solve_options), P, C.c_int, C.POINTER(C.c_double), C.c_int64,
+                                          i64p, C.POINTER(C.c_int)]
+    lib.ws_solver_solve_batch.restype = C.c_int
     lib.ws_solver_buffers.argtypes = [P, C.POINTER(C.c_void_p), C.POINTER(C.c_void_p)]
     lib.ws_solver_buffers.restype = C.c_int
     lib.ws_solver_time_kernels.argtypes = [P, C.c_int, C.POINTER(C.c_float), C.POINTER(C.c_double)]
@@ -110,6 +114,10 @@ def _load():
                                              C.POINTER(C.c_int), P]
     lib.ws_run_algorithm_noalloc.restype = C.c_int
     lib.ws_noalloc_scratch_bytes.restype = C.c_int64
+    lib.ws_gemm_bf16.argtypes = [P, P, P, P, P, C.c_int64, C.c_int64, C.c_int64, C.c_int64, C.c_int64, C.c_int64,
+                                 C.c_int, P, P]
+    lib.ws_gemm_bf16.restype = C.c_int
+    lib.ws_net_last_error.restype = C.c_char_p
     lib.ws_noalloc_last_error.restype = C.c_char_p
     return lib
 

@@ -52,6 +52,12 @@ struct RowLine {
   __device__ __forceinline__ float2& at(int i) const { return base[i * stride]; }
 };
 
+// Ask the bulk-copy engine to pull [p, p + bytes) into L2 (no registers, no
+// shared memory; p and bytes multiples of 16).
+__device__ __forceinline__ void prefetch_l2(const void* p, unsigned bytes) {
+  asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(p), "r"(bytes) : "memory");
+}
+
 struct SyncWarp {
   __device__ __forceinline__ void operator()() const { __syncwarp(); }
 };
@@ -147,7 +153,12 @@ __global__ void __launch_bounds__(kThreads, 2)
                  float2* __restrict__ T, const DevState* __restrict__ st) {
   using G = PlaneGeom<N, C, DO_X>;
   constexpr int P = G::P, LPR = G::LPR;
+  const int rhs = blockIdx.x / a.bpr, bid = blockIdx.x - rhs * a.bpr;
+  st += rhs;
   if (load_done(st)) return;
+  dE += rhs * a.fstride;
+  if (src) src += rhs * a.fstride;
+  T += rhs * a.fstride;
   extern __shared__ float2 sm[];
   const int tid = threadIdx.x;
   const Geom& g = a.g;
@@ -156,14 +167,14 @@ __global__ void __launch_bounds__(kThreads, 2)
   int rank = 0, plane = 0, x0 = 0, z = 0, ncol;
   long long colbase;
   if constexpr (DO_X) {
-    rank = C > 1 ? (int)(blockIdx.x % C) : 0;
-    plane = blockIdx.x / C;
+    rank = C > 1 ? (int)(bid % C) : 0;
+    plane = bid / C;
     x0 = rank * M;
     z = plane % g.nz;
     colbase = (long long)plane * nx + x0;
     ncol = M;
   } else {
-    colbase = (long long)blockIdx.x * M;
+    colbase = (long long)bid * M;
     ncol = (int)min((long long)M, (long long)nx * g.nc - colbase);
   }
   const float2 gzz = a.w.gz[z];
@@ -258,14 +269,17 @@ __global__ void __launch_bounds__(TY*(NO / 16) < 1024 ? TY*(NO / 16) : 1024)
     kf_pencil(OuterArgs a, float2* __restrict__ T, const DevState* __restrict__ st) {
   constexpr int P = NO / 16;
   constexpr int TYS = TY + 1;
+  const int rhs = blockIdx.x / a.bpr, bid = blockIdx.x - rhs * a.bpr;
+  st += rhs;
   if (load_done(st)) return;
+  T += rhs * a.fstride;
   extern __shared__ float2 sm[];
   const Geom& g = a.g;
   const int tid = threadIdx.x;
   const int yl = tid % TY, p = tid / TY;
   const int nyt = g.ny / TY;
-  const int yt = blockIdx.x % nyt;
-  const int mid = a.mode3d ? blockIdx.x / nyt : 0;
+  const int yt = bid % nyt;
+  const int mid = a.mode3d ? bid / nyt : 0;
   const int ky = yt * TY + yl;
   const long long ps = a.mode3d ? (long long)g.ny * g.nx : (long long)g.ny;
   float2* __restrict__ base = T + ky + (long long)g.ny * mid;
@@ -301,7 +315,13 @@ __global__ void __launch_bounds__(kThreads, 2)
                  const float2* __restrict__ gamma, const DevState* __restrict__ st, double* __restrict__ partials) {
   using G = PlaneGeom<N, C, DO_X>;
   constexpr int P = G::P, LPR = G::LPR;
+  const int rhs = blockIdx.x / a.bpr, bid = blockIdx.x - rhs * a.bpr;
+  st += rhs;
   if (load_done(st)) return;
+  T += rhs * a.fstride;
+  dE += rhs * a.fstride;
+  E += rhs * a.fstride;
+  partials += (long long)rhs * a.bpr;
   extern __shared__ float2 sm[];
   __shared__ float red[kThreads / 32];
   const int tid = threadIdx.x;
@@ -311,16 +331,27 @@ __global__ void __launch_bounds__(kThreads, 2)
   int rank = 0, plane = 0, x0 = 0, z = 0, comp = 0, ncol;
   long long colbase;
   if constexpr (DO_X) {
-    rank = C > 1 ? (int)(blockIdx.x % C) : 0;
-    plane = blockIdx.x / C;
+    rank = C > 1 ? (int)(bid % C) : 0;
+    plane = bid / C;
     x0 = rank * M;
     z = plane % g.nz;
     comp = plane / g.nz;
     colbase = (long long)plane * nx + x0;
     ncol = M;
   } else {
-    colbase = (long long)blockIdx.x * M;
+    colbase = (long long)bid * M;
     ncol = (int)min((long long)M, (long long)nx * g.nc - colbase);
+  }
+  // the epilogue's dE, E and gamma columns are contiguous: start pulling them
+  // into L2 now so that they arrive while the transforms run
+  if (tid == 0 && ncol > 0) {
+    const long long c0 = colbase;
+    const unsigned bytes = (unsigned)ncol * N * sizeof(float2);
+    const int comp0 = DO_X ? comp : (int)(colbase / nx);
+    const int comp1 = DO_X ? comp : (int)((colbase + ncol - 1) / nx);
+    prefetch_l2(dE + c0 * N, bytes);
+    prefetch_l2(E + c0 * N, bytes);
+    if (comp0 == comp1) prefetch_l2(gamma + c0 * N - (long long)comp0 * g.npts, bytes);
   }
   if constexpr (DO_X) {
     constexpr int ROWS = C > 1 ? G::LR : N;
@@ -438,7 +469,7 @@ __global__ void __launch_bounds__(kThreads, 2)
     float v = tid < kThreads / 32 ? red[tid] : 0.f;
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-    if (tid == 0) partials[blockIdx.x] = (double)v;
+    if (tid == 0) partials[bid] = (double)v;
   }
 }
 

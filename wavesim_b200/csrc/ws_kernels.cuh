@@ -77,6 +77,7 @@ struct Hist {
   double* diff;   // state.diff_energy
   double* fresh;  // energy of every iteration
   long long cap;
+  long long stride;  // distance between the histories of consecutive right-hand sides
 };
 
 struct InnerArgs {
@@ -88,6 +89,8 @@ struct InnerArgs {
   int csize;    // blocks per plane (cluster size), 3-D only
   int mode3d;
   int ncols;    // columns per block, 2-D only
+  int bpr;      // blocks per right-hand side (a batch of sources runs as consecutive block ranges)
+  long long fstride;  // elements between the fields of consecutive right-hand sides
 };
 
 struct OuterArgs {
@@ -98,6 +101,8 @@ struct OuterArgs {
   float norm;   // 1 / (Ny Nx Nz), the normalisation of ifftn
   int ty;       // consecutive y per block
   int mode3d;
+  int bpr;
+  long long fstride;
 };
 
 __device__ __forceinline__ int load_done(const DevState* st) { return __ldcg(&st->done); }
@@ -147,7 +152,12 @@ template <int EMAX, int RSET>
 __global__ void __launch_bounds__(512, 1) k_fwd_inner(InnerArgs a, const float2* __restrict__ dE,
                                                     const float2* __restrict__ src, float2 A,
                                                     float2* __restrict__ T, const DevState* __restrict__ st) {
+  const int rhs = blockIdx.x / a.bpr, bid = blockIdx.x - rhs * a.bpr;
+  st += rhs;
   if (load_done(st)) return;
+  dE += rhs * a.fstride;
+  if (src) src += rhs * a.fstride;
+  T += rhs * a.fstride;
   extern __shared__ float2 sm[];
   const int tid = threadIdx.x, nthr = blockDim.x;
   const Geom& g = a.g;
@@ -155,14 +165,14 @@ __global__ void __launch_bounds__(512, 1) k_fwd_inner(InnerArgs a, const float2*
   int ncol, plane = 0, rank = 0, x0 = 0, z = 0;
   long long colbase;
   if (a.mode3d) {
-    rank = blockIdx.x % a.csize;
-    plane = blockIdx.x / a.csize;
+    rank = bid % a.csize;
+    plane = bid / a.csize;
     ncol = g.nx / a.csize;
     x0 = rank * ncol;
     z = plane % g.nz;
     colbase = (long long)plane * g.nx + x0;
   } else {
-    colbase = (long long)blockIdx.x * a.ncols;
+    colbase = (long long)bid * a.ncols;
     ncol = (int)min((long long)a.ncols, (long long)g.nx * g.nc - colbase);
   }
   const int m = ncol * ny;
@@ -199,14 +209,17 @@ __global__ void __launch_bounds__(512, 1) k_fwd_inner(InnerArgs a, const float2*
 // K2 -------------------------------------------------------------------------
 template <int EMAX, int RSET>
 __global__ void __launch_bounds__(512, 1) k_outer(OuterArgs a, float2* __restrict__ T, const DevState* __restrict__ st) {
+  const int rhs = blockIdx.x / a.bpr, bid = blockIdx.x - rhs * a.bpr;
+  st += rhs;
   if (load_done(st)) return;
+  T += rhs * a.fstride;
   extern __shared__ float2 sm[];
   const int tid = threadIdx.x, nthr = blockDim.x;
   const Geom& g = a.g;
   const int ty = a.ty, nc = g.nc;
   const int nyt = (g.ny + ty - 1) / ty;
-  const int yt = blockIdx.x % nyt;
-  const int mid = a.mode3d ? blockIdx.x / nyt : 0;
+  const int yt = bid % nyt;
+  const int mid = a.mode3d ? bid / nyt : 0;
   const int y0 = yt * ty;
   const int no = a.mode3d ? g.nz : g.nx;
   const long long ps = a.mode3d ? (long long)g.ny * g.nx : (long long)g.ny;
@@ -300,7 +313,13 @@ template <int EMAX, int RSET>
 __global__ void __launch_bounds__(512, 1) k_inv_inner(InnerArgs a, const float2* __restrict__ T, float2* __restrict__ dE,
                                                     float2* __restrict__ E, const float2* __restrict__ gamma,
                                                     const DevState* __restrict__ st, double* __restrict__ partials) {
+  const int rhs = blockIdx.x / a.bpr, bid = blockIdx.x - rhs * a.bpr;
+  st += rhs;
   if (load_done(st)) return;
+  T += rhs * a.fstride;
+  dE += rhs * a.fstride;
+  E += rhs * a.fstride;
+  partials += (long long)rhs * a.bpr;
   extern __shared__ float2 sm[];
   __shared__ float red[32];
   const int tid = threadIdx.x, nthr = blockDim.x;
@@ -309,15 +328,15 @@ __global__ void __launch_bounds__(512, 1) k_inv_inner(InnerArgs a, const float2*
   int ncol, plane = 0, rank = 0, x0 = 0, z = 0, comp = 0;
   long long colbase;
   if (a.mode3d) {
-    rank = blockIdx.x % a.csize;
-    plane = blockIdx.x / a.csize;
+    rank = bid % a.csize;
+    plane = bid / a.csize;
     ncol = g.nx / a.csize;
     x0 = rank * ncol;
     z = plane % g.nz;
     comp = plane / g.nz;
     colbase = (long long)plane * g.nx + x0;
   } else {
-    colbase = (long long)blockIdx.x * a.ncols;
+    colbase = (long long)bid * a.ncols;
     ncol = (int)min((long long)a.ncols, (long long)g.nx * g.nc - colbase);
   }
   const int m = ncol * ny;
@@ -377,7 +396,7 @@ __global__ void __launch_bounds__(512, 1) k_inv_inner(InnerArgs a, const float2*
     float v = tid < (nthr + 31) / 32 ? red[tid] : 0.f;
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-    if (tid == 0) partials[blockIdx.x] = (double)v;
+    if (tid == 0) partials[bid] = (double)v;
   }
 }
 
@@ -386,6 +405,11 @@ __global__ void __launch_bounds__(512, 1) k_inv_inner(InnerArgs a, const float2*
 // Simulation.next (Simulation.m:193-217).  One block.
 static __global__ void __launch_bounds__(256) k_finish_iteration(DevState* st, StopRule rule, Hist h,
                                                           const double* __restrict__ partials, int nparts) {
+  const int rhs = blockIdx.x;  // one block per right-hand side
+  st += rhs;
+  partials += (long long)rhs * nparts;
+  h.diff += rhs * h.stride;
+  if (h.fresh) h.fresh += rhs * h.stride;
   if (load_done(st)) return;
   __shared__ double red[256];
   double acc = 0.0;
@@ -403,29 +427,33 @@ static __global__ void __launch_bounds__(256) k_finish_iteration(DevState* st, S
 }
 
 // Helpers --------------------------------------------------------------------
-static __global__ void k_reset_state(DevState* st) {
-  if (threadIdx.x == 0 && blockIdx.x == 0) {
-    st->it = 1;
-    st->done = 0;
-    st->converged = 0;
-    st->calc_energy = 1;
-    st->status = 0;
-    st->blocks_done = 0;
-    st->cycles = 0;
-    st->e_acc = 0.0;
-    st->last_step_energy = __longlong_as_double(0x7ff0000000000000LL);  // inf (Simulation.m:169)
-    st->diff1 = 0.0;
+static __global__ void k_reset_state(DevState* st, int n) {
+  for (int i = threadIdx.x; i < n; i += blockDim.x) {
+    DevState* s = st + i;
+    s->it = 1;
+    s->done = 0;
+    s->converged = 0;
+    s->calc_energy = 1;
+    s->status = 0;
+    s->blocks_done = 0;
+    s->cycles = 0;
+    s->e_acc = 0.0;
+    s->last_step_energy = __longlong_as_double(0x7ff0000000000000LL);  // inf (Simulation.m:169)
+    s->diff1 = 0.0;
   }
 }
 
 // Runs after each wiggle cycle of the graph: continues the device-side while
 // loop only if the stop rule has not fired and fewer than max_cycles cycles
 // have run, so the loop ends even if the stop logic were never reached.
-static __global__ void k_cycle_guard(DevState* st, cudaGraphConditionalHandle cond, long long max_cycles) {
+static __global__ void k_cycle_guard(DevState* st, int n, cudaGraphConditionalHandle cond, long long max_cycles) {
   if (threadIdx.x == 0 && blockIdx.x == 0) {
     const long long c = ++st->cycles;
-    const bool go = !st->done && c < max_cycles;
-    if (!go) st->done = 1;
+    bool any = false;
+    for (int i = 0; i < n; ++i) any |= !st[i].done;
+    const bool go = any && c < max_cycles;
+    if (!go)
+      for (int i = 0; i < n; ++i) st[i].done = 1;
     cudaGraphSetConditional(cond, go ? 1u : 0u);
   }
 }

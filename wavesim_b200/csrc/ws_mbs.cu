@@ -209,6 +209,7 @@ static int make_layout(const Geom& g, Layout& L, std::string& why) {
     for (const FastPencil& f : fast_pencil_table())
       if (f.no == no && g.ny % f.ty == 0) L.fp = &f;
   }
+  if (L.fp) L.grid_outer = (long long)(g.ny / L.fp->ty) * mids;  // blocks of the fast pencil kernel
   return WS_OK;
 }
 
@@ -218,10 +219,10 @@ static int make_layout(const Geom& g, Layout& L, std::string& why) {
 struct GraphKey {
   double threshold = -1;
   long long max_iter = -1;
-  int interval = -1, stop_rule = -1, nan_stop = -1;
+  int interval = -1, stop_rule = -1, nan_stop = -1, nrhs = -1;
   bool operator==(const GraphKey& o) const {
     return threshold == o.threshold && max_iter == o.max_iter && interval == o.interval &&
-           stop_rule == o.stop_rule && nan_stop == o.nan_stop;
+           stop_rule == o.stop_rule && nan_stop == o.nan_stop && nrhs == o.nrhs;
   }
 };
 
@@ -237,7 +238,10 @@ struct Solver {
   float* d_wigf = nullptr;   // all pxe/pye/pze
   float2* d_wigc = nullptr;  // all gx/gy/gz
   float2* d_gamma = nullptr;
+  // per right-hand side (batch of nrhs, capacity batch_cap): fields at r * field elements
   float2 *d_E = nullptr, *d_dE = nullptr, *d_T = nullptr, *d_src = nullptr;
+  int batch_cap = 0;
+  int nrhs = 1;
   float2* d_stage = nullptr;
   size_t stage_cap = 0;
   float2* d_out = nullptr;
@@ -327,6 +331,8 @@ static int set_kernel_attributes() {
   for (const FastInner& f : fast_inner_table()) {
     WS_CUDA(allow_dynamic_smem(f.fwd, optin));
     WS_CUDA(allow_dynamic_smem(f.inv, optin));
+    WS_CUDA(cudaFuncSetAttribute(f.fwd, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
+    WS_CUDA(cudaFuncSetAttribute(f.inv, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
   }
   for (const FastPencil& f : fast_pencil_table()) WS_CUDA(allow_dynamic_smem(f.fn, optin));
   if (dev < 31) done_mask |= 1 << dev;
@@ -362,6 +368,37 @@ static int check_args(const int64_t N[4], int64_t n_wiggles, const ws_wiggle* wi
 }
 
 static cudaMemcpyKind kind_from(int memory) { return memory == WS_DEVICE ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice; }
+
+static size_t field_elems(const Solver* s) { return (size_t)s->g.npts * s->g.nc; }
+
+// Buffers for nrhs right-hand sides (kept when large enough).
+static int ensure_batch(Solver* s, int nrhs) {
+  if (nrhs <= s->batch_cap) return WS_OK;
+  void* old[] = {s->d_E, s->d_dE, s->d_T, s->d_src, s->d_state, s->d_energy, s->d_partials};
+  for (void* p : old)
+    if (p) cudaFree(p);
+  s->d_E = s->d_dE = s->d_T = s->d_src = nullptr;
+  s->d_state = nullptr;
+  s->d_energy = s->d_partials = nullptr;
+  s->batch_cap = 0;
+  if (s->d_hist) cudaFree(s->d_hist);
+  s->d_hist = nullptr;
+  s->hist_cap = 0;
+  free_graph(s);
+  const size_t nb = field_elems(s) * nrhs * sizeof(float2);
+  WS_CUDA(cudaMalloc(&s->d_E, nb));
+  WS_CUDA(cudaMalloc(&s->d_dE, nb));
+  WS_CUDA(cudaMalloc(&s->d_T, nb));
+  WS_CUDA(cudaMalloc(&s->d_src, nb));
+  WS_CUDA(cudaMalloc(&s->d_state, nrhs * sizeof(DevState)));
+  WS_CUDA(cudaMalloc(&s->d_energy, nrhs * sizeof(double)));
+  WS_CUDA(cudaMalloc(&s->d_partials, (size_t)std::max<long long>(1, s->lay.grid_inner) * nrhs * sizeof(double)));
+  WS_CUDA(cudaMemset(s->d_E, 0, nb));
+  WS_CUDA(cudaMemset(s->d_dE, 0, nb));
+  WS_CUDA(cudaMemset(s->d_state, 0, nrhs * sizeof(DevState)));
+  s->batch_cap = nrhs;
+  return WS_OK;
+}
 
 static int create_solver(const int64_t N[4], const ws_complex* gamma, int64_t n_wiggles, const ws_wiggle* wiggles,
                          float epsilon, ws_complex k02e, const int64_t roi[8], int memory, int device, Solver** out) {
@@ -436,19 +473,14 @@ static int create_solver(const int64_t N[4], const ws_complex* gamma, int64_t n_
     WS_TRY(cudaMemcpy(c + g.nx + g.ny, W.gz, g.nz * sizeof(float2), kind));
     s->wig.push_back(Wig{f, f + g.nx, f + g.nx + g.ny, c, c + g.nx, c + g.nx + g.ny});
   }
-  const size_t nbytes = (size_t)g.npts * g.nc * sizeof(float2);
   WS_TRY(cudaMalloc(&s->d_gamma, (size_t)g.npts * sizeof(float2)));
   WS_TRY(cudaMemcpy(s->d_gamma, gamma, (size_t)g.npts * sizeof(float2), kind));
-  WS_TRY(cudaMalloc(&s->d_E, nbytes));
-  WS_TRY(cudaMalloc(&s->d_dE, nbytes));
-  WS_TRY(cudaMalloc(&s->d_T, nbytes));
-  WS_TRY(cudaMalloc(&s->d_src, nbytes));
-  WS_TRY(cudaMalloc(&s->d_state, sizeof(DevState)));
-  WS_TRY(cudaMalloc(&s->d_energy, sizeof(double)));
-  WS_TRY(cudaMalloc(&s->d_partials, (size_t)std::max<long long>(1, s->lay.grid_inner) * sizeof(double)));
-  WS_TRY(cudaMemset(s->d_E, 0, nbytes));
-  WS_TRY(cudaMemset(s->d_dE, 0, nbytes));
 #undef WS_TRY
+  const int rc2 = ensure_batch(s, 1);
+  if (rc2) {
+    destroy_solver(s);
+    return rc2;
+  }
   *out = s;
   return WS_OK;
 }
@@ -463,6 +495,8 @@ static InnerArgs inner_args(const Solver* s, int w) {
   a.csize = s->lay.csize;
   a.mode3d = s->lay.mode3d;
   a.ncols = s->lay.ncols;
+  a.bpr = (int)s->lay.grid_inner;
+  a.fstride = (long long)field_elems(s);
   return a;
 }
 
@@ -475,6 +509,8 @@ static OuterArgs outer_args(const Solver* s, int w) {
   a.norm = (float)(1.0 / ((double)s->g.npts));
   a.ty = s->lay.ty;
   a.mode3d = s->lay.mode3d;
+  a.bpr = (int)s->lay.grid_outer;
+  a.fstride = (long long)field_elems(s);
   return a;
 }
 
@@ -482,7 +518,7 @@ template <int RS>
 static cudaError_t launch_k1_t(const Solver* s, int w, bool with_source) {
   const float2 A = make_float2(0.f, (float)(1.0f / s->eps / (float)s->nw));  // 1i/epsilon/Nwiggles
   cudaLaunchConfig_t cfg{};
-  cfg.gridDim = dim3((unsigned)s->lay.grid_inner);
+  cfg.gridDim = dim3((unsigned)(s->lay.grid_inner * s->nrhs));
   cfg.blockDim = dim3(s->lay.th_inner);
   cfg.dynamicSmemBytes = s->lay.smem_inner;
   cfg.stream = s->stream;
@@ -500,7 +536,7 @@ static cudaError_t launch_k1_t(const Solver* s, int w, bool with_source) {
 
 template <int RS>
 static cudaError_t launch_k2_t(const Solver* s, int w) {
-  k_outer<kEmax, RS><<<(unsigned)s->lay.grid_outer, s->lay.th_outer, s->lay.smem_outer, s->stream>>>(
+  k_outer<kEmax, RS><<<(unsigned)(s->lay.grid_outer * s->nrhs), s->lay.th_outer, s->lay.smem_outer, s->stream>>>(
       outer_args(s, w), s->d_T, s->d_state);
   return cudaGetLastError();
 }
@@ -508,7 +544,7 @@ static cudaError_t launch_k2_t(const Solver* s, int w) {
 template <int RS>
 static cudaError_t launch_k3_t(const Solver* s, int w) {
   cudaLaunchConfig_t cfg{};
-  cfg.gridDim = dim3((unsigned)s->lay.grid_inner);
+  cfg.gridDim = dim3((unsigned)(s->lay.grid_inner * s->nrhs));
   cfg.blockDim = dim3(s->lay.th_inner);
   cfg.dynamicSmemBytes = s->lay.smem_inner;
   cfg.stream = s->stream;
@@ -530,7 +566,7 @@ static size_t fast_inner_smem(const Solver* s) {
 
 static cudaError_t launch_fast_inner(const Solver* s, const void* fn, void** args) {
   cudaLaunchConfig_t cfg{};
-  cfg.gridDim = dim3((unsigned)s->lay.grid_inner);
+  cfg.gridDim = dim3((unsigned)(s->lay.grid_inner * s->nrhs));
   cfg.blockDim = dim3(fast::kThreads);
   cfg.dynamicSmemBytes = fast_inner_smem(s);
   cfg.stream = s->stream;
@@ -564,7 +600,8 @@ static cudaError_t launch_k2(const Solver* s, int w) {
     const FastPencil* f = s->lay.fp;
     const int th = f->ty * (f->no / 16);
     const long long mids = s->lay.mode3d ? s->g.nx : 1;
-    const unsigned grid = (unsigned)((s->g.ny / f->ty) * mids);
+    const unsigned grid = (unsigned)(s->lay.grid_outer * s->nrhs);
+    (void)mids;
     const size_t smem = (size_t)(f->ty + 1) * f->no * sizeof(float2);
     float2* T = s->d_T;
     const DevState* st = s->d_state;
@@ -593,7 +630,7 @@ static cudaError_t launch_k3_only(const Solver* s, int w) {
 }
 
 static cudaError_t launch_finish(const Solver* s, const StopRule& rule, const Hist& h) {
-  k_finish_iteration<<<1, 256, 0, s->stream>>>(s->d_state, rule, h, s->d_partials, (int)s->lay.grid_inner);
+  k_finish_iteration<<<s->nrhs, 256, 0, s->stream>>>(s->d_state, rule, h, s->d_partials, (int)s->lay.grid_inner);
   return cudaGetLastError();
 }
 
@@ -613,13 +650,14 @@ static cudaError_t launch_iteration(const Solver* s, int it0, bool with_source, 
   return launch_k3(s, w, rule, h);
 }
 
+// Energy histories: per right-hand side r, diff at r * 2cap and fresh at r * 2cap + cap.
 static int ensure_hist(Solver* s, long long cap) {
   if (s->hist_cap >= cap) return WS_OK;
   if (s->d_hist) cudaFree(s->d_hist);
   s->d_hist = nullptr;
   s->hist_cap = 0;
   free_graph(s);  // graphs hold the old pointer
-  WS_CUDA(cudaMalloc(&s->d_hist, 2 * cap * sizeof(double)));
+  WS_CUDA(cudaMalloc(&s->d_hist, 2 * cap * std::max(1, s->batch_cap) * sizeof(double)));
   s->hist_cap = cap;
   return WS_OK;
 }
@@ -640,13 +678,13 @@ static int build_graph(Solver* s, const StopRule& rule, const Hist& h) {
   // prologue + first cycle (with the source)
   e = cudaStreamBeginCaptureToGraph(s->stream, graph, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal);
   if (e == cudaSuccess) {
-    const size_t nbytes = (size_t)s->g.npts * s->g.nc * sizeof(float2);
+    const size_t nbytes = field_elems(s) * s->nrhs * sizeof(float2);
     cudaMemsetAsync(s->d_E, 0, nbytes, s->stream);
     cudaMemsetAsync(s->d_dE, 0, nbytes, s->stream);
-    k_reset_state<<<1, 32, 0, s->stream>>>(s->d_state);
+    k_reset_state<<<1, 256, 0, s->stream>>>(s->d_state, s->nrhs);
     for (int i = 0; i < s->nw && e == cudaSuccess; ++i) e = launch_iteration(s, i, true, rule, h);
     if (e == cudaSuccess) {
-      k_cycle_guard<<<1, 32, 0, s->stream>>>(s->d_state, cond, max_cycles);
+      k_cycle_guard<<<1, 32, 0, s->stream>>>(s->d_state, s->nrhs, cond, max_cycles);
       e = cudaGetLastError();
     }
     cudaGraph_t g2 = graph;
@@ -684,7 +722,7 @@ static int build_graph(Solver* s, const StopRule& rule, const Hist& h) {
   if (e == cudaSuccess) {
     for (int i = 0; i < s->nw && e == cudaSuccess; ++i) e = launch_iteration(s, i, false, rule, h);
     if (e == cudaSuccess) {
-      k_cycle_guard<<<1, 32, 0, s->stream>>>(s->d_state, cond, max_cycles);
+      k_cycle_guard<<<1, 32, 0, s->stream>>>(s->d_state, s->nrhs, cond, max_cycles);
       e = cudaGetLastError();
     }
     cudaGraph_t b2 = body;
@@ -705,13 +743,18 @@ static int build_graph(Solver* s, const StopRule& rule, const Hist& h) {
   return WS_OK;
 }
 
-static int upload_source(Solver* s, int64_t n_blocks, const ws_source_block* src, int memory, double* energy) {
+// Source.add_to for every block of every right-hand side into the dense
+// source fields (r at r * field elements); source energies into energy[r].
+static int upload_sources(Solver* s, int nrhs, const int64_t* counts, const ws_source_block* src, int memory,
+                          std::vector<double>& energy) {
   const Geom& g = s->g;
-  const size_t nbytes = (size_t)g.npts * g.nc * sizeof(float2);
-  WS_CUDA(cudaMemsetAsync(s->d_src, 0, nbytes, s->stream));
-  WS_CUDA(cudaMemsetAsync(s->d_energy, 0, sizeof(double), s->stream));
+  const size_t F = field_elems(s);
+  WS_CUDA(cudaMemsetAsync(s->d_src, 0, F * nrhs * sizeof(float2), s->stream));
+  WS_CUDA(cudaMemsetAsync(s->d_energy, 0, nrhs * sizeof(double), s->stream));
   size_t need = 0;
-  for (int64_t b = 0; b < n_blocks; ++b) {
+  long long total = 0;
+  for (int r = 0; r < nrhs; ++r) total += counts[r];
+  for (long long b = 0; b < total; ++b) {
     const ws_source_block& B = src[b];
     size_t n = 1;
     for (int d = 0; d < 4; ++d) {
@@ -730,42 +773,65 @@ static int upload_source(Solver* s, int64_t n_blocks, const ws_source_block* src
     WS_CUDA(cudaMalloc(&s->d_stage, need * sizeof(float2)));
     s->stage_cap = need;
   }
-  for (int64_t b = 0; b < n_blocks; ++b) {
-    const ws_source_block& B = src[b];
-    const size_t n = (size_t)(B.size[0] * B.size[1] * B.size[2] * B.size[3]);
-    const float2* vals = (const float2*)B.values;
-    if (memory != WS_DEVICE) {
-      WS_CUDA(cudaMemcpyAsync(s->d_stage, B.values, n * sizeof(float2), cudaMemcpyHostToDevice, s->stream));
-      vals = s->d_stage;
+  long long b = 0;
+  for (int r = 0; r < nrhs; ++r) {
+    for (int64_t k = 0; k < counts[r]; ++k, ++b) {
+      const ws_source_block& B = src[b];
+      const size_t n = (size_t)(B.size[0] * B.size[1] * B.size[2] * B.size[3]);
+      const float2* vals = (const float2*)B.values;
+      if (memory != WS_DEVICE) {
+        WS_CUDA(cudaMemcpyAsync(s->d_stage, B.values, n * sizeof(float2), cudaMemcpyHostToDevice, s->stream));
+        vals = s->d_stage;
+      }
+      const int th = 256;
+      const long long blocks = std::min<long long>((n + th - 1) / th, 4096);
+      k_scatter_source<<<(unsigned)std::max(1LL, blocks), th, 0, s->stream>>>(
+          s->d_src + F * r, vals, g, (int)B.position[0] - 1, (int)B.position[1] - 1, (int)B.position[2] - 1,
+          (int)B.position[3] - 1, (int)B.size[0], (int)B.size[1], (int)B.size[2], (int)B.size[3], s->d_energy + r);
+      WS_CUDA(cudaGetLastError());
+      if (memory != WS_DEVICE) WS_CUDA(cudaStreamSynchronize(s->stream));  // staging buffer reuse
     }
-    const int th = 256;
-    const long long blocks = std::min<long long>((n + th - 1) / th, 4096);
-    k_scatter_source<<<(unsigned)std::max(1LL, blocks), th, 0, s->stream>>>(
-        s->d_src, vals, g, (int)B.position[0] - 1, (int)B.position[1] - 1, (int)B.position[2] - 1,
-        (int)B.position[3] - 1, (int)B.size[0], (int)B.size[1], (int)B.size[2], (int)B.size[3], s->d_energy);
-    WS_CUDA(cudaGetLastError());
-    if (memory != WS_DEVICE) WS_CUDA(cudaStreamSynchronize(s->stream));  // staging buffer reuse
   }
-  WS_CUDA(cudaMemcpyAsync(energy, s->d_energy, sizeof(double), cudaMemcpyDeviceToHost, s->stream));
+  energy.assign(nrhs, 0.0);
+  WS_CUDA(cudaMemcpyAsync(energy.data(), s->d_energy, nrhs * sizeof(double), cudaMemcpyDeviceToHost, s->stream));
   WS_CUDA(cudaStreamSynchronize(s->stream));
   return WS_OK;
 }
 
-static int solve(Solver* s, int64_t n_blocks, const ws_source_block* src, int source_memory,
-                 const ws_solve_options* o, ws_complex* E_out, int out_memory, double* diff_out, int64_t* n_it,
-                 int* converged) {
+static size_t roi_elems(const Geom& g) {
+  return (size_t)(g.r1[0] - g.r0[0]) * (g.r1[1] - g.r0[1]) * (g.r1[2] - g.r0[2]) * (g.r1[3] - g.r0[3]);
+}
+
+// One batch of nrhs right-hand sides on the solver's medium.  Each one follows
+// the reference loop and stop rule on its own; a converged one stops working
+// while the others continue.
+static int solve_batch(Solver* s, int nrhs, const int64_t* counts, const ws_source_block* src, int source_memory,
+                       const ws_solve_options* o, ws_complex* E_out, int out_memory, double* diff_out,
+                       int64_t diff_cap, int64_t* n_it, int* converged) {
   WS_CUDA(cudaSetDevice(s->device));
   ws_solve_options opt;
   ws_default_options(&opt);
   if (o) opt = *o;
+  if (nrhs < 1 || nrhs > 65536) return fail(WS_ERR_INVALID_ARGUMENT, "number of right-hand sides must be in [1, 65536]");
   if (opt.max_iterations < 1 || opt.max_iterations > 100000000LL)
     return fail(WS_ERR_INVALID_ARGUMENT, "max_iterations must be in [1, 1e8]");
   if (opt.energy_interval < 1) return fail(WS_ERR_INVALID_ARGUMENT, "energy_interval must be >= 1");
-  if (n_blocks < 1 || !src) return fail(WS_ERR_NO_SOURCE, "no source blocks");
-  double src_energy = 0;
-  int rc = upload_source(s, n_blocks, src, source_memory, &src_energy);
+  if (!counts || !src) return fail(WS_ERR_NO_SOURCE, "no source blocks");
+  for (int r = 0; r < nrhs; ++r)
+    if (counts[r] < 1) return fail(WS_ERR_NO_SOURCE, "a right-hand side has no source blocks");
+  const bool want_cb = opt.callback && opt.callback_type && std::strcmp(opt.callback_type, "NoCallback") != 0;
+  if (want_cb && nrhs > 1) return fail(WS_ERR_INVALID_ARGUMENT, "callbacks need a single right-hand side");
+  if (s->lay.grid_inner * (long long)nrhs > (1LL << 31) - 1 || s->lay.grid_outer * (long long)nrhs > (1LL << 31) - 1)
+    return fail(WS_ERR_INVALID_ARGUMENT, "batch too large for one launch");
+  int rc = ensure_batch(s, nrhs);
   if (rc) return rc;
-  if (!(src_energy > 0)) return fail(WS_ERR_NO_SOURCE, "There is no source inside the grid boundaries");
+  if (s->nrhs != nrhs) free_graph(s);
+  s->nrhs = nrhs;
+  std::vector<double> src_energy;
+  rc = upload_sources(s, nrhs, counts, src, source_memory, src_energy);
+  if (rc) return rc;
+  for (int r = 0; r < nrhs; ++r)
+    if (!(src_energy[r] > 0)) return fail(WS_ERR_NO_SOURCE, "There is no source inside the grid boundaries");
   // the loop can run at most max_iterations + Nw - 1 iterations
   const long long cap = opt.max_iterations + s->nw;
   rc = ensure_hist(s, cap);
@@ -777,10 +843,11 @@ static int solve(Solver* s, int64_t n_blocks, const ws_source_block* src, int so
   rule.interval = (int)std::min<int64_t>(opt.energy_interval, 1 << 30);
   rule.max_iter = opt.max_iterations;
   rule.threshold = opt.energy_threshold;
-  Hist h{s->d_hist, s->d_hist + cap, cap};
-  const bool want_cb = opt.callback && opt.callback_type && std::strcmp(opt.callback_type, "NoCallback") != 0;
+  const long long hs_stride = 2 * s->hist_cap;
+  Hist h{s->d_hist, s->d_hist + s->hist_cap, s->hist_cap, hs_stride};
+  std::vector<DevState> hs(nrhs);
   if (opt.use_graph && !want_cb) {
-    GraphKey key{rule.threshold, rule.max_iter, rule.interval, opt.stop_rule, rule.nan_stop};
+    GraphKey key{rule.threshold, rule.max_iter, rule.interval, opt.stop_rule, rule.nan_stop, nrhs};
     if (!s->gexec || !(key == s->gkey)) {
       rc = build_graph(s, rule, h);
       if (rc) return rc;
@@ -788,14 +855,13 @@ static int solve(Solver* s, int64_t n_blocks, const ws_source_block* src, int so
     }
     WS_CUDA(cudaGraphLaunch(s->gexec, s->stream));
   } else {
-    const size_t nbytes = (size_t)s->g.npts * s->g.nc * sizeof(float2);
+    const size_t nbytes = field_elems(s) * nrhs * sizeof(float2);
     WS_CUDA(cudaMemsetAsync(s->d_E, 0, nbytes, s->stream));
     WS_CUDA(cudaMemsetAsync(s->d_dE, 0, nbytes, s->stream));
-    k_reset_state<<<1, 32, 0, s->stream>>>(s->d_state);
+    k_reset_state<<<1, 256, 0, s->stream>>>(s->d_state, nrhs);
     std::vector<double> hist;
     long long it = 0;
     const long long cb_int = std::max<int64_t>(1, opt.callback_interval);
-    DevState hs{};
     const long long max_cycles = (rule.max_iter + s->nw - 1) / s->nw + 1;
     for (long long cycle = 0;; ++cycle) {
       if (cycle >= max_cycles) return fail(WS_ERR_CUDA, "loop did not stop within max_iterations (internal error)");
@@ -803,57 +869,76 @@ static int solve(Solver* s, int64_t n_blocks, const ws_source_block* src, int so
         WS_CUDA(launch_iteration(s, (int)(it % s->nw), it < s->nw, rule, h));
         ++it;
       }
-      WS_CUDA(cudaMemcpyAsync(&hs, s->d_state, sizeof(DevState), cudaMemcpyDeviceToHost, s->stream));
+      WS_CUDA(cudaMemcpyAsync(hs.data(), s->d_state, nrhs * sizeof(DevState), cudaMemcpyDeviceToHost, s->stream));
       WS_CUDA(cudaStreamSynchronize(s->stream));
-      const long long done_it = hs.it - 1;
       if (want_cb) {
+        const long long done_it = hs[0].it - 1;
         hist.resize(done_it);
         WS_CUDA(cudaMemcpy(hist.data(), s->d_hist, done_it * sizeof(double), cudaMemcpyDeviceToHost));
         for (long long k = done_it - s->nw + 1; k <= done_it; ++k)
-          if (k >= 1 && (k % cb_int == 0 || (hs.done && k == done_it)))
+          if (k >= 1 && (k % cb_int == 0 || (hs[0].done && k == done_it)))
             opt.callback(opt.callback_type, hist.data(), k, opt.energy_threshold, opt.user_data);
       }
-      if (hs.done) break;
+      bool all = true;
+      for (const DevState& d : hs) all = all && d.done;
+      if (all) break;
     }
   }
-  DevState hs{};
-  WS_CUDA(cudaMemcpyAsync(&hs, s->d_state, sizeof(DevState), cudaMemcpyDeviceToHost, s->stream));
+  WS_CUDA(cudaMemcpyAsync(hs.data(), s->d_state, nrhs * sizeof(DevState), cudaMemcpyDeviceToHost, s->stream));
   WS_CUDA(cudaStreamSynchronize(s->stream));
-  const long long n_iter = hs.it - 1;
-  if (n_it) *n_it = n_iter;
-  if (converged) *converged = hs.converged;
-  if (diff_out && n_iter > 0)
-    WS_CUDA(cudaMemcpy(diff_out, s->d_hist, std::min(n_iter, cap) * sizeof(double), cudaMemcpyDeviceToHost));
+  bool diverged = false;
+  for (int r = 0; r < nrhs; ++r) {
+    const long long n_iter = hs[r].it - 1;
+    if (n_it) n_it[r] = n_iter;
+    if (converged) converged[r] = hs[r].converged;
+    diverged = diverged || hs[r].status == WS_ERR_DIVERGED;
+    if (diff_out && n_iter > 0)
+      WS_CUDA(cudaMemcpy(diff_out + r * diff_cap, s->d_hist + r * hs_stride,
+                         std::min<long long>(std::min(n_iter, cap), diff_cap) * sizeof(double),
+                         cudaMemcpyDeviceToHost));
+  }
   if (E_out) {
     const Geom& g = s->g;
     const cudaMemcpyKind k = out_memory == WS_DEVICE ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost;
+    const size_t F = field_elems(s);
     if (opt.output == WS_OUTPUT_FIELD) {
-      const size_t n = (size_t)(g.r1[0] - g.r0[0]) * (g.r1[1] - g.r0[1]) * (g.r1[2] - g.r0[2]) * (g.r1[3] - g.r0[3]);
-      float2* dst = (float2*)E_out;
-      if (out_memory != WS_DEVICE) {
-        if (n > s->out_cap) {
-          if (s->d_out) cudaFree(s->d_out);
-          s->d_out = nullptr;
-          s->out_cap = 0;
-          WS_CUDA(cudaMalloc(&s->d_out, n * sizeof(float2)));
-          s->out_cap = n;
+      const size_t n = roi_elems(g);
+      for (int r = 0; r < nrhs; ++r) {
+        float2* dst = (float2*)E_out + n * r;
+        if (out_memory != WS_DEVICE) {
+          if (n > s->out_cap) {
+            if (s->d_out) cudaFree(s->d_out);
+            s->d_out = nullptr;
+            s->out_cap = 0;
+            WS_CUDA(cudaMalloc(&s->d_out, n * sizeof(float2)));
+            s->out_cap = n;
+          }
+          dst = s->d_out;
         }
-        dst = s->d_out;
+        const long long blocks = std::min<long long>(((long long)n + 255) / 256, 8 * kNumSms);
+        k_finalize<<<(unsigned)blocks, 256, 0, s->stream>>>(s->d_E + F * r, s->d_gamma, g, dst);
+        WS_CUDA(cudaGetLastError());
+        if (out_memory != WS_DEVICE)
+          WS_CUDA(cudaMemcpyAsync((float2*)E_out + n * r, s->d_out, n * sizeof(float2), k, s->stream));
+        WS_CUDA(cudaStreamSynchronize(s->stream));
       }
-      const long long blocks = std::min<long long>(((long long)n + 255) / 256, 8 * kNumSms);
-      k_finalize<<<(unsigned)blocks, 256, 0, s->stream>>>(s->d_E, s->d_gamma, g, dst);
-      WS_CUDA(cudaGetLastError());
-      if (out_memory != WS_DEVICE) WS_CUDA(cudaMemcpyAsync(E_out, s->d_out, n * sizeof(float2), k, s->stream));
     } else {
-      WS_CUDA(cudaMemcpyAsync(E_out, s->d_E, (size_t)g.npts * g.nc * sizeof(float2), k, s->stream));
+      WS_CUDA(cudaMemcpyAsync(E_out, s->d_E, F * nrhs * sizeof(float2), k, s->stream));
     }
     WS_CUDA(cudaStreamSynchronize(s->stream));
   }
-  if (!want_cb && opt.callback && opt.callback_type && std::strcmp(opt.callback_type, "NoCallback") != 0) {
-    // unreachable (want_cb covers it); kept for clarity of the contract
-  }
-  if (hs.status == WS_ERR_DIVERGED) return fail(WS_ERR_DIVERGED, "residual energy is not finite");
+  if (diverged) return fail(WS_ERR_DIVERGED, "residual energy is not finite");
   return WS_OK;
+}
+
+static int solve(Solver* s, int64_t n_blocks, const ws_source_block* src, int source_memory,
+                 const ws_solve_options* o, ws_complex* E_out, int out_memory, double* diff_out, int64_t* n_it,
+                 int* converged) {
+  if (n_blocks < 1 || !src) return fail(WS_ERR_NO_SOURCE, "no source blocks");
+  const int64_t counts[1] = {n_blocks};
+  const int64_t maxit = o ? o->max_iterations : 100000;
+  return solve_batch(s, 1, counts, src, source_memory, o, E_out, out_memory, diff_out, maxit + s->nw, n_it,
+                     converged);
 }
 
 }  // namespace ws
@@ -913,6 +998,14 @@ int ws_solver_solve(ws_solver h, int64_t n_blocks, const ws_source_block* source
                diff_energy_out, n_iterations, converged);
 }
 
+int ws_solver_solve_batch(ws_solver h, int64_t n_rhs, const int64_t* block_counts, const ws_source_block* blocks,
+                          int source_memory, const ws_solve_options* opts, ws_complex* E_out, int out_memory,
+                          double* diff_energy_out, int64_t diff_capacity, int64_t* n_iterations, int* converged) {
+  if (!h) return fail(WS_ERR_INVALID_ARGUMENT, "null solver");
+  return solve_batch(reinterpret_cast<Solver*>(h), (int)n_rhs, block_counts, blocks, source_memory, opts, E_out,
+                     out_memory, diff_energy_out, diff_capacity, n_iterations, converged);
+}
+
 int ws_solver_buffers(ws_solver h, void** E_prime, void** stream) {
   if (!h) return fail(WS_ERR_INVALID_ARGUMENT, "null solver");
   Solver* s = reinterpret_cast<Solver*>(h);
@@ -933,7 +1026,8 @@ int ws_solver_time_kernels(ws_solver h, int n_iterations, float ms_out[3], doubl
     if (rc) return rc;
   }
   StopRule rule{s->nw, 1, 0, 1, (long long)1 << 62, -1.0};
-  Hist hh{s->d_hist, s->d_hist + s->hist_cap, 0};  // cap 0: history untouched
+  Hist hh{s->d_hist, s->d_hist + s->hist_cap, 0, 0};  // cap 0: history untouched
+  s->nrhs = 1;  // time the first right-hand side alone
   k_resume_state<<<1, 32, 0, s->stream>>>(s->d_state);
   float acc[3] = {0, 0, 0};
   for (int i = 0; i < n_iterations; ++i) {

@@ -402,7 +402,7 @@ extern "C" int ws_run_algorithm_noalloc(const int64_t N[4], const ws_complex* ga
   // clear what must start at zero: dE, E (the caller's output), the loop state
   NA_CUDA(cudaMemsetAsync(r.dE, 0, field * sizeof(float2), s));
   NA_CUDA(cudaMemsetAsync(r.E, 0, field * sizeof(float2), s));
-  k_reset_state<<<1, 32, 0, s>>>(r.st);
+  k_reset_state<<<1, 32, 0, s>>>(r.st, 1);
   NA_CUDA(cudaGetLastError());
   Wig wig[64];
   for (int w = 0; w < n_wiggles; ++w) {
@@ -417,12 +417,16 @@ extern "C" int ws_run_algorithm_noalloc(const int64_t N[4], const ws_complex* ga
   r.ia.csize = sh.csize;
   r.ia.mode3d = sh.mode3d;
   r.ia.ncols = sh.ncols;
+  r.ia.bpr = (int)sh.grid_inner;  // a single right-hand side
+  r.ia.fstride = 0;
   r.oa.g = g;
   r.oa.po = po;
   r.oa.k02e = make_float2(k02e.re, k02e.im);
   r.oa.norm = (float)(1.0 / (double)g.npts);
   r.oa.ty = sh.ty;
   r.oa.mode3d = sh.mode3d;
+  r.oa.bpr = (int)sh.grid_outer;
+  r.oa.fstride = 0;
   StopRule rule{};
   rule.nw = (int)n_wiggles;
   rule.fresh = 0;
@@ -430,7 +434,7 @@ extern "C" int ws_run_algorithm_noalloc(const int64_t N[4], const ws_complex* ga
   rule.interval = (int)std::min<int64_t>(energy_interval, 1 << 30);
   rule.max_iter = max_iterations;
   rule.threshold = energy_threshold;
-  Hist h{diff_energy_out, nullptr, max_iterations + n_wiggles};
+  Hist h{diff_energy_out, nullptr, max_iterations + n_wiggles, 0};
   const float2 A = make_float2(0.f, (float)(1.0f / epsilon / (float)n_wiggles));
   const long long max_cycles = (max_iterations + n_wiggles - 1) / n_wiggles + 1;
   DevState hs{};

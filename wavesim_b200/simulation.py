@@ -265,6 +265,63 @@ class WaveSim:
         return np.ascontiguousarray(E), state
 
 
+    def exec_batch(self, sources):
+        """Many sources on this medium in one batched solve (ws_solver_solve_batch).
+
+        Equivalent to ``[self.exec(s) for s in sources]`` - every source runs
+        the reference loop and stop rule on its own - but all of them share the
+        medium's device data and each kernel launch covers the whole batch.
+        Returns (list of E, list of state)."""
+        t0 = time.perf_counter()
+        groups, keep, counts = [], [], []
+        for src in sources:
+            s, blocks, k = self.source_blocks(src)
+            if s.energy() == 0:
+                raise ValueError("a source has no part inside the grid boundaries")
+            groups.append(s)
+            keep.append(k)
+            counts.append(len(s.values))
+        total = sum(counts)
+        blocks = (_lib.ws_source_block * total)()
+        i = 0
+        for s, k in zip(groups, keep):
+            for p, v in zip(s.positions, k):
+                blocks[i] = _lib.ws_source_block((C.c_int64 * 4)(*[int(a) for a in p]),
+                                                 (C.c_int64 * 4)(*[int(a) for a in v.shape]), v.ctypes.data)
+                i += 1
+        h = self.solver()
+        o = _lib.default_options()
+        o.max_iterations = self.max_iterations()
+        o.energy_threshold = self.energy_threshold
+        o.energy_interval = self.energy_calculation_interval
+        o.stop_rule = _lib.WS_STOP_FRESH if self.stop_rule == "fresh" else _lib.WS_STOP_REFERENCE
+        o.output = _lib.WS_OUTPUT_FIELD
+        o.use_graph = 1 if self.use_graph else 0
+        r = self.roi
+        shape = tuple(int(r[1, d] - r[0, d] + 1) for d in range(4))
+        R = len(sources)
+        E = np.empty((R,) + shape[::-1], dtype=np.complex64)  # each field column-major
+        cap = o.max_iterations + len(self.wiggles) + 1
+        hist = np.zeros((R, cap))
+        n_it = np.zeros(R, dtype=np.int64)
+        conv = np.zeros(R, dtype=np.int32)
+        _lib.check(_lib.lib.ws_solver_solve_batch(
+            h, R, (C.c_int64 * R)(*counts), blocks, _lib.WS_HOST, C.byref(o), E.ctypes.data, _lib.WS_HOST,
+            hist.ctypes.data_as(C.POINTER(C.c_double)), cap, n_it.ctypes.data_as(C.POINTER(C.c_int64)),
+            conv.ctypes.data_as(C.POINTER(C.c_int))))
+        del keep
+        dt = time.perf_counter() - t0
+        outs, states = [], []
+        for i in range(R):
+            Ei = np.ascontiguousarray(E[i].transpose(3, 2, 1, 0))  # back to [y, x, z, c]
+            if not self.vector:
+                Ei = Ei[..., 0]
+            outs.append(Ei)
+            states.append(SimpleNamespace(source=groups[i], it=int(n_it[i]) + 1, converged=bool(conv[i]),
+                                          diff_energy=hist[i, :n_it[i]].copy(), time=dt))
+        return outs, states
+
+
 class WaveSimVector(WaveSim):
     """Vector (Maxwell) MBS with the dyadic Green's function (WaveSimVector.m)."""
 
