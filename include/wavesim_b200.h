@@ -103,6 +103,24 @@ typedef struct ws_solve_options {
   int64_t callback_interval;     /* Simulation.callback_interval (default 50) */
   ws_callback_fn callback;       /* may be NULL */
   void* user_data;
+  /* Warm start (no counterpart in the reference).  NULL: the reference's
+   * cold start from zero.  Else one full-grid starting field per right-hand
+   * side (Ny*Nx*Nz*Nc complex, column-major) in initial_memory: the field
+   * psi0 itself, or E' = gamma .* psi0 when initial_is_eprime is 1 (e.g. the
+   * E' output of an earlier solve).  The start enters the loop the way the
+   * reference's source does, spread evenly over the first wiggle cycle
+   * (u/Nw per iteration, u = gamma psi0); a zero start reproduces the cold
+   * loop exactly.  One extra probe iteration, the cold first iteration, runs
+   * first: its energy stays diff_energy(1), the stop rule's denominator.
+   * diff_energy(2..Nw) are energies of the shifted increments dE' + u/Nw. */
+  const ws_complex* initial_field;
+  int initial_memory;            /* WS_HOST or WS_DEVICE */
+  int initial_is_eprime;
+  /* A warm start whose true ROI increment energy at the end of its first
+   * wiggle cycle exceeds warm_discard_ratio x diff_energy(1) stops there,
+   * unconverged and marked discarded (ws_solver_warm_report), to be rerun
+   * cold.  0 keeps every start. */
+  double warm_discard_ratio;
 } ws_solve_options;
 
 typedef struct ws_solver_s* ws_solver;
@@ -188,6 +206,14 @@ int ws_solver_time_kernels(ws_solver s, int n_iterations, float ms_out[3], doubl
 
 /* Number of kernel launches one iteration makes. */
 int ws_solver_launches_per_iteration(ws_solver s);
+
+/* After a warm-started solve of right-hand side `rhs`: the ROI energy of the
+ * cold first increment (diff_energy(1), from the probe iteration), the ROI
+ * energy of the true increment at the end of the warm first wiggle cycle,
+ * and whether the start was discarded there.  Any pointer may be NULL; the
+ * values are -1 / 0 after a cold solve.  No counterpart in the reference. */
+int ws_solver_warm_report(ws_solver s, int64_t rhs, double* cold_first_energy, double* warm_cycle_energy,
+                          int* discarded);
 
 int ws_solver_destroy(ws_solver s);
 

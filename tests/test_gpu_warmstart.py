@@ -1,0 +1,126 @@
+"""Warm-started solves (no counterpart in the reference).  The starting field
+enters the loop spread over the first wiggle cycle, the way the reference's
+source does, so that a zero start is the cold loop itself and a start close
+to the solution stops early at the same energy tolerance, at least as close
+to the loop's limit as the cold solve."""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def rel(a, b):
+    return float(np.linalg.norm(np.ravel(a) - np.ravel(b)) / np.linalg.norm(np.ravel(b)))
+
+
+def _medium():
+    from wavesim_b200.warmstart import sphere_medium
+    return sphere_medium(32, np.random.default_rng(21))
+
+
+def _problem(tol, **kw):
+    import wavesim_b200 as ws
+    opt = {"lambda": 1.0, "pixel_size": 0.25, "boundary_widths": [16, 16, 16], "energy_threshold": tol}
+    opt.update(kw)
+    return ws.WaveSim(_medium(), opt), ws.Source(np.ones((32, 32)), [1, 1, 1])
+
+
+def _psi_full(sim, Ep):
+    """psi0 = E'/gamma on the full grid (zero where gamma vanishes)."""
+    g = sim.gamma
+    return np.where(g != 0, Ep / np.where(g != 0, g, 1), 0).astype(np.complex64)
+
+
+def _smooth_noise(shape, rng, amp, ref):
+    k = [np.fft.fftfreq(n) for n in shape]
+    lp = np.exp(-(k[0][:, None, None] ** 2 + k[1][None, :, None] ** 2 + k[2][None, None, :] ** 2)
+                * (2 * np.pi * 2) ** 2 / 2)
+    z = np.fft.ifftn(np.fft.fftn(rng.standard_normal(shape) + 1j * rng.standard_normal(shape)) * lp)
+    return z * (amp * np.linalg.norm(ref) / np.linalg.norm(z))
+
+
+def test_zero_start_is_the_cold_loop(gpu):
+    sim, src = _problem(1e-4)
+    E, st = sim.exec(src)
+    E0, s0 = sim.exec(src, warm_start=np.zeros_like(E))
+    assert not s0.warm_discarded
+    assert s0.it == st.it
+    assert rel(E0, E) < 1e-6
+    assert s0.diff_energy[0] == st.diff_energy[0]
+    assert s0.cold_first_energy == pytest.approx(st.diff_energy[0], rel=1e-12)
+
+
+def test_converged_start_stops_early(gpu):
+    """From the full-grid field of a tighter solve the loop stops within a
+    few cycles, closer to the loop's limit than the cold solve."""
+    sim, src = _problem(1e-4)
+    E, st = sim.exec(src)
+    Ep, _ = _problem(1e-7)[0].exec(src, output="eprime")
+    Einf, _ = _problem(1e-11)[0].exec(src)
+    Ew, sw = sim.exec(src, warm_start=_psi_full(sim, Ep))
+    nw = len(sim.wiggles)
+    assert not sw.warm_discarded
+    assert sw.it - 1 <= 3 * nw < st.it - 1, (sw.it, st.it)
+    assert rel(Ew, Einf) <= rel(E, Einf) + 1e-4, (rel(Ew, Einf), rel(E, Einf))
+
+
+def test_perturbed_start_is_faster_and_as_accurate(gpu):
+    """A start 5% (smooth, ROI only) away from the limit converges in fewer
+    iterations than the cold start and at least about as close to the limit."""
+    sim, src = _problem(1e-4)
+    E, st = sim.exec(src)
+    Einf, _ = _problem(1e-11)[0].exec(src)
+    u = Einf + _smooth_noise(Einf.shape, np.random.default_rng(2), 0.05, Einf)
+    Ew, sw = sim.exec(src, warm_start=u)
+    assert not sw.warm_discarded
+    assert sw.it < st.it, (sw.it, st.it)
+    assert rel(Ew, Einf) <= 1.5 * rel(E, Einf) + 1e-4, (rel(Ew, Einf), rel(E, Einf))
+
+
+def test_bad_start_is_discarded_after_one_cycle(gpu):
+    sim, src = _problem(1e-4)
+    E, st = sim.exec(src)
+    rng = np.random.default_rng(0)
+    noise = 50 * np.abs(E).max() * (rng.standard_normal(E.shape) + 1j * rng.standard_normal(E.shape))
+    Eb, sb = sim.exec(src, warm_start=noise)
+    assert sb.warm_discarded and sb.warm_cycle_energy > sim.warm_discard_ratio * sb.cold_first_energy
+    assert sb.warm_iterations == len(sim.wiggles)
+    assert sb.it == st.it and rel(Eb, E) < 1e-6
+
+
+def test_discard_can_be_switched_off(gpu):
+    sim, src = _problem(1e-3, warm_discard_ratio=0)
+    E, st = sim.exec(src)
+    rng = np.random.default_rng(0)
+    noise = 3 * np.abs(E).max() * (rng.standard_normal(E.shape) + 1j * rng.standard_normal(E.shape))
+    Eb, sb = sim.exec(src, warm_start=noise)
+    assert not sb.warm_discarded and sb.converged
+
+
+def test_device_start_matches_host_start(gpu):
+    """A full-grid field given as a device tensor runs the same loop as the
+    same field from host memory."""
+    import torch
+    sim, src = _problem(1e-4)
+    E, st = sim.exec(src)
+    u = sim.initial_field(E)
+    d = torch.from_numpy(np.ravel(u, order="F").copy()).cuda()
+    Eh, sh = sim.exec(src, warm_start=E)
+    Ed, sd = sim.exec(src, warm_start=d)
+    assert sh.it == sd.it
+    assert rel(Ed, Eh) < 1e-6
+
+
+def test_batched_warm_starts(gpu):
+    """exec_batch with one start per source: each right-hand side matches its
+    own warm-started exec."""
+    import wavesim_b200 as ws
+    sim, src = _problem(1e-4)
+    src2 = ws.Source(0.5 * np.ones((32, 32)), [1, 1, 1])
+    E, st = sim.exec(src)
+    Einf, _ = _problem(1e-11)[0].exec(src)
+    starts = [Einf, np.zeros_like(E)]
+    Es, ss = sim.exec_batch([src, src2], warm_starts=starts)
+    for s_, w_, Eb, sb in zip([src, src2], starts, Es, ss):
+        Ew, sw = sim.exec(s_, warm_start=w_)
+        assert sb.it == sw.it and rel(Eb, Ew) < 1e-5

@@ -54,14 +54,16 @@ class ws_solve_options(C.Structure):
     _fields_ = [("max_iterations", C.c_int64), ("energy_threshold", C.c_double),
                 ("energy_interval", C.c_int64), ("stop_rule", C.c_int), ("output", C.c_int),
                 ("stop_on_nonfinite", C.c_int), ("use_graph", C.c_int), ("callback_type", C.c_char_p),
-                ("callback_interval", C.c_int64), ("callback", CALLBACK), ("user_data", C.c_void_p)]
+                ("callback_interval", C.c_int64), ("callback", CALLBACK), ("user_data", C.c_void_p),
+                ("initial_field", C.c_void_p), ("initial_memory", C.c_int), ("initial_is_eprime", C.c_int),
+                ("warm_discard_ratio", C.c_double)]
 
 
 # every entry point declared in include/wavesim_b200.h
 EXPORTS = [
     "ws_default_options", "ws_version", "ws_last_error", "ws_size_supported", "ws_run_algorithm",
     "ws_solver_create", "ws_solver_solve", "ws_solver_solve_batch", "ws_solver_buffers", "ws_solver_time_kernels",
-    "ws_solver_launches_per_iteration", "ws_solver_destroy", "ws_run_algorithm_noalloc",
+    "ws_solver_launches_per_iteration", "ws_solver_warm_report", "ws_solver_destroy", "ws_run_algorithm_noalloc",
     "ws_noalloc_scratch_bytes", "ws_noalloc_last_error",
 ]
 
@@ -107,6 +109,9 @@ def _load():
     lib.ws_solver_time_kernels.restype = C.c_int
     lib.ws_solver_launches_per_iteration.argtypes = [P]
     lib.ws_solver_launches_per_iteration.restype = C.c_int
+    lib.ws_solver_warm_report.argtypes = [P, C.c_int64, C.POINTER(C.c_double), C.POINTER(C.c_double),
+                                          C.POINTER(C.c_int)]
+    lib.ws_solver_warm_report.restype = C.c_int
     lib.ws_solver_destroy.argtypes = [P]
     lib.ws_solver_destroy.restype = C.c_int
     lib.ws_run_algorithm_noalloc.argtypes = [i64p, P, C.c_int64, C.POINTER(ws_wiggle), P, C.c_float, ws_complex,

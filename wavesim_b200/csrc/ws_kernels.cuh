@@ -62,6 +62,10 @@ struct DevState {
   double e_acc;             // partial sums of this iteration's ROI energy
   double last_step_energy;  // state.last_step_energy
   double diff1;             // state.diff_energy(1)
+  // warm starts (no counterpart in the reference)
+  int diff1_locked;         // diff1 comes from the cold probe iteration; iteration 1 keeps it
+  int discarded;            // given up at the end of the first wiggle cycle
+  double warm_e;            // ROI energy of the true increment dE'_Nw of a warm start
 };
 
 struct StopRule {
@@ -287,6 +291,7 @@ __device__ __forceinline__ void finish_iteration(DevState* st, const StopRule& r
   const int it = st->it;
   if (h.fresh && it - 1 < h.cap) h.fresh[it - 1] = e;
   if (st->calc_energy || rule.fresh) st->last_step_energy = e;
+  if (it == 1 && st->diff1_locked) st->last_step_energy = st->diff1;  // warm start: the cold diff_energy(1)
   const double d = st->last_step_energy;
   if (it - 1 < h.cap) h.diff[it - 1] = d;
   if (it == 1) st->diff1 = d;
@@ -440,6 +445,101 @@ static __global__ void k_reset_state(DevState* st, int n) {
     s->e_acc = 0.0;
     s->last_step_energy = __longlong_as_double(0x7ff0000000000000LL);  // inf (Simulation.m:169)
     s->diff1 = 0.0;
+    s->diff1_locked = 0;
+    s->discarded = 0;
+    s->warm_e = 0.0;
+  }
+}
+
+// Warm start from a starting field u = gamma psi0 (no counterpart in the
+// reference).  The loop's limit depends on how an increment enters the
+// wiggle cycle, so a start is injected the way the reference injects its
+// source: spread evenly over the first cycle, u/Nw per iteration.  With
+// v = u/Nw that is exactly the cold first cycle run from dE' = v, E' = 0,
+// followed by dE' -= v (the Nw extra v's that E' accumulated sum to u).  A
+// zero start therefore reproduces the cold loop bit for bit.
+//
+// v <- gamma .* psi0 / Nw (or E'/Nw when the start is already primed); gamma
+// is shared by the components and right-hand sides (npts points each).
+static __global__ void k_warm_scale(float2* __restrict__ v, const float2* __restrict__ gamma, long long n,
+                                    long long npts, float inv_nw, int primed) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    const float2 u = primed ? v[i] : cmul(v[i], gamma[i % npts]);
+    v[i] = make_float2(u.x * inv_nw, u.y * inv_nw);
+  }
+}
+
+// After the cold probe iteration (which set diff_energy(1)): dE' <- v, E' <- 0
+// and the loop restarts at iteration 1 with diff1 kept.
+static __global__ void k_warm_begin(float2* __restrict__ dE, float2* __restrict__ E, const float2* __restrict__ v,
+                                    long long n) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    dE[i] = v[i];
+    E[i] = make_float2(0.f, 0.f);
+  }
+}
+static __global__ void k_warm_restart(DevState* st, int n) {
+  for (int i = threadIdx.x; i < n; i += blockDim.x) {
+    DevState* s = st + i;
+    if (s->status) continue;  // the probe diverged: leave it stopped
+    s->it = 1;
+    s->done = 0;
+    s->converged = 0;
+    s->calc_energy = 1;
+    s->blocks_done = 0;
+    s->e_acc = 0.0;
+    s->last_step_energy = __longlong_as_double(0x7ff0000000000000LL);
+    s->diff1_locked = 1;
+    s->discarded = 0;
+    s->warm_e = 0.0;
+  }
+}
+
+// End of the warm first cycle: dE' -= v (the true increment of iteration
+// Nw), and its ROI energy into warm_e of right-hand side blockIdx.y.
+static __global__ void __launch_bounds__(256) k_warm_shift(float2* __restrict__ dE, const float2* __restrict__ v,
+                                                           Geom g, long long fstride, DevState* st) {
+  const int r = blockIdx.y;
+  dE += (long long)r * fstride;
+  v += (long long)r * fstride;
+  float acc = 0.f;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < fstride; i += (long long)gridDim.x * blockDim.x) {
+    const float2 d = csub(dE[i], v[i]);
+    dE[i] = d;
+    long long k = i;
+    const int y = (int)(k % g.ny); k /= g.ny;
+    const int x = (int)(k % g.nx); k /= g.nx;
+    const int z = (int)(k % g.nz);
+    const int c = (int)(k / g.nz);
+    if (y >= g.r0[0] && y < g.r1[0] && x >= g.r0[1] && x < g.r1[1] && z >= g.r0[2] && z < g.r1[2] && c >= g.r0[3] &&
+        c < g.r1[3])
+      acc = fmaf(d.x, d.x, fmaf(d.y, d.y, acc));
+  }
+  __shared__ float red[8];
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = acc;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    float t = 0.f;
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t += red[w];
+    atomicAdd(&st[r].warm_e, (double)t);
+  }
+}
+
+// A warm start whose true increment energy after its first cycle exceeds
+// ratio x diff_energy(1) (NaN included) is worse than starting from zero: it
+// stops here, unconverged and marked discarded, so that the caller reruns
+// it cold having paid for one cycle only.  ratio <= 0 keeps every start.
+static __global__ void k_warm_check(DevState* st, int n, double ratio) {
+  for (int r = threadIdx.x; r < n; r += blockDim.x) {
+    DevState* d = st + r;
+    if (ratio <= 0.0 || d->done) continue;
+    if (!(d->warm_e <= ratio * d->diff1)) {
+      d->done = 1;
+      d->converged = 0;
+      d->discarded = 1;
+    }
   }
 }
 

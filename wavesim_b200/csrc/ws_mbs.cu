@@ -219,10 +219,12 @@ static int make_layout(const Geom& g, Layout& L, std::string& why) {
 struct GraphKey {
   double threshold = -1;
   long long max_iter = -1;
-  int interval = -1, stop_rule = -1, nan_stop = -1, nrhs = -1;
+  int interval = -1, stop_rule = -1, nan_stop = -1, nrhs = -1, warm = -1;
+  double warm_ratio = -1;
   bool operator==(const GraphKey& o) const {
     return threshold == o.threshold && max_iter == o.max_iter && interval == o.interval &&
-           stop_rule == o.stop_rule && nan_stop == o.nan_stop && nrhs == o.nrhs;
+           stop_rule == o.stop_rule && nan_stop == o.nan_stop && nrhs == o.nrhs && warm == o.warm &&
+           warm_ratio == o.warm_ratio;
   }
 };
 
@@ -251,6 +253,9 @@ struct Solver {
   long long hist_cap = 0;
   double* d_energy = nullptr;
   double* d_partials = nullptr;  // per-block ROI energy of K3
+  float2* d_init = nullptr;      // warm starts: v = gamma psi0 / Nw per right-hand side (batch_cap of them)
+  bool warm = false;             // the current solve starts from d_init
+  double warm_ratio = 0.0;       // discard threshold of the current solve
   float2* d_tw = nullptr;
   FftPlan py{}, pxl{}, po{};
   const float2* twx = nullptr;
@@ -272,7 +277,7 @@ static void destroy_solver(Solver* s) {
   cudaSetDevice(s->device);
   free_graph(s);
   void* ptrs[] = {s->d_wigf, s->d_wigc,  s->d_gamma,  s->d_E,        s->d_dE, s->d_T,   s->d_src,
-                  s->d_stage, s->d_out, s->d_state, s->d_hist, s->d_energy, s->d_tw, s->d_partials};
+                  s->d_stage, s->d_out, s->d_state, s->d_hist, s->d_energy, s->d_tw, s->d_partials, s->d_init};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   for (auto& e : s->ev)
@@ -374,10 +379,10 @@ static size_t field_elems(const Solver* s) { return (size_t)s->g.npts * s->g.nc;
 // Buffers for nrhs right-hand sides (kept when large enough).
 static int ensure_batch(Solver* s, int nrhs) {
   if (nrhs <= s->batch_cap) return WS_OK;
-  void* old[] = {s->d_E, s->d_dE, s->d_T, s->d_src, s->d_state, s->d_energy, s->d_partials};
+  void* old[] = {s->d_E, s->d_dE, s->d_T, s->d_src, s->d_state, s->d_energy, s->d_partials, s->d_init};
   for (void* p : old)
     if (p) cudaFree(p);
-  s->d_E = s->d_dE = s->d_T = s->d_src = nullptr;
+  s->d_E = s->d_dE = s->d_T = s->d_src = s->d_init = nullptr;
   s->d_state = nullptr;
   s->d_energy = s->d_partials = nullptr;
   s->batch_cap = 0;
@@ -662,6 +667,38 @@ static int ensure_hist(Solver* s, long long cap) {
   return WS_OK;
 }
 
+// The prologue and first wiggle cycle of a solve (with the source).  Cold:
+// the reference's iterations 1..Nw from E' = dE' = 0.  Warm (d_init holds
+// v = u/Nw, see k_warm_scale): a cold probe iteration for diff_energy(1),
+// the restart from dE' = v, E' = 0, iterations 1..Nw with the source, the
+// shift dE' -= v and the discard check.
+static cudaError_t launch_prologue(const Solver* s, const StopRule& rule, const Hist& h) {
+  const size_t nbytes = field_elems(s) * s->nrhs * sizeof(float2);
+  cudaError_t e;
+  if ((e = cudaMemsetAsync(s->d_E, 0, nbytes, s->stream)) != cudaSuccess) return e;
+  if ((e = cudaMemsetAsync(s->d_dE, 0, nbytes, s->stream)) != cudaSuccess) return e;
+  k_reset_state<<<1, 256, 0, s->stream>>>(s->d_state, s->nrhs);
+  if ((e = cudaGetLastError()) != cudaSuccess) return e;
+  if (s->warm) {
+    if ((e = launch_iteration(s, 0, true, rule, h)) != cudaSuccess) return e;  // the probe
+    const long long n = (long long)field_elems(s) * s->nrhs;
+    const unsigned blocks = (unsigned)std::min<long long>((n + 255) / 256, 8 * kNumSms);
+    k_warm_begin<<<blocks, 256, 0, s->stream>>>(s->d_dE, s->d_E, s->d_init, n);
+    k_warm_restart<<<1, 256, 0, s->stream>>>(s->d_state, s->nrhs);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+  }
+  for (int i = 0; i < s->nw; ++i)
+    if ((e = launch_iteration(s, i, true, rule, h)) != cudaSuccess) return e;
+  if (s->warm) {
+    const long long fe = (long long)field_elems(s);
+    const unsigned bpr = (unsigned)std::max<long long>(1, std::min<long long>((fe + 255) / 256, 4 * kNumSms));
+    k_warm_shift<<<dim3(bpr, s->nrhs), 256, 0, s->stream>>>(s->d_dE, s->d_init, s->g, fe, s->d_state);
+    k_warm_check<<<1, 256, 0, s->stream>>>(s->d_state, s->nrhs, s->warm_ratio);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+  }
+  return cudaSuccess;
+}
+
 static int build_graph(Solver* s, const StopRule& rule, const Hist& h) {
   free_graph(s);
   // the stop rule can only end the loop at a multiple of Nw, at the latest at
@@ -678,11 +715,7 @@ static int build_graph(Solver* s, const StopRule& rule, const Hist& h) {
   // prologue + first cycle (with the source)
   e = cudaStreamBeginCaptureToGraph(s->stream, graph, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal);
   if (e == cudaSuccess) {
-    const size_t nbytes = field_elems(s) * s->nrhs * sizeof(float2);
-    cudaMemsetAsync(s->d_E, 0, nbytes, s->stream);
-    cudaMemsetAsync(s->d_dE, 0, nbytes, s->stream);
-    k_reset_state<<<1, 256, 0, s->stream>>>(s->d_state, s->nrhs);
-    for (int i = 0; i < s->nw && e == cudaSuccess; ++i) e = launch_iteration(s, i, true, rule, h);
+    e = launch_prologue(s, rule, h);
     if (e == cudaSuccess) {
       k_cycle_guard<<<1, 32, 0, s->stream>>>(s->d_state, s->nrhs, cond, max_cycles);
       e = cudaGetLastError();
@@ -846,8 +879,22 @@ static int solve_batch(Solver* s, int nrhs, const int64_t* counts, const ws_sour
   const long long hs_stride = 2 * s->hist_cap;
   Hist h{s->d_hist, s->d_hist + s->hist_cap, s->hist_cap, hs_stride};
   std::vector<DevState> hs(nrhs);
+  s->warm = opt.initial_field != nullptr;
+  s->warm_ratio = opt.warm_discard_ratio;
+  if (s->warm) {
+    const long long fe = (long long)field_elems(s);
+    if (!s->d_init) WS_CUDA(cudaMalloc(&s->d_init, fe * s->batch_cap * sizeof(float2)));
+    WS_CUDA(cudaMemcpyAsync(s->d_init, opt.initial_field, fe * nrhs * sizeof(float2),
+                            opt.initial_memory == WS_DEVICE ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice,
+                            s->stream));
+    const long long n = fe * nrhs;
+    k_warm_scale<<<(unsigned)std::min<long long>((n + 255) / 256, 8 * kNumSms), 256, 0, s->stream>>>(
+        s->d_init, s->d_gamma, n, s->g.npts, 1.0f / (float)s->nw, opt.initial_is_eprime ? 1 : 0);
+    WS_CUDA(cudaGetLastError());
+  }
   if (opt.use_graph && !want_cb) {
-    GraphKey key{rule.threshold, rule.max_iter, rule.interval, opt.stop_rule, rule.nan_stop, nrhs};
+    GraphKey key{rule.threshold, rule.max_iter, rule.interval, opt.stop_rule, rule.nan_stop, nrhs,
+                 s->warm ? 1 : 0, s->warm ? s->warm_ratio : 0.0};
     if (!s->gexec || !(key == s->gkey)) {
       rc = build_graph(s, rule, h);
       if (rc) return rc;
@@ -855,19 +902,20 @@ static int solve_batch(Solver* s, int nrhs, const int64_t* counts, const ws_sour
     }
     WS_CUDA(cudaGraphLaunch(s->gexec, s->stream));
   } else {
-    const size_t nbytes = field_elems(s) * nrhs * sizeof(float2);
-    WS_CUDA(cudaMemsetAsync(s->d_E, 0, nbytes, s->stream));
-    WS_CUDA(cudaMemsetAsync(s->d_dE, 0, nbytes, s->stream));
-    k_reset_state<<<1, 256, 0, s->stream>>>(s->d_state, nrhs);
     std::vector<double> hist;
     long long it = 0;
     const long long cb_int = std::max<int64_t>(1, opt.callback_interval);
     const long long max_cycles = (rule.max_iter + s->nw - 1) / s->nw + 1;
     for (long long cycle = 0;; ++cycle) {
       if (cycle >= max_cycles) return fail(WS_ERR_CUDA, "loop did not stop within max_iterations (internal error)");
-      for (int i = 0; i < s->nw; ++i) {
-        WS_CUDA(launch_iteration(s, (int)(it % s->nw), it < s->nw, rule, h));
-        ++it;
+      if (cycle == 0) {
+        WS_CUDA(launch_prologue(s, rule, h));
+        it += s->nw;
+      } else {
+        for (int i = 0; i < s->nw; ++i) {
+          WS_CUDA(launch_iteration(s, (int)(it % s->nw), false, rule, h));
+          ++it;
+        }
       }
       WS_CUDA(cudaMemcpyAsync(hs.data(), s->d_state, nrhs * sizeof(DevState), cudaMemcpyDeviceToHost, s->stream));
       WS_CUDA(cudaStreamSynchronize(s->stream));
@@ -1054,6 +1102,20 @@ int ws_solver_time_kernels(ws_solver h, int n_iterations, float ms_out[3], doubl
     bytes_out[1] = 16.0 * n;                                // read T, write T
     bytes_out[2] = 40.0 * n + 8.0 * (double)s->g.npts;      // read T, dE, E, gamma; write dE, E
   }
+  return WS_OK;
+}
+
+int ws_solver_warm_report(ws_solver h, int64_t rhs, double* cold_first_energy, double* warm_cycle_energy,
+                          int* discarded) {
+  if (!h) return fail(WS_ERR_INVALID_ARGUMENT, "null solver");
+  Solver* s = reinterpret_cast<Solver*>(h);
+  if (rhs < 0 || rhs >= s->nrhs) return fail(WS_ERR_INVALID_ARGUMENT, "right-hand side out of range");
+  WS_CUDA(cudaSetDevice(s->device));
+  DevState st{};
+  WS_CUDA(cudaMemcpy(&st, s->d_state + rhs, sizeof(DevState), cudaMemcpyDeviceToHost));
+  if (cold_first_energy) *cold_first_energy = st.diff1;
+  if (warm_cycle_energy) *warm_cycle_energy = s->warm ? st.warm_e : -1.0;
+  if (discarded) *discarded = s->warm ? st.discarded : 0;
   return WS_OK;
 }
 

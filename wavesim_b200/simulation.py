@@ -77,6 +77,7 @@ class WaveSim:
         self.stop_rule = o.get("stop_rule", "reference")
         self.device = int(o.get("device", 0))
         self.use_graph = bool(o.get("use_graph", True))
+        self.warm_discard_ratio = float(o.get("warm_discard_ratio", 1.0))
 
         self.sample = Medium(refractive_index, o)
         self.grid = self.sample.grid
@@ -216,11 +217,86 @@ class WaveSim:
             return int(math.ceil(self.max_cycles * self.iterations_per_cycle))
         return 100000  # WaveSimBase.m:127-131
 
-    def exec(self, source):
+    def roi_medium(self):
+        """The (real) refractive index on the ROI, [y, x, z]."""
+        r = self.roi
+        n = np.sqrt(np.asarray(self.sample.e_r))
+        return np.real(n[r[0, 0] - 1:r[1, 0], r[0, 1] - 1:r[1, 1], r[0, 2] - 1:r[1, 2]]).astype(np.float32)
+
+    def initial_field(self, psi0):
+        """A starting field psi0 on the full grid (complex64, column-major, as
+        the C ABI takes it).  psi0 is given on the full grid or on the ROI
+        ([y, x, z] or [y, x, z, c]); an ROI field is continued into the
+        absorbing boundary layers by its edge values under a cos^2 taper that
+        reaches zero at the grid edge (a field cut to zero at the ROI edge
+        would carry a step there, whose residual costs iterations)."""
+        shape = tuple(int(v) for v in self.N)
+        p = np.asarray(psi0, np.complex64)
+        if p.ndim == 3:
+            p = p[..., None]
+        if p.shape == shape:
+            return np.asfortranarray(p)
+        r = self.roi
+        lo = [int(r[0, d]) - 1 for d in range(4)]
+        hi = [shape[d] - int(r[1, d]) for d in range(4)]
+        if tuple(int(r[1, d]) - int(r[0, d]) + 1 for d in range(4)) != p.shape:
+            raise ValueError(f"starting field shape {p.shape} matches neither the ROI nor the grid {shape}")
+        full = np.pad(p, [(lo[d], hi[d]) for d in range(3)] + [(0, 0)], mode="edge")
+        if lo[3] or hi[3]:
+            full = np.pad(full, [(0, 0)] * 3 + [(lo[3], hi[3])])
+        for d in range(3):
+            w = np.ones(shape[d], np.float32)
+            if lo[d]:
+                w[:lo[d]] = np.cos(0.5 * np.pi * np.arange(lo[d], 0, -1) / (lo[d] + 1)) ** 2
+            if hi[d]:
+                w[shape[d] - hi[d]:] = np.cos(0.5 * np.pi * np.arange(1, hi[d] + 1) / (hi[d] + 1)) ** 2
+            sh = [1, 1, 1, 1]
+            sh[d] = shape[d]
+            full = full * w.reshape(sh)
+        return np.asfortranarray(full.astype(np.complex64))
+
+    def _options(self, output="field"):
+        o = _lib.default_options()
+        o.max_iterations = self.max_iterations()
+        o.energy_threshold = self.energy_threshold
+        o.energy_interval = self.energy_calculation_interval
+        o.stop_rule = _lib.WS_STOP_FRESH if self.stop_rule == "fresh" else _lib.WS_STOP_REFERENCE
+        o.output = _lib.WS_OUTPUT_FIELD if output == "field" else _lib.WS_OUTPUT_EPRIME
+        o.use_graph = 1 if self.use_graph else 0
+        o.warm_discard_ratio = self.warm_discard_ratio
+        return o
+
+    def _warm_input(self, psi0):
+        """(pointer owner, memory kind, primed) of a warm start given as a
+        host array, a full-grid device tensor, or a model with predict_grid."""
+        if hasattr(psi0, "predict_grid"):
+            psi0 = psi0.predict_grid(self)
+        if hasattr(psi0, "data_ptr"):
+            if psi0.numel() != int(np.prod(self.N)):
+                raise ValueError("a device warm start must hold the full grid")
+            return psi0, _lib.WS_DEVICE
+        return self.initial_field(psi0), _lib.WS_HOST
+
+    def exec(self, source, warm_start=None, output="field"):
         """Simulation.exec (Simulation.m:138-190) with the loop on the GPU.
         Returns (E, state): E = E'/gamma on the ROI, indexed [y, x, z] (scalar)
-        or [y, x, z, c] (vector); state.it, state.diff_energy, state.converged,
-        state.time."""
+        or [y, x, z, c] (vector), or with output="eprime" the full-grid E'
+        that the MEX call returns (WaveSimBase.m:146); state.it,
+        state.diff_energy, state.converged, state.time.
+
+        warm_start (no counterpart in the reference): an estimate psi0 of the
+        field - a host array on the ROI or the full grid, a flat complex64
+        device tensor on the full grid (column-major), or a
+        wavesim_b200.warmstart.WarmStart model, whose prediction then stays
+        on the device.  The loop starts from it, injected over the first
+        wiggle cycle as the reference injects its source, and runs to the
+        same energy tolerance against the cold first-iteration energy.  A
+        start whose true increment after the first cycle carries more than
+        warm_discard_ratio (option, default 1) times the energy of the cold
+        first increment is given up there and the solve reruns cold
+        (state.warm_discarded; state.time covers both)."""
+        if output not in ("field", "eprime"):
+            raise ValueError("output must be 'field' or 'eprime'")
         t0 = time.perf_counter()
         s, blocks, keep = self.source_blocks(source)
         state = SimpleNamespace(source=s, source_energy=s.energy())
@@ -228,13 +304,11 @@ class WaveSim:
             warnings.warn("There is no source inside the grid boundaries, expect to get zero field everywhere.")
             return None, state
         h = self.solver()
-        o = _lib.default_options()
-        o.max_iterations = self.max_iterations()
-        o.energy_threshold = self.energy_threshold
-        o.energy_interval = self.energy_calculation_interval
-        o.stop_rule = _lib.WS_STOP_FRESH if self.stop_rule == "fresh" else _lib.WS_STOP_REFERENCE
-        o.output = _lib.WS_OUTPUT_FIELD
-        o.use_graph = 1 if self.use_graph else 0
+        o = self._options(output)
+        init = None
+        if warm_start is not None:
+            init, o.initial_memory = self._warm_input(warm_start)
+            o.initial_field = init.data_ptr() if hasattr(init, "data_ptr") else init.ctypes.data
         cb_keep = None
         if self.callback is not None:
             sim = self
@@ -247,7 +321,10 @@ class WaveSim:
             o.callback_type = b"Custom"
             o.callback_interval = self.callback_interval
         r = self.roi
-        shape = tuple(int(r[1, d] - r[0, d] + 1) for d in range(4))
+        if output == "field":
+            shape = tuple(int(r[1, d] - r[0, d] + 1) for d in range(4))
+        else:
+            shape = tuple(int(v) for v in self.N)
         E = np.empty(shape, dtype=np.complex64, order="F")
         hist = np.zeros(o.max_iterations + len(self.wiggles) + 1)
         n_it = C.c_int64()
@@ -259,19 +336,32 @@ class WaveSim:
         state.it = int(n_it.value) + 1  # Simulation.next leaves it one past the last iteration
         state.diff_energy = hist[:n_it.value].copy()
         state.converged = bool(conv.value)
+        if init is not None:
+            cold, warm, disc = C.c_double(), C.c_double(), C.c_int()
+            _lib.check(_lib.lib.ws_solver_warm_report(h, 0, C.byref(cold), C.byref(warm), C.byref(disc)))
+            state.cold_first_energy, state.warm_cycle_energy = cold.value, warm.value
+            state.warm_discarded = bool(disc.value)
+            del init
+            if state.warm_discarded:
+                E, st2 = self.exec(source, output=output)
+                st2.cold_first_energy, st2.warm_cycle_energy = state.cold_first_energy, state.warm_cycle_energy
+                st2.warm_discarded, st2.warm_iterations = True, state.it - 1
+                st2.time = time.perf_counter() - t0
+                return E, st2
         state.time = time.perf_counter() - t0
         if not self.vector:
             E = E[..., 0]
-        return np.ascontiguousarray(E), state
+        return (np.ascontiguousarray(E) if output == "field" else E), state
 
-
-    def exec_batch(self, sources):
+    def exec_batch(self, sources, warm_starts=None):
         """Many sources on this medium in one batched solve (ws_solver_solve_batch).
 
         Equivalent to ``[self.exec(s) for s in sources]`` - every source runs
         the reference loop and stop rule on its own - but all of them share the
         medium's device data and each kernel launch covers the whole batch.
-        Returns (list of E, list of state)."""
+        warm_starts: None, or one starting field per source (host arrays on
+        the ROI or the full grid), see exec; a discarded start is rerun cold
+        on its own.  Returns (list of E, list of state)."""
         t0 = time.perf_counter()
         groups, keep, counts = [], [], []
         for src in sources:
@@ -290,16 +380,17 @@ class WaveSim:
                                                  (C.c_int64 * 4)(*[int(a) for a in v.shape]), v.ctypes.data)
                 i += 1
         h = self.solver()
-        o = _lib.default_options()
-        o.max_iterations = self.max_iterations()
-        o.energy_threshold = self.energy_threshold
-        o.energy_interval = self.energy_calculation_interval
-        o.stop_rule = _lib.WS_STOP_FRESH if self.stop_rule == "fresh" else _lib.WS_STOP_REFERENCE
-        o.output = _lib.WS_OUTPUT_FIELD
-        o.use_graph = 1 if self.use_graph else 0
+        o = self._options()
+        R = len(sources)
+        init = None
+        if warm_starts is not None:
+            if len(warm_starts) != R:
+                raise ValueError("one warm start per source")
+            init = np.stack([np.ravel(self.initial_field(w), order="F") for w in warm_starts])
+            o.initial_field = init.ctypes.data
+            o.initial_memory = _lib.WS_HOST
         r = self.roi
         shape = tuple(int(r[1, d] - r[0, d] + 1) for d in range(4))
-        R = len(sources)
         E = np.empty((R,) + shape[::-1], dtype=np.complex64)  # each field column-major
         cap = o.max_iterations + len(self.wiggles) + 1
         hist = np.zeros((R, cap))
@@ -319,6 +410,20 @@ class WaveSim:
             outs.append(Ei)
             states.append(SimpleNamespace(source=groups[i], it=int(n_it[i]) + 1, converged=bool(conv[i]),
                                           diff_energy=hist[i, :n_it[i]].copy(), time=dt))
+        if init is not None:
+            for i in range(R):
+                cold, warm, disc = C.c_double(), C.c_double(), C.c_int()
+                _lib.check(_lib.lib.ws_solver_warm_report(h, i, C.byref(cold), C.byref(warm), C.byref(disc)))
+                states[i].cold_first_energy, states[i].warm_cycle_energy = cold.value, warm.value
+                states[i].warm_discarded = bool(disc.value)
+            for i in range(R):
+                if states[i].warm_discarded:
+                    outs[i], st = self.exec(sources[i])
+                    st.warm_discarded, st.warm_iterations = True, states[i].it - 1
+                    st.cold_first_energy = states[i].cold_first_energy
+                    st.warm_cycle_energy = states[i].warm_cycle_energy
+                    st.time += dt
+                    states[i] = st
         return outs, states
 
 
