@@ -14,7 +14,7 @@ def rel(a, b):
 
 
 def _medium():
-    from wavesim_b200.warmstart import sphere_medium
+    from wavesim_b200.workloads import sphere_medium
     return sphere_medium(32, np.random.default_rng(21))
 
 

@@ -132,6 +132,16 @@ def c4(scale=1):
     return n, opt, np.ones((roi, roi)), [1, 1, 1, 1], True
 
 
+def sphere_medium(roi, rng, n_bg=1.33, n_sphere=1.5, spheres_per_224=2000):
+    """A roi^3 cube of the c3 sphere distribution (radius U[0.5, 2] lambda at
+    4 pixels per wavelength, n_sphere in n_bg) with as many spheres per
+    volume as 2000 in a 224^3 cube: the media of the warm-start training set
+    and of small test problems."""
+    count = max(1, int(round(spheres_per_224 * (roi / 224.0) ** 3)))
+    cen, rad = sphere_packing(roi, count, 0.5 * PPW, 2.0 * PPW, rng)
+    return rasterise_spheres((roi, roi, roi), cen, rad, n_bg, n_sphere)
+
+
 def plane_wave_edge(roi_len, angle, pixel_size, lam, n_bg=1.0):
     """exp(i k sin(theta) y) along the entry edge (a column at x = 1)."""
     k = 2 * np.pi / lam * n_bg
