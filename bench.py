@@ -266,13 +266,19 @@ def run_ours(args):
     ms_per_solve_gpu = local_ms / args.steps
     value = total_ms / (args.steps * ws)
     n_iter = iters[-1]
-    launches_per_solve = 3 * n_iter + (n_iter // len(sim.wiggles)) + 1 + len(s.values) + 1
+    # K1, K2, K3 and the stop-rule kernel per iteration, the cycle guard per
+    # wiggle cycle, state reset, source scatter, finalize
+    launches_per_solve = (_lib.lib.ws_solver_launches_per_iteration(h) * n_iter + (n_iter // len(sim.wiggles)) + 1
+                          + len(s.values) + 1)
 
     # per-kernel device time (CUDA events on the solver's stream) -> roofline
     ms3 = (C.c_float * 3)()
     by3 = (C.c_double * 3)()
     _lib.check(_lib.lib.ws_solver_time_kernels(h, 24, ms3, by3))
-    names = ["k_fwd_inner", "k_outer", "k_inv_inner"]
+    # K1: wiggle + source + inner (y, x) FFT; K2: outer (z) FFT + Green's
+    # function + inverse; K3: inverse inner FFT + unwiggle + mix + accumulate
+    # + ROI energy (kf_plane_fwd / kf_pencil / kf_plane_inv on the 256^3 grid)
+    names = ["K1", "K2", "K3"]
     peaks, peak_kind = measured_peaks()
     peak = float(peaks.get("hbm_gbs", 6650.0))
     kern = []
