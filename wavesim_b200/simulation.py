@@ -77,7 +77,7 @@ class WaveSim:
         self.stop_rule = o.get("stop_rule", "reference")
         self.device = int(o.get("device", 0))
         self.use_graph = bool(o.get("use_graph", True))
-        self.warm_discard_ratio = float(o.get("warm_discard_ratio", 1.0))
+        self.warm_discard_ratio = o.get("warm_discard_ratio", None)  # None: 2 Nw (set with the wiggles)
 
         self.sample = Medium(refractive_index, o)
         self.grid = self.sample.grid
@@ -105,6 +105,12 @@ class WaveSim:
         self.epsilon = np.float32(eps)
         self.k0, self.k0c = k0, k0c
         self.wiggles, self.ACC = self._wiggles(o.get("ACC", True))
+        # a zero start (the cold loop) carries about Nw times the first
+        # increment's energy at the end of its first cycle: starts above twice
+        # that are worse than no start
+        if self.warm_discard_ratio is None:
+            self.warm_discard_ratio = 2.0 * len(self.wiggles)
+        self.warm_discard_ratio = float(self.warm_discard_ratio)
         if self.vector:
             if o.get("roi") is None:
                 self.roi[1, 3] = 3  # WaveSimVector.m:14-16
@@ -292,8 +298,8 @@ class WaveSim:
         wiggle cycle as the reference injects its source, and runs to the
         same energy tolerance against the cold first-iteration energy.  A
         start whose true increment after the first cycle carries more than
-        warm_discard_ratio (option, default 1) times the energy of the cold
-        first increment is given up there and the solve reruns cold
+        warm_discard_ratio (option, default 2 Nw) times the energy of the
+        cold first increment is given up there and the solve reruns cold
         (state.warm_discarded; state.time covers both)."""
         if output not in ("field", "eprime"):
             raise ValueError("output must be 'field' or 'eprime'")
