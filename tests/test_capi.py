@@ -9,8 +9,8 @@ import numpy as np
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 
 
-def header_functions():
-    text = open(os.path.join(ROOT, "include", "wavesim_b200.h")).read()
+def header_functions(name="wavesim_b200.h"):
+    text = open(os.path.join(ROOT, "include", name)).read()
     text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
     return sorted(set(re.findall(r"\b(ws_[a-z_0-9]+)\s*\(", text)) - {"ws_callback_fn"})
 
@@ -22,6 +22,15 @@ def test_library_exports_header_symbols():
     for n in names:
         assert hasattr(_lib.lib, n), n
     assert sorted(_lib.EXPORTS) == names
+
+
+def test_library_exports_network_header_symbols():
+    """include/wavesim_b200_net.h (the warm-start network kernels)."""
+    from wavesim_b200 import _lib
+    names = header_functions("wavesim_b200_net.h")
+    assert len(names) > 10
+    for n in names:
+        assert hasattr(_lib.lib, n), n
 
 
 def test_version_and_defaults():
