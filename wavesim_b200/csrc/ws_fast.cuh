@@ -177,6 +177,25 @@ __global__ void __launch_bounds__(kThreads, 2)
     colbase = (long long)bid * M;
     ncol = (int)min((long long)M, (long long)nx * g.nc - colbase);
   }
+  // Blocks run roughly in index order, a.pf of them at a time: pull the
+  // columns block bid + a.pf will load into L2 now, so that HBM keeps
+  // streaming while this block transforms (same right-hand side only).
+  if (a.pf && bid + a.pf < a.bpr) {
+    const int fb = bid + a.pf;
+    long long fcol;
+    int fn;
+    if constexpr (DO_X) {
+      fcol = (long long)(fb / C) * nx + (long long)(C > 1 ? fb % C : 0) * M;
+      fn = M;
+    } else {
+      fcol = (long long)fb * M;
+      fn = (int)min((long long)M, (long long)nx * g.nc - fcol);
+    }
+    for (int c = tid; c < fn; c += kThreads) {
+      prefetch_l2(dE + (fcol + c) * N, N * sizeof(float2));
+      if (src) prefetch_l2(src + (fcol + c) * N, N * sizeof(float2));
+    }
+  }
   const float2 gzz = a.w.gz[z];
   // phase A: y transform of each held column, straight from global memory
   for (int c0 = 0; c0 < ncol; c0 += LPR) {
@@ -283,6 +302,12 @@ __global__ void __launch_bounds__(TY*(NO / 16) < 1024 ? TY*(NO / 16) : 1024)
   const int ky = yt * TY + yl;
   const long long ps = a.mode3d ? (long long)g.ny * g.nx : (long long)g.ny;
   float2* __restrict__ base = T + ky + (long long)g.ny * mid;
+  if (a.pf && bid + a.pf < a.bpr) {
+    // the TY-element rows of pencil block bid + a.pf into L2 (see kf_plane_fwd)
+    const int fb = bid + a.pf;
+    const float2* fbase = T + (long long)(fb % nyt) * TY + (long long)g.ny * (a.mode3d ? fb / nyt : 0);
+    for (int r = tid; r < NO; r += TY * P) prefetch_l2(fbase + ps * r, TY * sizeof(float2));
+  }
   float2 v[16];
 #pragma unroll
   for (int r = 0; r < 16; ++r) v[r] = base[ps * (p + P * r)];
@@ -352,6 +377,24 @@ __global__ void __launch_bounds__(kThreads, 2)
     prefetch_l2(dE + c0 * N, bytes);
     prefetch_l2(E + c0 * N, bytes);
     if (comp0 == comp1) prefetch_l2(gamma + c0 * N - (long long)comp0 * g.npts, bytes);
+  }
+  if (a.pf && bid + a.pf < a.bpr) {
+    // the transform input of block bid + a.pf into L2 (see kf_plane_fwd)
+    const int fb = bid + a.pf;
+    if constexpr (DO_X) {
+      const long long fplane = fb / C;
+      if constexpr (C > 1) {
+        const int frank = fb % C;
+        for (int kx = tid; kx < nx; kx += kThreads)
+          prefetch_l2(T + (fplane * nx + kx) * N + (long long)frank * G::LR, G::LR * sizeof(float2));
+      } else {
+        if (tid == 0) prefetch_l2(T + fplane * nx * N, (unsigned)((long long)nx * N * sizeof(float2)));
+      }
+    } else {
+      const long long fcol = (long long)fb * M;
+      const int fn = (int)min((long long)M, (long long)nx * g.nc - fcol);
+      if (tid == 0 && fn > 0) prefetch_l2(T + fcol * N, (unsigned)fn * N * sizeof(float2));
+    }
   }
   if constexpr (DO_X) {
     constexpr int ROWS = C > 1 ? G::LR : N;

@@ -95,6 +95,7 @@ struct InnerArgs {
   int ncols;    // columns per block, 2-D only
   int bpr;      // blocks per right-hand side (a batch of sources runs as consecutive block ranges)
   long long fstride;  // elements between the fields of consecutive right-hand sides
+  int pf;       // fast kernels: block b pulls the inputs of block b + pf into L2 (0: off)
 };
 
 struct OuterArgs {
@@ -107,6 +108,7 @@ struct OuterArgs {
   int mode3d;
   int bpr;
   long long fstride;
+  int pf;       // fast kernels: block b pulls the inputs of block b + pf into L2 (0: off)
 };
 
 __device__ __forceinline__ int load_done(const DevState* st) { return __ldcg(&st->done); }

@@ -254,6 +254,7 @@ struct Solver {
   double* d_energy = nullptr;
   double* d_partials = nullptr;  // per-block ROI energy of K3
   float2* d_init = nullptr;      // warm starts: v = gamma psi0 / Nw per right-hand side (batch_cap of them)
+  int pf_inner = 0, pf_outer = 0;  // L2 prefetch distance of the fast kernels, in blocks (0: off)
   bool warm = false;             // the current solve starts from d_init
   double warm_ratio = 0.0;       // discard threshold of the current solve
   float2* d_tw = nullptr;
@@ -428,6 +429,16 @@ static int create_solver(const int64_t N[4], const ws_complex* gamma, int64_t n_
     destroy_solver(s);
     return fail(rc, why);
   }
+  {
+    // L2 prefetch distance of the fast kernels: about one wave of resident
+    // blocks (2 per SM), a whole number of clusters.  WAVESIM_B200_PREFETCH
+    // sets the waves' size in blocks per SM (0 switches the prefetch off).
+    int per_sm = 2;
+    if (const char* e = std::getenv("WAVESIM_B200_PREFETCH")) per_sm = std::max(0, std::atoi(e));
+    const int c = s->lay.fi ? std::max(1, s->lay.fi->c) : 1;
+    s->pf_inner = (per_sm * kNumSms / c) * c;
+    s->pf_outer = per_sm * kNumSms;
+  }
 #define WS_TRY(call)                 \
   do {                               \
     cudaError_t e__ = (call);        \
@@ -502,6 +513,7 @@ static InnerArgs inner_args(const Solver* s, int w) {
   a.ncols = s->lay.ncols;
   a.bpr = (int)s->lay.grid_inner;
   a.fstride = (long long)field_elems(s);
+  a.pf = s->lay.fi ? s->pf_inner : 0;
   return a;
 }
 
@@ -516,6 +528,7 @@ static OuterArgs outer_args(const Solver* s, int w) {
   a.mode3d = s->lay.mode3d;
   a.bpr = (int)s->lay.grid_outer;
   a.fstride = (long long)field_elems(s);
+  a.pf = s->lay.fp ? s->pf_outer : 0;
   return a;
 }
 
