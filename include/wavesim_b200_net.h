@@ -103,6 +103,8 @@ int ws_net_mse(const float* pred, const float* target, float* grad, double* loss
                int64_t ldp, void* stream);
 /* out = bf16(in) */
 int ws_net_f32_to_bf16(const float* in, void* out, int64_t n, void* stream);
+/* y += x (fp32) */
+int ws_net_add(float* y, const float* x, int64_t n, void* stream);
 const char* ws_net_last_error(void);
 
 #ifdef __cplusplus

@@ -1091,3 +1091,23 @@ extern "C" int ws_net_relu_grad_bf16(float* dy, const void* y, int64_t rows, int
                                                                             (__nv_bfloat16*)out, Cpad);
   NET_LAUNCH_CHECK();
 }
+
+namespace ws {
+namespace net {
+__global__ void k_add(float* __restrict__ y, const float* __restrict__ x, long long n) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+    y[i] += x[i];
+}
+}  // namespace net
+}  // namespace ws
+
+// y += x (fp32)
+extern "C" int ws_net_add(float* y, const float* x, int64_t n, void* stream) {
+  if (!y || !x || n < 0) {
+    t_err = "ws_net_add: bad arguments";
+    return WS_ERR_INVALID_ARGUMENT;
+  }
+  if (n == 0) return WS_OK;
+  k_add<<<grid_for(n), 256, 0, (cudaStream_t)stream>>>(y, x, n);
+  NET_LAUNCH_CHECK();
+}

@@ -28,7 +28,8 @@ the forward convolutions and the input gradients are implicit GEMMs on the
 tcgen05 tensor cores (ws_conv3_fwd_bf16 / ws_conv3_upcat_fwd_bf16, the input
 gradient with tap-flipped weights), the weight gradients explicit GEMMs
 (ws_gemm_bf16) of transposed im2col matrices; Adam keeps fp32 master
-weights and a bf16 copy for the GEMMs.  PyTorch only allocates device memory.
+weights and a bf16 copy for the GEMMs.  PyTorch only allocates and clears
+device memory.
 """
 from __future__ import annotations
 
@@ -66,6 +67,7 @@ def _bind():
         "ws_net_adam": [P, P, P, P, P, I64, C.c_float, C.c_float, C.c_float, C.c_float, INT, P],
         "ws_net_mse": [P, P, P, P, I64, INT, I64, P],
         "ws_net_f32_to_bf16": [P, P, I64, P],
+        "ws_net_add": [P, P, I64, P],
     }
     for name, args in sig.items():
         f = getattr(L, name)
@@ -168,7 +170,7 @@ class Conv3:
                                     self.cpad, None), "relu grad")
         gb = torch.empty(self.cout, device=dy.device)
         _ck(L.ws_net_bias_grad(dy.data_ptr(), gb.data_ptr(), nvox, self.cout, None), "bias grad")
-        self.gb += gb
+        _ck(L.ws_net_add(self.gb.data_ptr(), gb.data_ptr(), self.cout, None), "add")
         # weight gradient: dW[co][k] = sum_vox dy[vox][co] im2col(x)[vox][k]
         voxp = pad64(nvox)
         col = torch.empty(nvox, self.kp, device=dy.device, dtype=torch.bfloat16)
@@ -181,7 +183,7 @@ class Conv3:
         gw = torch.empty(self.cout, self.kp, device=dy.device)
         _ck(_lib.lib.ws_gemm_bf16(dyT.data_ptr(), colT.data_ptr(), gw.data_ptr(), None, None, self.cout, self.kp,
                                   voxp, voxp, voxp, self.kp, 0, _ptr(err), None), "gemm wgrad")
-        self.gw += gw
+        _ck(L.ws_net_add(self.gw.data_ptr(), gw.data_ptr(), gw.numel(), None), "add")
         del colT, dyT
         dx = None
         if need_dx:
@@ -311,9 +313,11 @@ class WarmStartNet:
                 "upcat grad")
             return da, ds
 
-        def pool_grad(g, v, c):
+        def pool_grad(g, v, c, skip):
+            """gradient through the pooling, plus the skip path's gradient"""
             dx = torch.empty(n(v), c, device=self.dev)
             _ck(L.ws_net_avgpool2_grad(g.data_ptr(), dx.data_ptr(), v[0], v[1], v[2], v[3], c, None), "pool grad")
+            _ck(L.ws_net_add(dx.data_ptr(), skip.data_ptr(), dx.numel(), None), "add")
             return dx
 
         g = self.head.backward(a["d1"], None, dout.clone(), v1, err=err)
@@ -328,13 +332,13 @@ class WarmStartNet:
         g_b4, g_e3 = upcat_grad(g, v3, w4, w3)
         g = self.c4b.backward(a["b4a"], a["b4"], g_b4, v4, err=err)
         g = self.c4a.backward(a["p3"], a["b4a"], g, v4, err=err)
-        g = pool_grad(g, v3, w3) + g_e3
+        g = pool_grad(g, v3, w3, g_e3)
         g = self.c3b.backward(a["e3a"], a["e3"], g, v3, err=err)
         g = self.c3a.backward(a["p2"], a["e3a"], g, v3, err=err)
-        g = pool_grad(g, v2, w2) + g_e2
+        g = pool_grad(g, v2, w2, g_e2)
         g = self.c2b.backward(a["e2a"], a["e2"], g, v2, err=err)
         g = self.c2a.backward(a["p1"], a["e2a"], g, v2, err=err)
-        g = pool_grad(g, v1, w1) + g_e1
+        g = pool_grad(g, v1, w1, g_e1)
         g = self.c1b.backward(a["e1a"], a["e1"], g, v1, err=err)
         self.c1a.backward(a["x"], a["e1a"], g, v1, need_dx=False, err=err)
 
@@ -514,8 +518,12 @@ class WarmStart:
         self.net._check_err()
         return psi
 
-    def save(self, path):
+    def save(self, path, bf16=False):
+        """Weights and normalisation to an .npz; bf16=True stores the weights
+        as bfloat16 bit patterns (uint16), the precision the kernels use."""
         st = self.net.state()
+        if bf16:
+            st = {k: _to_bf16_bits(v) for k, v in st.items()}
         st["meta"] = np.array([self.n_bg, self.pixel_size, self.lam] + list(self.net.widths), np.float64)
         np.savez_compressed(path, **st)
 
@@ -523,6 +531,17 @@ class WarmStart:
     def load(cls, path, device=0):
         st = dict(np.load(path))
         meta = st.pop("meta")
+        st = {k: (_from_bf16_bits(v) if v.dtype == np.uint16 else v) for k, v in st.items()}
         net = WarmStartNet(widths=tuple(int(v) for v in meta[3:7]), device=device)
         net.load(st)
         return cls(net, n_bg=float(meta[0]), pixel_size=float(meta[1]), lam=float(meta[2]), device=device)
+
+
+def _to_bf16_bits(a):
+    """fp32 -> bfloat16 bit patterns, round to nearest even."""
+    u = np.ascontiguousarray(a, np.float32).view(np.uint32)
+    return ((u + 0x7FFF + ((u >> 16) & 1)) >> 16).astype(np.uint16)
+
+
+def _from_bf16_bits(b):
+    return (b.astype(np.uint32) << 16).view(np.float32)
