@@ -49,6 +49,8 @@ def parse():
     p.add_argument("--cpu-iters", type=int, default=3, help="iterations in the CPU baseline sample")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-e2e", action="store_true")
+    p.add_argument("--no-warm", action="store_true", help="skip the learned warm-start leg")
+    p.add_argument("--batch", type=int, default=4, help="right-hand sides of the batched leg (0: skip)")
     return p.parse_args()
 
 
@@ -298,6 +300,14 @@ def run_ours(args):
         if ws > 1:
             e2e["value"] = max_over_ranks(dist, ws, e2e["value"] * args.steps, dev) / (args.steps * ws)
 
+    # the other side of the metric: batched right-hand sides, learned warm start
+    legs = {}
+    if ws == 1 and args.config == "c3":
+        if args.batch > 0:
+            legs["batched"] = run_batched(args, sim, h, stream, torch, dev, value)
+        if not args.no_warm:
+            legs["warm_start"] = run_warm(args, sim, h, s, blocks, opts, torch, dev, E_dev, value)
+
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
         ms_it, done = cpu_sample(spec, args.cpu_iters)
@@ -325,6 +335,7 @@ def run_ours(args):
                          "peak_kind": peak_kind, "unit": "GB/s", "frac": dom["achieved_gbs"] / peak,
                          "traffic": profile_traffic(dom["kernel"]),
                          "algorithmic_bytes_per_launch": dom["algorithmic_bytes"]},
+            "plain_vs_warm_start_batched": dict(legs, plain_ms_per_solve=value),
             "e2e": e2e, "gpu_launches": launches_per_solve * args.steps, "cpu_baseline": cpu,
             "clocks": clk.summary(), "host_setup_s": setup_s,
         }
@@ -333,6 +344,110 @@ def run_ours(args):
     if ws > 1:
         dist.barrier()
         dist.destroy_process_group()
+
+
+def run_batched(args, sim, h, stream, torch, dev, plain_ms):
+    """args.batch plane waves at incidence angles spread over +-30 degrees
+    (exp(i k n_bg sin(theta) x) on the z = 1 face) on the c3 medium, one
+    batched solve (ws_solver_solve_batch, every source with its own stop
+    rule); time per solve = batch time / batch size."""
+    from wavesim_b200 import _lib
+    B = args.batch
+    r = sim.roi
+    ny, nx = int(r[1, 0] - r[0, 0] + 1), int(r[1, 1] - r[0, 1] + 1)
+    k = 2 * np.pi / sim.lambda_ * 1.33 * float(sim.options["pixel_size"])
+    angles = np.linspace(-30, 30, B) if B > 1 else np.zeros(1)
+    keep, blocks = [], (_lib.ws_source_block * B)()
+    for i, a in enumerate(angles):
+        v = np.ascontiguousarray(np.broadcast_to(np.exp(1j * k * np.sin(np.radians(a)) * np.arange(nx))[None, :],
+                                                 (ny, nx)).astype(np.complex64).ravel(order="F"))
+        t = torch.from_numpy(v.view(np.float32)).to(dev)
+        keep.append(t)
+        blocks[i] = _lib.ws_source_block((C.c_int64 * 4)(int(r[0, 0]), int(r[0, 1]), int(r[0, 2]), 1),
+                                         (C.c_int64 * 4)(ny, nx, 1, 1), t.data_ptr())
+    opts = _lib.default_options()
+    opts.max_iterations = sim.max_iterations()
+    opts.energy_threshold = sim.energy_threshold
+    opts.output = _lib.WS_OUTPUT_FIELD
+    out_n = ny * nx * int(r[1, 2] - r[0, 2] + 1)
+    E = torch.empty(B * out_n * 2, dtype=torch.float32, device=dev)
+    n_it = (C.c_int64 * B)()
+    conv = (C.c_int * B)()
+    counts = (C.c_int64 * B)(*([1] * B))
+
+    def solve():
+        _lib.check(_lib.lib.ws_solver_solve_batch(h, B, counts, blocks, _lib.WS_DEVICE, C.byref(opts), E.data_ptr(),
+                                                  _lib.WS_DEVICE, None, 0, n_it, conv))
+    for _ in range(max(1, args.warmup)):
+        solve()
+    torch.cuda.synchronize()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    steps = max(1, args.steps // 2)
+    ev0.record(stream)
+    for _ in range(steps):
+        solve()
+    ev1.record(stream)
+    ev1.synchronize()
+    ms = ev0.elapsed_time(ev1) / steps
+    # back to one right-hand side for the rest of the run
+    return {"sources": B, "angles_deg": [float(a) for a in angles], "ms_per_batch": ms,
+            "ms_per_solve": ms / B, "iterations": [int(v) for v in n_it], "converged": all(bool(c) for c in conv),
+            "speedup_vs_plain": plain_ms / (ms / B)}
+
+
+def run_warm(args, sim, h, s, blocks, opts, torch, dev, E_plain, plain_ms):
+    """The learned warm start on the c3 problem: network inference on the
+    device (features, encoder-decoder, full-grid start) + the warm-started
+    solve, timed together; iterations, discard and the difference from the
+    plain answer.  Needs the committed checkpoint of the training script."""
+    from wavesim_b200 import _lib, warmstart
+    from wavesim_b200.train_warmstart import DEFAULT_OUT
+    if not os.path.exists(DEFAULT_OUT):
+        return {"unavailable": "no trained checkpoint (python -m wavesim_b200.train_warmstart)"}
+    model = warmstart.WarmStart.load(DEFAULT_OUT, device=dev.index or 0)
+    n_roi = torch.from_numpy(np.ascontiguousarray(sim.roi_medium().ravel(order="F"))).to(dev)
+    n_roi = n_roi.reshape(tuple(int(v) for v in sim.roi_medium().shape))
+    E_ref = E_plain.clone()
+    E_w = torch.empty_like(E_plain)
+    o = _lib.ws_solve_options()
+    C.pointer(o)[0] = opts
+    o.warm_discard_ratio = sim.warm_discard_ratio
+    o.initial_memory = _lib.WS_DEVICE
+    n_it, conv = C.c_int64(), C.c_int()
+
+    cold, warm, disc = C.c_double(), C.c_double(), C.c_int()
+
+    def step():
+        psi = model.predict_grid(sim, n_roi)
+        o.initial_field = psi.data_ptr()
+        _lib.check(_lib.lib.ws_solver_solve(h, len(s.values), blocks, _lib.WS_DEVICE, C.byref(o), E_w.data_ptr(),
+                                            _lib.WS_DEVICE, None, C.byref(n_it), C.byref(conv)))
+        _lib.check(_lib.lib.ws_solver_warm_report(h, 0, C.byref(cold), C.byref(warm), C.byref(disc)))
+        if disc.value:  # given up after one cycle: the cold solve decides
+            _lib.check(_lib.lib.ws_solver_solve(h, len(s.values), blocks, _lib.WS_DEVICE, C.byref(opts),
+                                                E_w.data_ptr(), _lib.WS_DEVICE, None, C.byref(n_it), C.byref(conv)))
+        return psi
+    for _ in range(max(1, args.warmup)):
+        step()
+    torch.cuda.synchronize()
+    steps = max(1, args.steps // 2)
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        step()
+    torch.cuda.synchronize()
+    ms = (time.perf_counter() - t0) * 1e3 / steps
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        model.predict_grid(sim, n_roi)
+    torch.cuda.synchronize()
+    ms_pred = (time.perf_counter() - t0) * 1e3 / steps
+    o.initial_field = None
+    diff = float((E_w - E_ref).norm() / E_ref.norm())
+    return {"ms_per_solve": ms, "ms_inference": ms_pred,
+            "iterations": int(n_it.value) + (0 if disc.value else 1),
+            "note_iterations": "loop iterations plus the cold probe iteration of a warm start",
+            "discarded": bool(disc.value), "first_cycle_energy_ratio": warm.value / cold.value,
+            "rel_l2_vs_plain": diff, "speedup_vs_plain": plain_ms / ms, "checkpoint": os.path.relpath(DEFAULT_OUT, ROOT)}
 
 
 def run_e2e(args, sim, s, keep, torch, dev):
