@@ -513,7 +513,7 @@ static InnerArgs inner_args(const Solver* s, int w) {
   a.ncols = s->lay.ncols;
   a.bpr = (int)s->lay.grid_inner;
   a.fstride = (long long)field_elems(s);
-  a.pf = s->lay.fi ? s->pf_inner : 0;
+  a.pf = 0;  // K3 (and the generic kernels) measured slower with it
   return a;
 }
 
@@ -528,7 +528,7 @@ static OuterArgs outer_args(const Solver* s, int w) {
   a.mode3d = s->lay.mode3d;
   a.bpr = (int)s->lay.grid_outer;
   a.fstride = (long long)field_elems(s);
-  a.pf = s->lay.fp ? s->pf_outer : 0;
+  a.pf = 0;  // K2 measured slower with it
   return a;
 }
 
@@ -602,6 +602,7 @@ static cudaError_t launch_k1(const Solver* s, int w, bool with_source) {
   if (s->lay.fi) {
     InnerArgs a = inner_args(s, w);
     a.ncols = s->lay.ncols;
+    a.pf = s->pf_inner;  // K1 only: its loads come first, so the next wave's columns are worth pulling early
     const float2* dE = s->d_dE;
     const float2* src = with_source ? s->d_src : nullptr;
     float2 A = make_float2(0.f, (float)(1.0f / s->eps / (float)s->nw));
