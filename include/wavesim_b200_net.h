@@ -57,12 +57,19 @@ int ws_net_features(const float* n, const float* src, int ny, int nx, int nz, fl
                     void* stream);
 
 /* Full-grid starting field psi0 (complex64, Ny x Nx x Nz column-major) from
- * the network output pred[vox][2] (the ROI envelope, voxels in the ROI's
- * column-major order): scale * pred * exp(i kz z) in the ROI, continued into
- * the boundary layers by the nearest ROI value under a cos^2 taper.  N, roi0
- * (0-based first ROI index) and roin (ROI size) as (y, x, z). */
+ * the network output (the ROI envelope): scale * pred * exp(i kz z) in the
+ * ROI, continued into the boundary layers by the nearest ROI value under a
+ * cos^2 taper.  pred is [vox][2] with voxels in the ROI's column-major order,
+ * or with s2d = 1 the half-resolution [hvox][16] of ws_net_space_to_depth
+ * (sub-voxel s at columns 2s, 2s + 1).  N, roi0 (0-based first ROI index)
+ * and roin (ROI size) as (y, x, z). */
 int ws_net_envelope_to_field(const float* pred, const int64_t N[3], const int64_t roi0[3], const int64_t roin[3],
-                             float scale, float kz, void* psi, void* stream);
+                             float scale, float kz, int s2d, void* psi, void* stream);
+
+/* Space to depth: (b, d, h, w) x C bf16 -> (b, d/2, h/2, w/2) x 8C, the
+ * 2x2x2 sub-voxel s = ((z & 1) 2 + (y & 1)) 2 + (x & 1) at channels
+ * [s C, (s + 1) C); C % 8 == 0, even sides. */
+int ws_net_space_to_depth(const void* in, void* out, int b, int d, int h, int w, int C, void* stream);
 
 /* Weights of the input-gradient convolution: Wf[ci][t Cpad + co] =
  * W[co][(26 - t) Cin + ci], zero for co >= Cout; W bf16 [Cout][kp], Wf bf16

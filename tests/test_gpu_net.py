@@ -150,11 +150,32 @@ def test_features_and_envelope_kernels(gpu):
     rn = (W.I64 * 3)(Ny, Nx, Nz)
     psi = torch.empty(int(np.prod(sim.N[:3])), dtype=torch.complex64, device="cuda")
     kz = k0 * nbg
-    W._ck(W.lib().ws_net_envelope_to_field(pred.data_ptr(), N, r0, rn, 0.5, kz, psi.data_ptr(), None), "env")
+    W._ck(W.lib().ws_net_envelope_to_field(pred.data_ptr(), N, r0, rn, 0.5, kz, 0, psi.data_ptr(), None), "env")
     got = psi.cpu().numpy().reshape(tuple(sim.N[:3]), order="F")
     field = 0.5 * env * np.exp(1j * kz * np.arange(Nz))[None, None, :]
     want = np.asarray(sim.initial_field(field))[..., 0]
     assert np.abs(got - want).max() < 1e-4 * np.abs(want).max()
+    # the same envelope in the half-resolution (space-to-depth) layout
+    half = torch.from_numpy(W.field_to_target(env, 1.0, half=True)).cuda()
+    psi2 = torch.empty_like(psi)
+    W._ck(W.lib().ws_net_envelope_to_field(half.data_ptr(), N, r0, rn, 0.5, kz, 1, psi2.data_ptr(), None), "env")
+    assert float((psi2 - psi).abs().max()) < 1e-5 * float(psi.abs().max())
+
+
+def test_space_to_depth_matches_numpy(gpu):
+    """ws_net_space_to_depth against the host layout of the training targets."""
+    import torch
+
+    from wavesim_b200 import warmstart as W
+    rng = np.random.default_rng(7)
+    shape = (16, 32, 48)  # (Ny, Nx, Nz)
+    x = rng.standard_normal((int(np.prod(shape)), 8)).astype(np.float32)
+    xb = torch.from_numpy(x).cuda().to(torch.bfloat16)
+    y = W.space_to_depth(xb, shape, torch).float().cpu().numpy()
+    Ny, Nx, Nz = shape
+    v = xb.float().cpu().numpy().reshape(Nz // 2, 2, Nx // 2, 2, Ny // 2, 2, 8)
+    want = np.transpose(v, (0, 2, 4, 1, 3, 5, 6)).reshape(-1, 64)
+    assert np.array_equal(y, want)
 
 
 def _gpu_net(widths, seed=0):

@@ -683,7 +683,7 @@ __device__ __forceinline__ float taper(int j, int lo, int n, int N) {
   return 1.f;
 }
 __global__ void k_envelope_to_field(const float* __restrict__ pred, RoiMap m, float scale, float kz,
-                                    float2* __restrict__ psi) {
+                                    float2* __restrict__ psi, int s2d) {
   const long long total = (long long)m.N[0] * m.N[1] * m.N[2];
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < total; i += (long long)gridDim.x * blockDim.x) {
     const int y = (int)(i % m.N[0]);
@@ -695,7 +695,15 @@ __global__ void k_envelope_to_field(const float* __restrict__ pred, RoiMap m, fl
     const int zc = min(max(z - m.r0[2], 0), m.rn[2] - 1);
     const float w = scale * taper(y, m.r0[0], m.rn[0], m.N[0]) * taper(x, m.r0[1], m.rn[1], m.N[1]) *
                     taper(z, m.r0[2], m.rn[2], m.N[2]);
-    const long long v = yc + (long long)m.rn[0] * (xc + (long long)m.rn[1] * zc);
+    long long v;
+    if (s2d) {
+      // half-resolution network output, sub-voxel s of the (z, x, y) volume at channels [2s, 2s + 2)
+      const int hy = m.rn[0] >> 1, hx = m.rn[1] >> 1;
+      const int s = ((zc & 1) * 2 + (xc & 1)) * 2 + (yc & 1);
+      v = ((yc >> 1) + (long long)hy * ((xc >> 1) + (long long)hx * (zc >> 1))) * 8 + s;
+    } else {
+      v = yc + (long long)m.rn[0] * (xc + (long long)m.rn[1] * zc);
+    }
     const float2 p = reinterpret_cast<const float2*>(pred)[v];
     float s, c;
     sincosf(kz * (float)zc, &s, &c);
@@ -1003,7 +1011,8 @@ extern "C" int ws_net_features(const float* n, const float* src, int ny, int nx,
 // (k_envelope_to_field).  N = grid (Ny, Nx, Nz); roi0 = first ROI index
 // (0-based), roin = ROI size, both (y, x, z); psi complex64 column-major.
 extern "C" int ws_net_envelope_to_field(const float* pred, const int64_t N[3], const int64_t roi0[3],
-                                        const int64_t roin[3], float scale, float kz, void* psi, void* stream) {
+                                        const int64_t roin[3], float scale, float kz, int s2d, void* psi,
+                                        void* stream) {
   if (!pred || !N || !roi0 || !roin || !psi) {
     t_err = "ws_net_envelope_to_field: null argument";
     return WS_ERR_INVALID_ARGUMENT;
@@ -1018,8 +1027,12 @@ extern "C" int ws_net_envelope_to_field(const float* pred, const int64_t N[3], c
     m.r0[d] = (int)roi0[d];
     m.rn[d] = (int)roin[d];
   }
+  if (s2d && ((roin[0] | roin[1] | roin[2]) & 1)) {
+    t_err = "ws_net_envelope_to_field: a half-resolution output needs even ROI sides";
+    return WS_ERR_INVALID_ARGUMENT;
+  }
   k_envelope_to_field<<<grid_for(N[0] * N[1] * N[2]), 256, 0, (cudaStream_t)stream>>>(pred, m, scale, kz,
-                                                                                      (float2*)psi);
+                                                                                      (float2*)psi, s2d);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) {
     t_err = cudaGetErrorString(e);
@@ -1109,5 +1122,43 @@ extern "C" int ws_net_add(float* y, const float* x, int64_t n, void* stream) {
   }
   if (n == 0) return WS_OK;
   k_add<<<grid_for(n), 256, 0, (cudaStream_t)stream>>>(y, x, n);
+  NET_LAUNCH_CHECK();
+}
+
+namespace ws {
+namespace net {
+// Space to depth: a (b, d, h, w) x C volume -> (b, d/2, h/2, w/2) x 8C, the
+// 2x2x2 sub-voxel s = ((z & 1) * 2 + (y & 1)) * 2 + (x & 1) at channels
+// [s C, (s + 1) C).  One thread per 16-byte chunk (C % 8 == 0).
+__global__ void k_space_to_depth(const __nv_bfloat16* __restrict__ in, __nv_bfloat16* __restrict__ out, Vol vo,
+                                 int C) {
+  const int cc = C >> 3;  // chunks per sub-voxel
+  const long long total = (long long)vo.b * vo.d * vo.h * vo.w * 8 * cc;
+  const Vol vi{vo.b, vo.d * 2, vo.h * 2, vo.w * 2};
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < total; i += (long long)gridDim.x * blockDim.x) {
+    const int q = (int)(i % (8 * cc));
+    long long r = i / (8 * cc);
+    const int x = (int)(r % vo.w); r /= vo.w;
+    const int y = (int)(r % vo.h); r /= vo.h;
+    const int z = (int)(r % vo.d);
+    const int b = (int)(r / vo.d);
+    const int s = q / cc, c8 = q - s * cc;
+    const long long src = vox_index(vi, b, 2 * z + (s >> 2), 2 * y + ((s >> 1) & 1), 2 * x + (s & 1));
+    reinterpret_cast<uint4*>(out)[i] = reinterpret_cast<const uint4*>(in + src * C)[c8];
+  }
+}
+}  // namespace net
+}  // namespace ws
+
+// (b, d, h, w) x C bf16 -> (b, d/2, h/2, w/2) x 8C (k_space_to_depth)
+extern "C" int ws_net_space_to_depth(const void* in, void* out, int b, int d, int h, int w, int C, void* stream) {
+  if (!in || !out || C % 8 || (d | h | w) & 1 || b < 1 || d < 2 || h < 2 || w < 2 || ((uintptr_t)in & 15) ||
+      ((uintptr_t)out & 15)) {
+    t_err = "ws_net_space_to_depth: need C % 8 == 0, even sides and 16-byte aligned buffers";
+    return WS_ERR_INVALID_ARGUMENT;
+  }
+  Vol vo{b, d / 2, h / 2, w / 2};
+  k_space_to_depth<<<grid_for((long long)b * d * h * w / 8 * C), 256, 0, (cudaStream_t)stream>>>(
+      (const __nv_bfloat16*)in, (__nv_bfloat16*)out, vo, C);
   NET_LAUNCH_CHECK();
 }

@@ -6,7 +6,8 @@ The training set is made by this package's own solver: seeded cubes of the
 c3 sphere distribution (radius U[0.5, 2] lambda, n = 1.5 in 1.33, 2000
 spheres per 224^3) with the c3 plane-wave source, solved to an energy ratio of
 1e-4.  Training runs on the GPU with the network's own forward and backward
-kernels (wavesim_b200.warmstart).  The checkpoint stores bf16 weights
+kernels (wavesim_b200.warmstart; the half-resolution network, ROI sides
+multiples of 16).  The checkpoint stores bf16 weights
 (``WarmStart.save(..., bf16=True)``); ``WarmStart.load`` reads it back.
 At the end the script reports, on held-out media of the training size and
 of twice it, the prediction error and the iterations of cold and

@@ -51,7 +51,9 @@ def _bind():
         "ws_conv3_fwd_bf16": [P, P, P, P, P] + [INT] * 8 + [P, P],
         "ws_conv3_upcat_fwd_bf16": [P, P, P, P, P, P] + [INT] * 9 + [P, P],
         "ws_net_features": [P, P, INT, INT, INT, C.c_float, C.c_float, P, P],
-        "ws_net_envelope_to_field": [P, C.POINTER(I64), C.POINTER(I64), C.POINTER(I64), C.c_float, C.c_float, P, P],
+        "ws_net_envelope_to_field": [P, C.POINTER(I64), C.POINTER(I64), C.POINTER(I64), C.c_float, C.c_float, INT, P,
+                                     P],
+        "ws_net_space_to_depth": [P, P, INT, INT, INT, INT, INT, P],
         "ws_net_flip_weights": [P, INT, INT, INT, P, INT, INT, P],
         "ws_net_relu_grad_bf16": [P, P, I64, INT, P, INT, P],
         "ws_net_im2col3": [P, P, INT, INT, INT, INT, INT, INT, P],
@@ -211,12 +213,12 @@ class Conv3:
 
 
 class WarmStartNet:
-    """The encoder-decoder of the module docstring."""
+    """A 4-level encoder-decoder of 3x3x3 convolutions (see the module
+    docstring) from in_ch to out_ch channels."""
 
-    IN_CH, OUT_CH = 8, 2
-
-    def __init__(self, widths=(32, 64, 96, 128), device=0, seed=0):
+    def __init__(self, widths=(32, 64, 96, 128), device=0, seed=0, in_ch=8, out_ch=2):
         import torch
+        self.IN_CH, self.OUT_CH = in_ch, out_ch
         self.torch = torch
         self.dev = torch.device("cuda", device)
         rng = np.random.default_rng(seed)
@@ -350,8 +352,8 @@ class WarmStartNet:
         out, a = self.forward(x, vol, keep=True)
         grad = torch.empty_like(out)
         loss = torch.zeros(1, dtype=torch.float64, device=self.dev)
-        _ck(lib().ws_net_mse(out.data_ptr(), target.data_ptr(), grad.data_ptr(), loss.data_ptr(), out.shape[0], 2, 2,
-                             None), "mse")
+        _ck(lib().ws_net_mse(out.data_ptr(), target.data_ptr(), grad.data_ptr(), loss.data_ptr(), out.shape[0],
+                             self.OUT_CH, self.OUT_CH, None), "mse")
         self.backward(a, grad, vol)
         self.step_count += 1
         for l in self.layers:
@@ -374,11 +376,12 @@ class WarmStartNet:
 # ----------------------------------------------------------------------------
 # inputs and outputs
 # ----------------------------------------------------------------------------
-def roi_volume(shape):
+def roi_volume(shape, half=False):
     """Network volume (b, d, h, w) of a ROI (Ny, Nx, Nz): voxels in the ROI's
-    column-major order, i.e. (z, x, y) with y fastest."""
+    column-major order, i.e. (z, x, y) with y fastest; half=True: the
+    half-resolution volume after space to depth."""
     Ny, Nx, Nz = shape
-    return (1, Nz, Nx, Ny)
+    return (1, Nz // 2, Nx // 2, Ny // 2) if half else (1, Nz, Nx, Ny)
 
 
 def _shape(n_roi):
@@ -404,22 +407,46 @@ def features(n_roi, k0, n_bg, torch, dev, src=None):
     return out
 
 
+def space_to_depth(x, shape, torch):
+    """[vox][C] bf16 of a ROI volume -> [hvox][8C] at half resolution (ws_net_space_to_depth)."""
+    b, d, h, w = roi_volume(shape)
+    C = x.shape[1]
+    y = torch.empty(x.shape[0] // 8, 8 * C, device=x.device, dtype=torch.bfloat16)
+    _ck(lib().ws_net_space_to_depth(x.data_ptr(), y.data_ptr(), b, d, h, w, C, None), "space to depth")
+    return y
+
+
 def carrier(shape, k0, n_bg):
     """exp(i k0 n_bg z) on a (y, x, z) ROI, z counted from the source plane."""
     z = np.arange(shape[2])
     return np.broadcast_to(np.exp(1j * k0 * n_bg * z)[None, None, :], shape)
 
 
-def field_to_target(env_roi, scale):
-    """Training target: the ROI envelope (y, x, z) as fp32 [vox][2], voxels in
-    the ROI's column-major order."""
-    e = np.asarray(env_roi).ravel(order="F") / scale
-    return np.stack([e.real, e.imag], axis=-1).astype(np.float32)
+def field_to_target(env_roi, scale, half=False):
+    """Training target from the ROI envelope (y, x, z): fp32 [vox][2] in the
+    ROI's column-major order, or (half=True) [hvox][16] in the
+    space-to-depth layout (sub-voxel s of the (z, x, y) volume at columns 2s,
+    2s + 1)."""
+    e = np.asarray(env_roi) / scale
+    if not half:
+        e = e.ravel(order="F")
+        return np.stack([e.real, e.imag], axis=-1).astype(np.float32)
+    Ny, Nx, Nz = e.shape
+    v = np.transpose(e, (2, 1, 0)).reshape(Nz // 2, 2, Nx // 2, 2, Ny // 2, 2)
+    v = np.transpose(v, (0, 2, 4, 1, 3, 5)).reshape(-1, 8)
+    return np.ascontiguousarray(np.stack([v.real, v.imag], axis=-1).reshape(-1, 16).astype(np.float32))
 
 
-def target_to_field(pred, shape, scale):
-    p = np.asarray(pred).reshape(-1, 2)
-    return (p[:, 0] + 1j * p[:, 1]).reshape(shape, order="F") * scale
+def target_to_field(pred, shape, scale, half=False):
+    p = np.asarray(pred)
+    if not half:
+        p = p.reshape(-1, 2)
+        return (p[:, 0] + 1j * p[:, 1]).reshape(shape, order="F") * scale
+    Ny, Nx, Nz = shape
+    c = p.reshape(-1, 8, 2)
+    c = (c[..., 0] + 1j * c[..., 1]).reshape(Nz // 2, Nx // 2, Ny // 2, 2, 2, 2)
+    c = np.transpose(c, (0, 3, 1, 4, 2, 5)).reshape(Nz, Nx, Ny)
+    return np.transpose(c, (2, 1, 0)) * scale
 
 
 def field_scale(pixel_size, lam, n_bg):
@@ -452,29 +479,44 @@ def make_training_set(count, roi=48, bw=8, seed=0, n_bg=1.33, tol=1e-4, pixel_si
 
 class WarmStart:
     """A trained network plus the normalisation of its inputs and outputs.
-    Media and fields are on the ROI, (Ny, Nx, Nz), z the propagation
-    direction, the source a plane of ones at z = 1 (the c3 benchmark's)."""
 
-    def __init__(self, net=None, n_bg=1.33, pixel_size=0.25, lam=1.0, device=0):
-        self.net = net or WarmStartNet(device=device)
+    Media and fields are on the ROI, (Ny, Nx, Nz), z the propagation
+    direction, the source a plane of ones at z = 1 (the c3 benchmark's).  The
+    network works at half resolution: the 8 input channels of 2x2x2 voxels
+    go in as 64 channels (space to depth), the 2 x 8 output channels come out
+    as the envelope of those 8 voxels, so no convolution runs on the full
+    grid.  ROI sides must be multiples of 16."""
+
+    HALF_WIDTHS = (64, 96, 128, 128)
+
+    def __init__(self, net=None, n_bg=1.33, pixel_size=0.25, lam=1.0, device=0, seed=0):
+        self.net = net or WarmStartNet(widths=self.HALF_WIDTHS, device=device, seed=seed, in_ch=64, out_ch=16)
+        self.half = self.net.IN_CH == 64
         self.n_bg, self.pixel_size, self.lam = n_bg, pixel_size, lam
         self.k0 = 2 * np.pi / lam * pixel_size  # wavenumber per pixel
         self.scale = field_scale(pixel_size, lam, n_bg)
 
-    @staticmethod
-    def _check(shape):
-        if len(shape) != 3 or any(v % 8 for v in shape):
-            raise ValueError(f"the ROI sides must be multiples of 8, got {tuple(shape)}")
+    def _check(self, shape):
+        m = 16 if self.half else 8
+        if len(shape) != 3 or any(v % m for v in shape):
+            raise ValueError(f"the ROI sides must be multiples of {m}, got {tuple(shape)}")
+
+    def _input(self, n_roi):
+        shape = _shape(n_roi)
+        x = features(n_roi, self.k0, self.n_bg, self.net.torch, self.net.dev)
+        if self.half:
+            x = space_to_depth(x, shape, self.net.torch)
+        return x, roi_volume(shape, self.half)
 
     def train(self, data, steps, lr=2e-3, lr_end=2e-4, log=None):
         torch = self.net.torch
         prepared = []
         for n, E in data:
             self._check(np.shape(n))
-            x = features(n, self.k0, self.n_bg, torch, self.net.dev)
+            x, vol = self._input(n)
             env = np.asarray(E) / carrier(np.shape(E), self.k0, self.n_bg)  # the field's envelope
-            t = torch.from_numpy(field_to_target(env, self.scale)).to(self.net.dev)
-            prepared.append((x, t, roi_volume(np.shape(n))))
+            t = torch.from_numpy(field_to_target(env, self.scale, self.half)).to(self.net.dev)
+            prepared.append((x, t, vol))
         losses = []
         for s in range(steps):
             x, t, vol = prepared[s % len(prepared)]
@@ -485,17 +527,15 @@ class WarmStart:
         return losses
 
     def envelope(self, n_roi):
-        """The network output (fp32 [vox][2] device tensor) for a ROI medium."""
-        shape = _shape(n_roi)
-        self._check(shape)
-        x = features(n_roi, self.k0, self.n_bg, self.net.torch, self.net.dev)
-        out = self.net.forward(x, roi_volume(shape))
-        return out
+        """The network output (fp32 device tensor) for a ROI medium."""
+        self._check(_shape(n_roi))
+        x, vol = self._input(n_roi)
+        return self.net.forward(x, vol)
 
     def predict(self, n_roi):
         """psi0 on the ROI (y, x, z) as a host array."""
         shape = _shape(n_roi)
-        env = target_to_field(self.envelope(n_roi).cpu().numpy(), shape, self.scale)
+        env = target_to_field(self.envelope(n_roi).cpu().numpy(), shape, self.scale, self.half)
         self.net._check_err()
         return env * carrier(shape, self.k0, self.n_bg)
 
@@ -514,7 +554,7 @@ class WarmStart:
         rn = (I64 * 3)(*[int(v) for v in shape])
         psi = torch.empty(int(np.prod(sim.N[:3])), dtype=torch.complex64, device=self.net.dev)
         _ck(lib().ws_net_envelope_to_field(pred.data_ptr(), N, r0, rn, self.scale, self.k0 * self.n_bg,
-                                           psi.data_ptr(), None), "envelope to field")
+                                           1 if self.half else 0, psi.data_ptr(), None), "envelope to field")
         self.net._check_err()
         return psi
 
@@ -524,7 +564,8 @@ class WarmStart:
         st = self.net.state()
         if bf16:
             st = {k: _to_bf16_bits(v) for k, v in st.items()}
-        st["meta"] = np.array([self.n_bg, self.pixel_size, self.lam] + list(self.net.widths), np.float64)
+        st["meta"] = np.array([self.n_bg, self.pixel_size, self.lam] + list(self.net.widths) +
+                              [self.net.IN_CH, self.net.OUT_CH], np.float64)
         np.savez_compressed(path, **st)
 
     @classmethod
@@ -532,7 +573,8 @@ class WarmStart:
         st = dict(np.load(path))
         meta = st.pop("meta")
         st = {k: (_from_bf16_bits(v) if v.dtype == np.uint16 else v) for k, v in st.items()}
-        net = WarmStartNet(widths=tuple(int(v) for v in meta[3:7]), device=device)
+        in_ch, out_ch = (int(meta[7]), int(meta[8])) if meta.size > 7 else (8, 2)
+        net = WarmStartNet(widths=tuple(int(v) for v in meta[3:7]), device=device, in_ch=in_ch, out_ch=out_ch)
         net.load(st)
         return cls(net, n_bg=float(meta[0]), pixel_size=float(meta[1]), lam=float(meta[2]), device=device)
 
