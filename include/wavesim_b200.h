@@ -201,7 +201,10 @@ int ws_solver_buffers(ws_solver s, void** E_prime, void** stream);
  * ms_out[0] forward inner (wiggle + source + inner FFT),
  * ms_out[1] outer (FFT, Green's function, inverse FFT),
  * ms_out[2] inverse inner (inverse FFT, unwiggle, mix, accumulate, energy).
- * bytes_out[3] (may be NULL): algorithmic bytes each launch moves. */
+ * bytes_out[3] (may be NULL): algorithmic bytes each launch moves (for the
+ * inverse inner kernel the mean of an odd and an even iteration: with an
+ * even number of wiggles E' takes the increments in pairs, after even
+ * iterations only, and every stop of the loop falls after an even one). */
 int ws_solver_time_kernels(ws_solver s, int n_iterations, float ms_out[3], double bytes_out[3]);
 
 /* Number of kernel launches one iteration makes. */

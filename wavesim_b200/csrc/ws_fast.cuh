@@ -343,6 +343,8 @@ __global__ void __launch_bounds__(kThreads, 2)
   const int rhs = blockIdx.x / a.bpr, bid = blockIdx.x - rhs * a.bpr;
   st += rhs;
   if (load_done(st)) return;
+  // with a.acc2, E' takes dE'_{k-1} + dE'_k after even iterations k only
+  const bool acc_now = !a.acc2 || (__ldcg(&st->it) & 1) == 0;
   T += rhs * a.fstride;
   dE += rhs * a.fstride;
   E += rhs * a.fstride;
@@ -375,7 +377,7 @@ __global__ void __launch_bounds__(kThreads, 2)
     const int comp0 = DO_X ? comp : (int)(colbase / nx);
     const int comp1 = DO_X ? comp : (int)((colbase + ncol - 1) / nx);
     prefetch_l2(dE + c0 * N, bytes);
-    prefetch_l2(E + c0 * N, bytes);
+    if (acc_now) prefetch_l2(E + c0 * N, bytes);
     if (comp0 == comp1) prefetch_l2(gamma + c0 * N - (long long)comp0 * g.npts, bytes);
   }
   if (a.pf && bid + a.pf < a.bpr) {
@@ -487,7 +489,7 @@ __global__ void __launch_bounds__(kThreads, 2)
           const int y = p + P * (8 * h + i);
           gm[i] = gmc[y];
           d0[i] = dEc[y];
-          e0[i] = Ec[y];
+          e0[i] = acc_now ? Ec[y] : make_float2(0.f, 0.f);
         }
 #pragma unroll
         for (int i = 0; i < 8; ++i) {
@@ -498,7 +500,7 @@ __global__ void __launch_bounds__(kThreads, 2)
           const float2 t = cmul(cmul(gm[i], gm[i]), ep);
           const float2 dn = cadd(cmul(one_m, d0[i]), make_float2(kAlpha * t.y, -kAlpha * t.x));
           dEc[y] = dn;
-          Ec[y] = cadd(e0[i], dn);
+          if (acc_now) Ec[y] = cadd(e0[i], a.acc2 ? cadd(d0[i], dn) : dn);
           if (in_xzc && y >= g.r0[0] && y < g.r1[0]) esum = fmaf(dn.x, dn.x, fmaf(dn.y, dn.y, esum));
         }
       }

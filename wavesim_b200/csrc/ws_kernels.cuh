@@ -96,6 +96,7 @@ struct InnerArgs {
   int bpr;      // blocks per right-hand side (a batch of sources runs as consecutive block ranges)
   long long fstride;  // elements between the fields of consecutive right-hand sides
   int pf;       // fast kernels: block b pulls the inputs of block b + pf into L2 (0: off)
+  int acc2;     // K3: E' += dE' in pairs, every second iteration (Nw even; 0: every iteration)
 };
 
 struct OuterArgs {
@@ -323,6 +324,8 @@ __global__ void __launch_bounds__(512, 1) k_inv_inner(InnerArgs a, const float2*
   const int rhs = blockIdx.x / a.bpr, bid = blockIdx.x - rhs * a.bpr;
   st += rhs;
   if (load_done(st)) return;
+  // with a.acc2, E' takes dE'_{k-1} + dE'_k after even iterations k only
+  const bool acc_now = !a.acc2 || (__ldcg(&st->it) & 1) == 0;
   T += rhs * a.fstride;
   dE += rhs * a.fstride;
   E += rhs * a.fstride;
@@ -388,8 +391,10 @@ __global__ void __launch_bounds__(512, 1) k_inv_inner(InnerArgs a, const float2*
     const float2 t = cmul(g2, ep);
     const float2 dn = cadd(cmul(one_m, d0), make_float2(kAlpha * t.y, -kAlpha * t.x));
     dE[gi] = dn;
-    const float2 e0 = E[gi];
-    E[gi] = cadd(e0, dn);
+    if (acc_now) {
+      const float2 e0 = E[gi];
+      E[gi] = cadd(e0, a.acc2 ? cadd(d0, dn) : dn);
+    }
     if (y >= g.r0[0] && y < g.r1[0] && x >= g.r0[1] && x < g.r1[1] && z >= g.r0[2] && z < g.r1[2] &&
         c >= g.r0[3] && c < g.r1[3])
       esum = fmaf(dn.x, dn.x, fmaf(dn.y, dn.y, esum));

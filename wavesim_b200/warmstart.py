@@ -487,7 +487,7 @@ class WarmStart:
     as the envelope of those 8 voxels, so no convolution runs on the full
     grid.  ROI sides must be multiples of 16."""
 
-    HALF_WIDTHS = (64, 96, 128, 128)
+    HALF_WIDTHS = (32, 64, 96, 128)
 
     def __init__(self, net=None, n_bg=1.33, pixel_size=0.25, lam=1.0, device=0, seed=0):
         self.net = net or WarmStartNet(widths=self.HALF_WIDTHS, device=device, seed=seed, in_ch=64, out_ch=16)
