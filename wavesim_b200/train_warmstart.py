@@ -55,7 +55,7 @@ def main(argv=None):
     report = {"samples": args.samples, "roi": args.roi, "steps": args.steps, "params": model.net.nparams,
               "data_s": t_data, "train_s": t_train, "final_loss": float(np.mean(losses[-50:])), "eval": []}
     rng = np.random.default_rng(12345)
-    for roi in (args.roi, 2 * args.roi):
+    for roi in [args.roi] + ([2 * args.roi] if 2 * args.roi <= 128 else []):
         for _ in range(args.eval):
             n = sphere_medium(roi, rng)
             opt = {"lambda": 1.0, "pixel_size": 0.25, "boundary_widths": [args.boundary] * 3}
