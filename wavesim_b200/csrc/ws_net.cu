@@ -474,7 +474,7 @@ constexpr unsigned conv_smem_bytes() {
   return S * ConvTile<NT>::kStage + 1024;
 }
 
-template <int NT, int S>
+template <int NT, int S, bool UP>
 __global__ void __launch_bounds__(kGemmThreads)
     k_conv3(ConvIn in, const __nv_bfloat16* __restrict__ W, const float* __restrict__ bias, float* __restrict__ out32,
             __nv_bfloat16* __restrict__ outb, int M, int Cout, int kp, int mode, int* __restrict__ err) {
@@ -505,19 +505,38 @@ __global__ void __launch_bounds__(kGemmThreads)
   const int chunk = tid & 7;
   const int C = in.Cu + in.Cx;
   const int hd = in.d >> 1, hh = in.h >> 1, hw = in.w >> 1;
-  int vz[8], vy[8], vx[8], vb[8];
+  // UP: the coordinates of each row (the upsampled part needs them per tap);
+  // else the linear voxel index and a 27-bit mask of the taps that fall
+  // inside the volume, so that a tap costs one add and one bit test per row
+  constexpr int NR = UP ? 8 : 1;
+  int vz[NR], vy[NR], vx[NR], vb[NR];
+  int vlin[8];
+  uint32_t vmask[8];
 #pragma unroll
   for (int i = 0; i < 8; ++i) {
     const int vox = m0 + (tid >> 3) + 16 * i;
+    int x = 0, y = 0, z = 0, b = -1;
     if (vox < M) {
       int r = vox;
-      vx[i] = r % in.w; r /= in.w;
-      vy[i] = r % in.h; r /= in.h;
-      vz[i] = r % in.d;
-      vb[i] = r / in.d;
+      x = r % in.w; r /= in.w;
+      y = r % in.h; r /= in.h;
+      z = r % in.d;
+      b = r / in.d;
+    }
+    if constexpr (UP) {
+      vz[i] = z;
+      vy[i] = y;
+      vx[i] = x;
+      vb[i] = b;
     } else {
-      vb[i] = -1;
-      vz[i] = vy[i] = vx[i] = 0;
+      const uint32_t mz = (z > 0 ? 1u : 0u) | 2u | (z < in.d - 1 ? 4u : 0u);
+      const uint32_t my = (y > 0 ? 1u : 0u) | 2u | (y < in.h - 1 ? 4u : 0u);
+      const uint32_t mx = (x > 0 ? 1u : 0u) | 2u | (x < in.w - 1 ? 4u : 0u);
+      uint32_t m = 0;
+#pragma unroll
+      for (int t = 0; t < 27; ++t) m |= ((mz >> (t / 9)) & (my >> ((t / 3) % 3)) & (mx >> (t % 3)) & 1u) << t;
+      vmask[i] = b >= 0 ? m : 0u;
+      vlin[i] = vox;
     }
   }
   const uint32_t swz = (uint32_t)((chunk ^ ((tid >> 3) & 7)) << 4);  // row & 7 is the same for all 8 rows
@@ -528,21 +547,33 @@ __global__ void __launch_bounds__(kGemmThreads)
     const int tap = k / C;
     const int ch = k - tap * C;
     const int dz = tap / 9 - 1, dy = (tap / 3) % 3 - 1, dx = tap % 3 - 1;
-    const bool up = ch < in.Cu;
+    if constexpr (UP) {
+      const bool up = ch < in.Cu;
 #pragma unroll
-    for (int i = 0; i < 8; ++i) {
-      const int row = (tid >> 3) + 16 * i;
-      const int z = vz[i] + dz, y = vy[i] + dy, x = vx[i] + dx;
-      const bool ok = tap < 27 && vb[i] >= 0 && (unsigned)z < (unsigned)in.d && (unsigned)y < (unsigned)in.h &&
-                      (unsigned)x < (unsigned)in.w;
-      const __nv_bfloat16* src = in.X;
-      if (ok) {
-        if (up)
-          src = in.U + ((((long long)vb[i] * hd + (z >> 1)) * hh + (y >> 1)) * hw + (x >> 1)) * in.Cu + ch;
-        else
-          src = in.X + ((((long long)vb[i] * in.d + z) * in.h + y) * in.w + x) * in.Cx + (ch - in.Cu);
+      for (int i = 0; i < 8; ++i) {
+        const int row = (tid >> 3) + 16 * i;
+        const int z = vz[i] + dz, y = vy[i] + dy, x = vx[i] + dx;
+        const bool ok = tap < 27 && vb[i] >= 0 && (unsigned)z < (unsigned)in.d && (unsigned)y < (unsigned)in.h &&
+                        (unsigned)x < (unsigned)in.w;
+        const __nv_bfloat16* src = in.X;
+        if (ok) {
+          if (up)
+            src = in.U + ((((long long)vb[i] * hd + (z >> 1)) * hh + (y >> 1)) * hw + (x >> 1)) * in.Cu + ch;
+          else
+            src = in.X + ((((long long)vb[i] * in.d + z) * in.h + y) * in.w + x) * in.Cx + (ch - in.Cu);
+        }
+        cp_async16(sa + row * 128 + swz, src, ok ? 16u : 0u);
       }
-      cp_async16(sa + row * 128 + swz, src, ok ? 16u : 0u);
+    } else {
+      const int toff = (dz * in.h + dy) * in.w + dx;
+      const int tsh = tap < 27 ? tap : 31;  // bit 31 of a mask is never set
+#pragma unroll
+      for (int i = 0; i < 8; ++i) {
+        const int row = (tid >> 3) + 16 * i;
+        const bool ok = (vmask[i] >> tsh) & 1u;
+        const __nv_bfloat16* src = ok ? in.X + (long long)(vlin[i] + toff) * in.Cx + ch : in.X;
+        cp_async16(sa + row * 128 + swz, src, ok ? 16u : 0u);
+      }
     }
 #pragma unroll
     for (int i = 0; i < (NT * 8) / kGemmThreads; ++i) {
@@ -902,7 +933,7 @@ extern "C" int ws_net_f32_to_bf16(const float* in, void* out, int64_t n, void* s
 
 // Launches k_conv3 with the smallest output-channel tile that holds Cout
 // (Cout > 128: tiles of 128 across blockIdx.y); voxel tiles across blockIdx.x.
-template <int NT, int S>
+template <int NT, int S, bool UP>
 static int launch_conv3(const ConvIn& in, const void* W, const float* bias, float* out_f32, void* out_bf16, int M,
                         int Cout, int kp, int mode, int* err, cudaStream_t stream) {
   constexpr unsigned smem = conv_smem_bytes<NT, S>();
@@ -911,7 +942,7 @@ static int launch_conv3(const ConvIn& in, const void* W, const float* bias, floa
   cudaGetDevice(&dev);
   if (dev < 0 || dev >= 64) dev = 0;
   if (!attr[dev]) {
-    cudaError_t e = cudaFuncSetAttribute(k_conv3<NT, S>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    cudaError_t e = cudaFuncSetAttribute(k_conv3<NT, S, UP>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) {
       t_err = std::string("conv3: ") + cudaGetErrorString(e);
       return WS_ERR_CUDA;
@@ -923,7 +954,7 @@ static int launch_conv3(const ConvIn& in, const void* W, const float* bias, floa
     t_err = "conv3: too many output channels";
     return WS_ERR_INVALID_ARGUMENT;
   }
-  k_conv3<NT, S><<<dim3((unsigned)mt, (unsigned)nt), kGemmThreads, smem, stream>>>(
+  k_conv3<NT, S, UP><<<dim3((unsigned)mt, (unsigned)nt), kGemmThreads, smem, stream>>>(
       in, (const __nv_bfloat16*)W, bias, out_f32, (__nv_bfloat16*)out_bf16, M, Cout, kp, mode, err);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) {
@@ -931,6 +962,16 @@ static int launch_conv3(const ConvIn& in, const void* W, const float* bias, floa
     return WS_ERR_CUDA;
   }
   return WS_OK;
+}
+
+template <bool UP>
+static int conv3_dispatch(const ConvIn& in, const void* W, const float* bias, float* out_f32, void* out_bf16, int M,
+                          int Cout, int kp, int mode, int* err, cudaStream_t st) {
+  if (Cout <= 16) return launch_conv3<16, 4, UP>(in, W, bias, out_f32, out_bf16, M, Cout, kp, mode, err, st);
+  if (Cout <= 32) return launch_conv3<32, 4, UP>(in, W, bias, out_f32, out_bf16, M, Cout, kp, mode, err, st);
+  if (Cout <= 64) return launch_conv3<64, 4, UP>(in, W, bias, out_f32, out_bf16, M, Cout, kp, mode, err, st);
+  if (Cout <= 96) return launch_conv3<96, 3, UP>(in, W, bias, out_f32, out_bf16, M, Cout, kp, mode, err, st);
+  return launch_conv3<128, 3, UP>(in, W, bias, out_f32, out_bf16, M, Cout, kp, mode, err, st);
 }
 
 static int conv3_fwd(const ConvIn& in, const void* W, const float* bias, float* out_f32, void* out_bf16, int Cout,
@@ -964,11 +1005,8 @@ static int conv3_fwd(const ConvIn& in, const void* W, const float* bias, float* 
     err_flag = dummy[dev];
   }
   cudaStream_t st = (cudaStream_t)stream;
-  if (Cout <= 16) return launch_conv3<16, 4>(in, W, bias, out_f32, out_bf16, (int)M, Cout, kp, mode, err_flag, st);
-  if (Cout <= 32) return launch_conv3<32, 4>(in, W, bias, out_f32, out_bf16, (int)M, Cout, kp, mode, err_flag, st);
-  if (Cout <= 64) return launch_conv3<64, 4>(in, W, bias, out_f32, out_bf16, (int)M, Cout, kp, mode, err_flag, st);
-  if (Cout <= 96) return launch_conv3<96, 3>(in, W, bias, out_f32, out_bf16, (int)M, Cout, kp, mode, err_flag, st);
-  return launch_conv3<128, 3>(in, W, bias, out_f32, out_bf16, (int)M, Cout, kp, mode, err_flag, st);
+  if (in.Cu) return conv3_dispatch<true>(in, W, bias, out_f32, out_bf16, (int)M, Cout, kp, mode, err_flag, st);
+  return conv3_dispatch<false>(in, W, bias, out_f32, out_bf16, (int)M, Cout, kp, mode, err_flag, st);
 }
 
 // Forward 3x3x3 convolution (zero padding 1) as an implicit GEMM on the
