@@ -218,6 +218,17 @@ int ws_solver_launches_per_iteration(ws_solver s);
 int ws_solver_warm_report(ws_solver s, int64_t rhs, double* cold_first_energy, double* warm_cycle_energy,
                           int* discarded);
 
+/* Autotuner (no counterpart in the reference): times the kernel layouts the
+ * solver's grid supports - the power-of-two fast kernels or the generic
+ * mixed-radix ones for the inner and the outer pass, the generic outer
+ * pass's y tile, the 2-D columns per block - over n_iterations iterations
+ * each, keeps the fastest inner and outer pass, and uses them from the next
+ * solve on.  A candidate must first reproduce one iteration of the current
+ * layout to 1e-4.  Outputs (may be NULL): candidates tried, and the time of
+ * one iteration (K1 + K2 + K3, ms) before and after.  Overwrites the solver's
+ * fields; call it between solves. */
+int ws_solver_autotune(ws_solver s, int n_iterations, int* n_tried, float* ms_before, float* ms_after);
+
 int ws_solver_destroy(ws_solver s);
 
 /*

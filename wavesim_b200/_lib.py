@@ -63,7 +63,8 @@ class ws_solve_options(C.Structure):
 EXPORTS = [
     "ws_default_options", "ws_version", "ws_last_error", "ws_size_supported", "ws_run_algorithm",
     "ws_solver_create", "ws_solver_solve", "ws_solver_solve_batch", "ws_solver_buffers", "ws_solver_time_kernels",
-    "ws_solver_launches_per_iteration", "ws_solver_warm_report", "ws_solver_destroy", "ws_run_algorithm_noalloc",
+    "ws_solver_launches_per_iteration", "ws_solver_warm_report", "ws_solver_autotune", "ws_solver_destroy",
+    "ws_run_algorithm_noalloc",
     "ws_noalloc_scratch_bytes", "ws_noalloc_last_error",
 ]
 
@@ -112,6 +113,8 @@ def _load():
     lib.ws_solver_warm_report.argtypes = [P, C.c_int64, C.POINTER(C.c_double), C.POINTER(C.c_double),
                                           C.POINTER(C.c_int)]
     lib.ws_solver_warm_report.restype = C.c_int
+    lib.ws_solver_autotune.argtypes = [P, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_float), C.POINTER(C.c_float)]
+    lib.ws_solver_autotune.restype = C.c_int
     lib.ws_solver_destroy.argtypes = [P]
     lib.ws_solver_destroy.restype = C.c_int
     lib.ws_run_algorithm_noalloc.argtypes = [i64p, P, C.c_int64, C.POINTER(ws_wiggle), P, C.c_float, ws_complex,

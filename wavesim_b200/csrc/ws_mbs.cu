@@ -121,7 +121,20 @@ struct Layout {
 
 static bool is_pow2(long long n) { return n >= 1 && (n & (n - 1)) == 0; }
 
-static int make_layout(const Geom& g, Layout& L, std::string& why) {
+// Overrides of the layout heuristics, for the autotuner (0 = heuristic).
+struct LayoutChoice {
+  int inner = 0;  // 1: fast inner kernels when a shape matches, 2: generic
+  int outer = 0;  // 1: fast pencil when a shape matches, 2: generic
+  int csize = 0;  // 3-D generic: smallest blocks per plane to try
+  int ncols = 0;  // 2-D generic: columns per block
+  int ty = 0;     // generic outer: consecutive y per block
+  bool operator==(const LayoutChoice& o) const {
+    return inner == o.inner && outer == o.outer && csize == o.csize && ncols == o.ncols && ty == o.ty;
+  }
+};
+
+static int make_layout(const Geom& g, Layout& L, std::string& why, const LayoutChoice& ch = LayoutChoice{}) {
+  L = Layout{};
   L.mode3d = g.nz > 1;
   L.rset = kPow2;
   for (long long n : {(long long)g.ny, (long long)g.nx, (long long)g.nz})
@@ -137,7 +150,7 @@ static int make_layout(const Geom& g, Layout& L, std::string& why) {
   if (L.mode3d) {
     // smallest divisor C of Nx (<= 16) whose tile fits
     int best = 0;
-    for (int c = 1; c <= 16; ++c) {
+    for (int c = ch.csize ? ch.csize : 1; c <= 16; ++c) {
       if (g.nx % c) continue;
       const long long cols = g.nx / c;
       const long long elems = cols * ny;
@@ -167,6 +180,7 @@ static int make_layout(const Geom& g, Layout& L, std::string& why) {
     // aim for >= 2 blocks per SM, at most ~8K elements per block
     long long want = std::max(1LL, std::min(max_cols_fit, (8192LL + ny - 1) / ny));
     while (want > 1 && (total_cols + want - 1) / want < 2 * kNumSms) want /= 2;
+    if (ch.ncols) want = std::max(1LL, std::min<long long>(ch.ncols, max_cols_fit));
     L.ncols = (int)want;
     L.th_inner = threads_for((long long)want * ny);
     L.smem_inner = want * col_bytes;
@@ -181,6 +195,7 @@ static int make_layout(const Geom& g, Layout& L, std::string& why) {
     ty /= 2;
   if (ty > g.ny) ty = std::max(1, g.ny);
   while (ty > 4 && ((g.ny + ty - 1) / ty) * mids < 2 * kNumSms) ty /= 2;
+  if (ch.ty) ty = std::max(1, std::min(ch.ty, g.ny));
   if ((long long)padded(g.nc * ty) * no * sizeof(float2) > kSmemBudget ||
       (long long)g.nc * ty * no > (long long)kMaxThreads * kEmax) {
     why = "outer dimension too long for one block";
@@ -194,6 +209,7 @@ static int make_layout(const Geom& g, Layout& L, std::string& why) {
   const char* path = std::getenv("WAVESIM_B200_PATH");
   if (path && std::strcmp(path, "generic") == 0) return WS_OK;
   for (const FastInner& f : fast_inner_table()) {
+    if (ch.inner == 2) break;
     if (L.mode3d && f.do_x && g.ny == f.n && g.nx == f.n) L.fi = &f;
     if (!L.mode3d && !f.do_x && g.ny == f.n) L.fi = &f;
   }
@@ -205,7 +221,7 @@ static int make_layout(const Geom& g, Layout& L, std::string& why) {
     L.grid_inner = (total_cols + want - 1) / want;
   }
   if (L.fi && L.mode3d) L.grid_inner = (long long)g.nz * g.nc * L.fi->c;
-  if (g.nc == 1) {
+  if (g.nc == 1 && ch.outer != 2) {
     for (const FastPencil& f : fast_pencil_table())
       if (f.no == no && g.ny % f.ty == 0) L.fp = &f;
   }
@@ -253,9 +269,11 @@ struct Solver {
   long long hist_cap = 0;
   double* d_energy = nullptr;
   double* d_partials = nullptr;  // per-block ROI energy of K3
+  long long partials_cap = 0;    // elements of d_partials
   float2* d_init = nullptr;      // warm starts: v = gamma psi0 / Nw per right-hand side (batch_cap of them)
   int pf_inner = 0, pf_outer = 0;  // L2 prefetch distance of the fast kernels, in blocks (0: off)
   bool warm = false;             // the current solve starts from d_init
+  LayoutChoice tuned{};          // the autotuner's choice (all zero: the heuristics)
   double warm_ratio = 0.0;       // discard threshold of the current solve
   float2* d_tw = nullptr;
   FftPlan py{}, pxl{}, po{};
@@ -378,6 +396,18 @@ static cudaMemcpyKind kind_from(int memory) { return memory == WS_DEVICE ? cudaM
 static size_t field_elems(const Solver* s) { return (size_t)s->g.npts * s->g.nc; }
 
 // Buffers for nrhs right-hand sides (kept when large enough).
+// d_partials holds at least n per-block energies (graphs hold the old pointer)
+static int ensure_partials(Solver* s, long long n) {
+  if (n <= s->partials_cap) return WS_OK;
+  double* p = nullptr;
+  WS_CUDA(cudaMalloc(&p, (size_t)n * sizeof(double)));
+  if (s->d_partials) cudaFree(s->d_partials);
+  s->d_partials = p;
+  s->partials_cap = n;
+  free_graph(s);
+  return WS_OK;
+}
+
 static int ensure_batch(Solver* s, int nrhs) {
   if (nrhs <= s->batch_cap) return WS_OK;
   void* old[] = {s->d_E, s->d_dE, s->d_T, s->d_src, s->d_state, s->d_energy, s->d_partials, s->d_init};
@@ -398,7 +428,8 @@ static int ensure_batch(Solver* s, int nrhs) {
   WS_CUDA(cudaMalloc(&s->d_src, nb));
   WS_CUDA(cudaMalloc(&s->d_state, nrhs * sizeof(DevState)));
   WS_CUDA(cudaMalloc(&s->d_energy, nrhs * sizeof(double)));
-  WS_CUDA(cudaMalloc(&s->d_partials, (size_t)std::max<long long>(1, s->lay.grid_inner) * nrhs * sizeof(double)));
+  s->partials_cap = std::max<long long>(1, s->lay.grid_inner) * nrhs;
+  WS_CUDA(cudaMalloc(&s->d_partials, (size_t)s->partials_cap * sizeof(double)));
   WS_CUDA(cudaMemset(s->d_E, 0, nb));
   WS_CUDA(cudaMemset(s->d_dE, 0, nb));
   WS_CUDA(cudaMemset(s->d_state, 0, nrhs * sizeof(DevState)));
@@ -874,6 +905,8 @@ static int solve_batch(Solver* s, int nrhs, const int64_t* counts, const ws_sour
     return fail(WS_ERR_INVALID_ARGUMENT, "batch too large for one launch");
   int rc = ensure_batch(s, nrhs);
   if (rc) return rc;
+  rc = ensure_partials(s, s->lay.grid_inner * (long long)nrhs);
+  if (rc) return rc;
   if (s->nrhs != nrhs) free_graph(s);
   s->nrhs = nrhs;
   std::vector<double> src_energy;
@@ -1134,6 +1167,191 @@ int ws_solver_warm_report(ws_solver h, int64_t rhs, double* cold_first_energy, d
   if (cold_first_energy) *cold_first_energy = st.diff1;
   if (warm_cycle_energy) *warm_cycle_energy = s->warm ? st.warm_e : -1.0;
   if (discarded) *discarded = s->warm ? st.discarded : 0;
+  return WS_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Autotuner: among the kernel layouts this grid supports (fast power-of-two
+// kernels or the generic mixed-radix ones for the inner and the outer pass,
+// the generic outer pass's y tile, the 2-D columns per block), keep the
+// fastest inner and the fastest outer pass.  Each candidate first runs one
+// iteration from a fixed field and must reproduce the current layout's
+// increment to 1e-4; only then is it timed.
+// ---------------------------------------------------------------------------
+}  // extern "C"
+
+namespace ws {
+static __global__ void k_fill_pattern(float2* __restrict__ a, long long n) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    unsigned h = (unsigned)(i * 2654435761u) ^ (unsigned)(i >> 32) * 2246822519u;
+    h ^= h >> 15;
+    h *= 2246822519u;
+    h ^= h >> 13;
+    a[i] = make_float2((float)(h & 0xffff) / 65536.f - 0.5f, (float)(h >> 16) / 65536.f - 0.5f);
+  }
+}
+// out[0] = max |a - b|, out[1] = max |b| (float bits of non-negative values compare as unsigned)
+static __global__ void k_max_diff(const float2* __restrict__ a, const float2* __restrict__ b, long long n,
+                                  unsigned* __restrict__ out) {
+  float d = 0.f, m = 0.f;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    const float2 u = a[i], v = b[i];
+    d = fmaxf(d, fmaxf(fabsf(u.x - v.x), fabsf(u.y - v.y)));
+    m = fmaxf(m, fmaxf(fabsf(v.x), fabsf(v.y)));
+  }
+  if (!(d == d)) d = __int_as_float(0x7f800000);  // NaN counts as a mismatch
+  atomicMax(out, __float_as_uint(d));
+  atomicMax(out + 1, __float_as_uint(m));
+}
+
+// One iteration (wiggle 0, no source) from the fixed pattern; dE' -> out.
+static int tune_probe(Solver* s, const StopRule& rule, const Hist& hh, float2* out) {
+  const long long n = (long long)field_elems(s);
+  const unsigned blocks = (unsigned)std::min<long long>((n + 255) / 256, 8 * kNumSms);
+  k_fill_pattern<<<blocks, 256, 0, s->stream>>>(s->d_dE, n);
+  k_resume_state<<<1, 32, 0, s->stream>>>(s->d_state);
+  WS_CUDA(cudaGetLastError());
+  WS_CUDA(launch_k1(s, 0, false));
+  WS_CUDA(launch_k2(s, 0));
+  WS_CUDA(launch_k3_only(s, 0));
+  WS_CUDA(launch_finish(s, rule, hh));
+  WS_CUDA(cudaMemcpyAsync(out, s->d_dE, n * sizeof(float2), cudaMemcpyDeviceToDevice, s->stream));
+  WS_CUDA(cudaStreamSynchronize(s->stream));
+  return WS_OK;
+}
+
+static int tune_time(Solver* s, const StopRule& rule, const Hist& hh, int iters, float ms[3]) {
+  k_resume_state<<<1, 32, 0, s->stream>>>(s->d_state);
+  float acc[3] = {0, 0, 0};
+  for (int i = 0; i < iters; ++i) {
+    const int w = i % s->nw;
+    WS_CUDA(cudaEventRecord(s->ev[0], s->stream));
+    WS_CUDA(launch_k1(s, w, false));
+    WS_CUDA(cudaEventRecord(s->ev[1], s->stream));
+    WS_CUDA(launch_k2(s, w));
+    WS_CUDA(cudaEventRecord(s->ev[2], s->stream));
+    WS_CUDA(launch_k3_only(s, w));
+    WS_CUDA(cudaEventRecord(s->ev[3], s->stream));
+    WS_CUDA(launch_finish(s, rule, hh));
+    WS_CUDA(cudaEventSynchronize(s->ev[3]));
+    float t;
+    for (int k = 0; k < 3; ++k) {
+      WS_CUDA(cudaEventElapsedTime(&t, s->ev[k], s->ev[k + 1]));
+      acc[k] += t;
+    }
+  }
+  for (int k = 0; k < 3; ++k) ms[k] = acc[k] / iters;
+  return WS_OK;
+}
+}  // namespace ws
+
+extern "C" {
+
+int ws_solver_autotune(ws_solver h, int n_iterations, int* n_tried, float* ms_before, float* ms_after) {
+  if (!h || n_iterations < 1) return fail(WS_ERR_INVALID_ARGUMENT, "bad argument");
+  Solver* s = reinterpret_cast<Solver*>(h);
+  WS_CUDA(cudaSetDevice(s->device));
+  if (s->hist_cap < 2) {
+    const int rc = ensure_hist(s, 2);
+    if (rc) return rc;
+  }
+  StopRule rule{s->nw, 1, 0, 1, (long long)1 << 62, -1.0};
+  Hist hh{s->d_hist, s->d_hist + s->hist_cap, 0, 0};  // cap 0: history untouched
+  s->nrhs = 1;
+  free_graph(s);
+  const long long n = (long long)field_elems(s);
+  float2* ref = nullptr;
+  float2* got = nullptr;
+  unsigned* dmax = nullptr;
+  auto cleanup = [&]() {
+    if (ref) cudaFree(ref);
+    if (got) cudaFree(got);
+    if (dmax) cudaFree(dmax);
+  };
+  if (cudaMalloc(&ref, n * sizeof(float2)) != cudaSuccess || cudaMalloc(&got, n * sizeof(float2)) != cudaSuccess ||
+      cudaMalloc(&dmax, 2 * sizeof(unsigned)) != cudaSuccess) {
+    cleanup();
+    return fail(WS_ERR_OUT_OF_MEMORY, "autotune: no memory for the probe fields");
+  }
+  const Layout base = s->lay;
+  int rc = tune_probe(s, rule, hh, ref);
+  float base_ms[3];
+  if (!rc) rc = tune_time(s, rule, hh, n_iterations, base_ms);
+  if (rc) {
+    cleanup();
+    return rc;
+  }
+  // candidates
+  std::vector<LayoutChoice> inner_c, outer_c;
+  inner_c.push_back(LayoutChoice{1, 0, 0, 0, 0});
+  inner_c.push_back(LayoutChoice{2, 0, 0, 0, 0});
+  if (!base.mode3d)
+    for (int f : {4, 2, -2})
+      inner_c.push_back(LayoutChoice{2, 0, 0, f > 0 ? std::max(1, base.ncols / f) : base.ncols * 2, 0});
+  outer_c.push_back(LayoutChoice{0, 1, 0, 0, 0});
+  for (int t : {1, 2, 4, 8, 16}) outer_c.push_back(LayoutChoice{0, 2, 0, 0, t});
+  int tried = 0;
+  LayoutChoice best_in{}, best_out{};
+  float t_in = base_ms[0] + base_ms[2], t_out = base_ms[1];
+  auto evaluate = [&](const LayoutChoice& c, float ms[3]) -> bool {
+    Layout L;
+    std::string why;
+    if (make_layout(s->g, L, why, c) != WS_OK) return false;
+    if (ensure_partials(s, L.grid_inner * std::max(1, s->batch_cap)) != WS_OK) return false;
+    s->lay = L;
+    bool ok = tune_probe(s, rule, hh, got) == WS_OK;
+    if (ok) {
+      unsigned hmax[2] = {0, 0};
+      cudaMemsetAsync(dmax, 0, 2 * sizeof(unsigned), s->stream);
+      k_max_diff<<<(unsigned)std::min<long long>((n + 255) / 256, 8 * kNumSms), 256, 0, s->stream>>>(got, ref, n,
+                                                                                                  dmax);
+      ok = cudaMemcpyAsync(hmax, dmax, sizeof(hmax), cudaMemcpyDeviceToHost, s->stream) == cudaSuccess &&
+           cudaStreamSynchronize(s->stream) == cudaSuccess;
+      float d, m;
+      std::memcpy(&d, &hmax[0], 4);
+      std::memcpy(&m, &hmax[1], 4);
+      ok = ok && d <= 1e-4f * m;
+    }
+    if (ok) ok = tune_time(s, rule, hh, n_iterations, ms) == WS_OK;
+    s->lay = base;
+    cudaGetLastError();  // a launch refused for a candidate must not leak into later calls
+    ++tried;
+    return ok;
+  };
+  for (const LayoutChoice& c : inner_c) {
+    float ms[3];
+    if (evaluate(c, ms) && ms[0] + ms[2] < 0.97f * t_in) {
+      t_in = ms[0] + ms[2];
+      best_in = c;
+    }
+  }
+  for (const LayoutChoice& c : outer_c) {
+    float ms[3];
+    if (evaluate(c, ms) && ms[1] < 0.97f * t_out) {
+      t_out = ms[1];
+      best_out = c;
+    }
+  }
+  LayoutChoice fin = best_in;
+  fin.outer = best_out.outer;
+  fin.ty = best_out.ty;
+  float fin_ms[3] = {base_ms[0], base_ms[1], base_ms[2]};
+  if (!(fin == LayoutChoice{})) {
+    if (!evaluate(fin, fin_ms)) {
+      fin = LayoutChoice{};
+      std::memcpy(fin_ms, base_ms, sizeof(fin_ms));
+    } else {
+      Layout L;
+      std::string why;
+      make_layout(s->g, L, why, fin);
+      s->lay = L;
+    }
+  }
+  s->tuned = fin;
+  cleanup();
+  if (n_tried) *n_tried = tried;
+  if (ms_before) *ms_before = base_ms[0] + base_ms[1] + base_ms[2];
+  if (ms_after) *ms_after = fin_ms[0] + fin_ms[1] + fin_ms[2];
   return WS_OK;
 }
 
