@@ -153,6 +153,9 @@ int ws_size_supported(const int64_t N[4]);
  *          stops at the first multiple of Nwiggles >= max_iterations);
  *          receives the per-iteration energy history; *n_iterations its length.
  * callback / user_data: may be NULL.
+ * The device buffers of a call are kept (one set per device) and reused by
+ * the next call on the same grid with the same wiggle count, which then
+ * uploads only the medium; ws_run_algorithm_release frees them.
  */
 int ws_run_algorithm(const int64_t N[4], const ws_complex* gamma, int64_t n_wiggles, const ws_wiggle* wiggles,
                      int64_t n_blocks, const ws_source_block* source, float epsilon, ws_complex k02e,
@@ -160,6 +163,9 @@ int ws_run_algorithm(const int64_t N[4], const ws_complex* gamma, int64_t n_wigg
                      const char* callback_string, int64_t callback_interval, ws_callback_fn callback,
                      void* user_data, int memory, ws_complex* E_out, double* diff_energy_out,
                      int64_t* n_iterations);
+
+/* Frees the device buffers ws_run_algorithm keeps between calls. */
+void ws_run_algorithm_release(void);
 
 /* ws_solver_create - uploads (or references, for WS_DEVICE) the medium and
  * wiggle data once, plans the FFTs and allocates the iteration buffers, so

@@ -62,6 +62,7 @@ class ws_solve_options(C.Structure):
 # every entry point declared in include/wavesim_b200.h
 EXPORTS = [
     "ws_default_options", "ws_version", "ws_last_error", "ws_size_supported", "ws_run_algorithm",
+    "ws_run_algorithm_release",
     "ws_solver_create", "ws_solver_solve", "ws_solver_solve_batch", "ws_solver_buffers", "ws_solver_time_kernels",
     "ws_solver_launches_per_iteration", "ws_solver_warm_report", "ws_solver_autotune", "ws_solver_destroy",
     "ws_run_algorithm_noalloc",

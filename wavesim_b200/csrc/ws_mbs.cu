@@ -14,6 +14,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <string>
+#include <mutex>
 #include <vector>
 
 #include "wavesim_b200.h"
@@ -532,6 +533,43 @@ static int create_solver(const int64_t N[4], const ws_complex* gamma, int64_t n_
   return WS_OK;
 }
 
+// A new medium (gamma, wiggles, epsilon, k02e, roi) of the same grid and
+// wiggle count into an existing solver: uploads only, no allocation.  The
+// solver's stream must be idle (it is after a solve returns).
+static int reload_medium(Solver* s, const int64_t N[4], const ws_complex* gamma, int64_t n_wiggles,
+                         const ws_wiggle* wiggles, float epsilon, ws_complex k02e, const int64_t roi[8], int memory) {
+  Geom g{};
+  int rc = check_args(N, n_wiggles, wiggles, gamma, roi, g);
+  if (rc) return rc;
+  WS_CUDA(cudaSetDevice(s->device));
+  const cudaMemcpyKind kind = kind_from(memory);
+  const size_t nf = (size_t)g.nx + g.ny + g.nz;
+  for (int w = 0; w < n_wiggles; ++w) {
+    const ws_wiggle& W = wiggles[w];
+    if (!W.pxe || !W.pye || !W.pze || !W.gx || !W.gy || !W.gz) return fail(WS_ERR_INVALID_ARGUMENT, "null wiggle array");
+    float* f = s->d_wigf + nf * w;
+    float2* c = s->d_wigc + nf * w;
+    WS_CUDA(cudaMemcpy(f, W.pxe, g.nx * sizeof(float), kind));
+    WS_CUDA(cudaMemcpy(f + g.nx, W.pye, g.ny * sizeof(float), kind));
+    WS_CUDA(cudaMemcpy(f + g.nx + g.ny, W.pze, g.nz * sizeof(float), kind));
+    WS_CUDA(cudaMemcpy(c, W.gx, g.nx * sizeof(float2), kind));
+    WS_CUDA(cudaMemcpy(c + g.nx, W.gy, g.ny * sizeof(float2), kind));
+    WS_CUDA(cudaMemcpy(c + g.nx + g.ny, W.gz, g.nz * sizeof(float2), kind));
+  }
+  WS_CUDA(cudaMemcpy(s->d_gamma, gamma, (size_t)g.npts * sizeof(float2), kind));
+  const float2 k = make_float2(k02e.re, k02e.im);
+  bool same = s->eps == epsilon && s->k02e.x == k.x && s->k02e.y == k.y;
+  for (int d = 0; d < 4; ++d) same = same && s->g.r0[d] == g.r0[d] && s->g.r1[d] == g.r1[d];
+  if (!same) {
+    // scalars and the roi are kernel arguments inside the graph
+    s->eps = epsilon;
+    s->k02e = k;
+    s->g = g;
+    free_graph(s);
+  }
+  return WS_OK;
+}
+
 static InnerArgs inner_args(const Solver* s, int w) {
   InnerArgs a{};
   a.g = s->g;
@@ -1042,6 +1080,11 @@ static int solve(Solver* s, int64_t n_blocks, const ws_source_block* src, int so
 
 using namespace ws;
 
+// ws_run_algorithm's solver of the previous call, per device
+static constexpr int kRunCacheDevices = 64;
+static Solver* g_run_cache[kRunCacheDevices] = {};
+static std::mutex g_run_mu;
+
 extern "C" {
 
 void ws_default_options(ws_solve_options* o) {
@@ -1368,9 +1411,23 @@ int ws_run_algorithm(const int64_t N[4], const ws_complex* gamma, int64_t n_wigg
                      int64_t* n_iterations) {
   int dev = 0;
   cudaGetDevice(&dev);
-  Solver* s = nullptr;
-  int rc = create_solver(N, gamma, n_wiggles, wiggles, epsilon, k02e, roi, memory, dev, &s);
-  if (rc) return rc;
+  if (dev < 0 || dev >= kRunCacheDevices) return fail(WS_ERR_INVALID_ARGUMENT, "device ordinal beyond the call cache");
+  std::lock_guard<std::mutex> lock(g_run_mu);
+  // the solver of the previous call on this device is reused when the grid
+  // and the wiggle count match: only the medium is uploaded again
+  Solver*& s = g_run_cache[dev];
+  int rc = WS_ERR_INVALID_ARGUMENT;
+  if (s && N && s->g.ny == N[0] && s->g.nx == N[1] && s->g.nz == N[2] && s->g.nc == N[3] && s->nw == n_wiggles)
+    rc = reload_medium(s, N, gamma, n_wiggles, wiggles, epsilon, k02e, roi, memory);
+  if (rc) {
+    destroy_solver(s);
+    s = nullptr;
+    rc = create_solver(N, gamma, n_wiggles, wiggles, epsilon, k02e, roi, memory, dev, &s);
+    if (rc) {
+      s = nullptr;
+      return rc;
+    }
+  }
   ws_solve_options o;
   ws_default_options(&o);
   o.max_iterations = max_iterations;
@@ -1381,8 +1438,19 @@ int ws_run_algorithm(const int64_t N[4], const ws_complex* gamma, int64_t n_wigg
   o.callback = callback;
   o.user_data = user_data;
   rc = solve(s, n_blocks, source, memory, &o, E_out, memory, diff_energy_out, n_iterations, nullptr);
-  destroy_solver(s);
+  if (rc && rc != WS_ERR_DIVERGED && rc != WS_ERR_NO_SOURCE && rc != WS_ERR_INVALID_ARGUMENT) {
+    destroy_solver(s);  // after a CUDA error start afresh next time
+    s = nullptr;
+  }
   return rc;
+}
+
+void ws_run_algorithm_release(void) {
+  std::lock_guard<std::mutex> lock(g_run_mu);
+  for (Solver*& s : g_run_cache) {
+    destroy_solver(s);
+    s = nullptr;
+  }
 }
 
 }  // extern "C"
