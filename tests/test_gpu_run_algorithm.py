@@ -11,7 +11,7 @@ import pytest
 pytestmark = pytest.mark.gpu
 
 
-def _call(sim, source, maxit=400):
+def _call(sim, source, maxit=100000):
     from wavesim_b200 import _lib
     s, blocks, keep = sim.source_blocks(source)
     E = np.zeros(int(np.prod(sim.N)), np.complex64)
