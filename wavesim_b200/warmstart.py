@@ -146,9 +146,11 @@ class Conv3:
                                     _ptr(err), None), "conv fwd")
         return y
 
-    def forward_upcat(self, u, skip, vol, cu, cs, err=None):
+    def forward_upcat_fused(self, u, skip, vol, cu, cs, err=None):
         """The layer on [nearest x2 upsampling of u (cu channels), skip (cs
-        channels)] at the resolution `vol`, without writing the concat."""
+        channels)] at the resolution `vol`, without writing the concat (the
+        kernel computes the upsampled coordinates per tap: slower than
+        writing the concat first, see forward_upcat)."""
         torch = self.torch
         b, d, h, w = vol
         y = torch.empty(b * d * h * w, self.cout, device=skip.device, dtype=torch.bfloat16)
@@ -157,6 +159,17 @@ class Conv3:
                                           y.data_ptr(), b, d, h, w, cu, cs, self.cout, self.kp, mode, _ptr(err), None),
             "conv upcat fwd")
         return y
+
+    def forward_upcat(self, u, skip, vol, cu, cs, err=None):
+        """The layer on [nearest x2 upsampling of u (cu channels), skip (cs
+        channels)]: the concat is written once (ws_net_upcat) and read by the
+        plain convolution, whose gather is cheaper than the fused one's.
+        Returns (output, concat)."""
+        torch = self.torch
+        b, d, h, w = vol
+        cat = torch.empty(b * d * h * w, cu + cs, device=skip.device, dtype=torch.bfloat16)
+        _ck(lib().ws_net_upcat(u.data_ptr(), skip.data_ptr(), cat.data_ptr(), b, d, h, w, cu, cs, None), "upcat")
+        return self.forward(cat, vol, err=err), cat
 
     def backward(self, x, y, dy, vol, need_dx=True, err=None):
         """x: layer input (bf16 [vox][cin]); y: its ReLU output (bf16) or None
@@ -284,17 +297,14 @@ class WarmStartNet:
         a["p3"] = self._pool(a["e3"], v3, w3)
         a["b4a"] = self.c4a.forward(a["p3"], v4, err=err)
         a["b4"] = self.c4b.forward(a["b4a"], v4, err=err)
-        a["d3a"] = self.d3a.forward_upcat(a["b4"], a["e3"], v3, w4, w3, err=err)
+        a["d3a"], a["u3"] = self.d3a.forward_upcat(a["b4"], a["e3"], v3, w4, w3, err=err)
         a["d3"] = self.d3b.forward(a["d3a"], v3, err=err)
-        a["d2a"] = self.d2a.forward_upcat(a["d3"], a["e2"], v2, w3, w2, err=err)
+        a["d2a"], a["u2"] = self.d2a.forward_upcat(a["d3"], a["e2"], v2, w3, w2, err=err)
         a["d2"] = self.d2b.forward(a["d2a"], v2, err=err)
-        a["d1a"] = self.d1a.forward_upcat(a["d2"], a["e1"], v1, w2, w1, err=err)
+        a["d1a"], a["u1"] = self.d1a.forward_upcat(a["d2"], a["e1"], v1, w2, w1, err=err)
         a["d1"] = self.d1b.forward(a["d1a"], v1, err=err)
         out = self.head.forward(a["d1"], v1, out_f32=True, err=err)
         if keep:
-            a["u3"] = self._upcat(a["b4"], a["e3"], v3, w4, w3)
-            a["u2"] = self._upcat(a["d3"], a["e2"], v2, w3, w2)
-            a["u1"] = self._upcat(a["d2"], a["e1"], v1, w2, w1)
             return out, a
         return out
 
