@@ -238,6 +238,28 @@ int ws_solver_autotune(ws_solver s, int n_iterations, int* n_tried, float* ms_be
 int ws_solver_destroy(ws_solver s);
 
 /*
+ * Medium set-up on the device (no counterpart in the reference, which builds
+ * gamma in MATLAB on the host; WaveSimBase.m:58-81, 201-258, Medium.m:44-62).
+ * n is the refractive index of the ROI, Ny*Nx*Nz column-major, complex
+ * double (is_complex = 1) or double, in device memory.
+ *
+ * ws_medium_reduce: out[0] = min real(n^2), out[1] = max real(n^2) (e_r_min,
+ * e_r_max of Medium.m:45-47); with k0sq > 0 also out[2] = max |n^2 k0^2 -
+ * k0c^2| (epsilon = max(out[2] / 0.95, 3), WaveSimBase.m:201-215).
+ * ws_build_gamma: gamma = (i/epsilon)(e_r k0^2 - k0c^2 - i epsilon) fy fx fz
+ * on the full Ny x Nx x Nz grid (complex64, device), e_r = n^2 replicated
+ * into the boundary layers (the ROI starts at roi_lo, 0-based), fy/fx/fz the
+ * 1-D ARL windows (device floats of lengths Ny, Nx, Nz).  Computed in double,
+ * rounded once.  ws_setup_last_error gives the message of a failure.
+ */
+int ws_medium_reduce(const void* n, int is_complex, int64_t count, double k0sq, double k0c2, double out[3],
+                     void* stream);
+int ws_build_gamma(const void* n, int is_complex, const int64_t roi_size[3], const int64_t N[3],
+                   const int64_t roi_lo[3], const float* fy, const float* fx, const float* fz, double k0sq,
+                   double k0c2, double epsilon, void* gamma, void* stream);
+const char* ws_setup_last_error(void);
+
+/*
  * ws_run_algorithm_noalloc - the same loop as ws_run_algorithm for callers
  * that cannot allocate GPU memory (an application that owns the device
  * through its own memory pool, a real-time loop that forbids allocation after

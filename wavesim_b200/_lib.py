@@ -65,7 +65,7 @@ EXPORTS = [
     "ws_run_algorithm_release",
     "ws_solver_create", "ws_solver_solve", "ws_solver_solve_batch", "ws_solver_buffers", "ws_solver_time_kernels",
     "ws_solver_launches_per_iteration", "ws_solver_warm_report", "ws_solver_autotune", "ws_solver_destroy",
-    "ws_run_algorithm_noalloc",
+    "ws_run_algorithm_noalloc", "ws_medium_reduce", "ws_build_gamma", "ws_setup_last_error",
     "ws_noalloc_scratch_bytes", "ws_noalloc_last_error",
 ]
 
@@ -116,6 +116,12 @@ def _load():
     lib.ws_solver_warm_report.restype = C.c_int
     lib.ws_solver_autotune.argtypes = [P, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_float), C.POINTER(C.c_float)]
     lib.ws_solver_autotune.restype = C.c_int
+    i64a = C.POINTER(C.c_int64)
+    lib.ws_medium_reduce.argtypes = [P, C.c_int, C.c_int64, C.c_double, C.c_double, C.POINTER(C.c_double), P]
+    lib.ws_medium_reduce.restype = C.c_int
+    lib.ws_build_gamma.argtypes = [P, C.c_int, i64a, i64a, i64a, P, P, P, C.c_double, C.c_double, C.c_double, P, P]
+    lib.ws_build_gamma.restype = C.c_int
+    lib.ws_setup_last_error.restype = C.c_char_p
     lib.ws_solver_destroy.argtypes = [P]
     lib.ws_solver_destroy.restype = C.c_int
     lib.ws_run_algorithm_noalloc.argtypes = [i64p, P, C.c_int64, C.POINTER(ws_wiggle), P, C.c_float, ws_complex,
@@ -137,6 +143,12 @@ lib = _load()
 def check(status):
     if status != WS_OK:
         raise WaveSimError(status, lib.ws_last_error().decode(errors="replace"))
+    return status
+
+
+def check_setup(status):
+    if status != WS_OK:
+        raise WaveSimError(status, lib.ws_setup_last_error().decode(errors="replace"))
     return status
 
 

@@ -16,7 +16,7 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-shared", "-I" + os.path.join(ROOT, "include")]
 
 TARGETS = {
-    "libwavesim_b200.so": ["ws_mbs.cu", "ws_noalloc.cu", "ws_net.cu"],
+    "libwavesim_b200.so": ["ws_mbs.cu", "ws_noalloc.cu", "ws_net.cu", "ws_setup.cu"],
 }
 
 

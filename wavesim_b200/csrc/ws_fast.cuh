@@ -148,7 +148,7 @@ struct PlaneGeom {
 // K1
 // ----------------------------------------------------------------------------
 template <int N, int C, bool DO_X>
-__global__ void __launch_bounds__(kThreads, 2)
+__global__ void __launch_bounds__(kThreads, 3)
     kf_plane_fwd(InnerArgs a, const float2* __restrict__ dE, const float2* __restrict__ src, float2 A,
                  float2* __restrict__ T, const DevState* __restrict__ st) {
   using G = PlaneGeom<N, C, DO_X>;
@@ -284,7 +284,7 @@ __global__ void __launch_bounds__(kThreads, 2)
 // K2: outer-dimension pencils of length NO, TY consecutive y per block
 // ----------------------------------------------------------------------------
 template <int NO, int TY>
-__global__ void __launch_bounds__(TY*(NO / 16) < 1024 ? TY*(NO / 16) : 1024)
+__global__ void __launch_bounds__(TY*(NO / 16) < 1024 ? TY*(NO / 16) : 1024, 3)
     kf_pencil(OuterArgs a, float2* __restrict__ T, const DevState* __restrict__ st) {
   constexpr int P = NO / 16;
   constexpr int TYS = TY + 1;

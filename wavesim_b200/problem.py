@@ -98,7 +98,10 @@ class SimulationGrid:
 class Medium:
     """Medium.m:15-132: e_r = n^2 with replicated edges added as boundary."""
 
-    def __init__(self, refractive_index, options):
+    def __init__(self, refractive_index, options, build_field=True):
+        """build_field=False: the checks and the grid geometry only (the
+        field set-up then runs on the device, WaveSim option device_setup);
+        self.n keeps the ROI's refractive index."""
         n = as_field(refractive_index)
         if np.iscomplexobj(n) and (n.imag < 0).any():
             raise ValueError("Medium cannot have gain, imaginary part of refractive index should be positive")
@@ -111,16 +114,20 @@ class Medium:
             raise ValueError("boundary_widths array is too long")
         if np.any(np.round(bw) != bw):
             raise ValueError("boundary_widths should be integer numbers")
-        e_r = n.astype(complex if np.iscomplexobj(n) else float) ** 2
-        self.e_r_min = float(np.real(e_r).min())
-        self.e_r_max = float(np.real(e_r).max())
-        self.e_r_center = 0.5 * (self.e_r_min + self.e_r_max)
-        sz = np.array(e_r.shape[:3], dtype=np.int64)
+        sz = np.array(n.shape[:3], dtype=np.int64)
         bw2 = _pad3(bw * 2, 0).astype(np.int64)
         self.grid = SimulationGrid(sz + bw2, options["pixel_size"], bw2 == 0)
         extra = self.grid.N - sz
         self.Bl = (extra + 1) // 2   # ceil
         self.Br = extra // 2         # floor
+        self.n = n
+        if not build_field:
+            self.e_r = None
+            return
+        e_r = n.astype(complex if np.iscomplexobj(n) else float) ** 2
+        self.e_r_min = float(np.real(e_r).min())
+        self.e_r_max = float(np.real(e_r).max())
+        self.e_r_center = 0.5 * (self.e_r_min + self.e_r_max)
         e_r = np.pad(e_r, [(int(a), int(b)) for a, b in zip(self.Bl, self.Br)], mode="edge")
         if self.boundary_type[:3] == "PBL" and (self.Bl != 0).any():
             e_r = self._pbl(e_r, options)

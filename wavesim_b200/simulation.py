@@ -79,7 +79,10 @@ class WaveSim:
         self.use_graph = bool(o.get("use_graph", True))
         self.warm_discard_ratio = o.get("warm_discard_ratio", None)  # None: 2 Nw (set with the wiggles)
 
-        self.sample = Medium(refractive_index, o)
+        # device_setup: e_r, V, the ARL window and gamma are built on the GPU
+        # (wavesim_b200/csrc/ws_setup.cu) instead of in NumPy; same values
+        self.device_setup = bool(o.get("device_setup", False)) and o.get("boundary_type", "ARL") == "ARL"
+        self.sample = Medium(refractive_index, o, build_field=not self.device_setup)
         self.grid = self.sample.grid
         self.N = np.concatenate([self.grid.N, [1]]).astype(np.int64)
         lo = self.sample.Bl + 1
@@ -92,15 +95,19 @@ class WaveSim:
             self.roi[:, :3] += lo - 1
 
         k0 = 2 * np.pi / self.lambda_
-        k0c = np.sqrt(self.sample.e_r_center) * k0
-        if "epsilon" in o:
-            eps = float(o["epsilon"])
-        else:  # WaveSimBase.m:201-215
-            eps = max(float(np.abs(self.sample.e_r * k0 ** 2 - k0c ** 2).max()) / 0.95, 3.0)
+        self._gamma_host = self._gamma_dev = None
+        if self.device_setup:
+            eps, k0c = self._setup_on_device(k0, o)
+        else:
+            k0c = np.sqrt(self.sample.e_r_center) * k0
+            if "epsilon" in o:
+                eps = float(o["epsilon"])
+            else:  # WaveSimBase.m:201-215
+                eps = max(float(np.abs(self.sample.e_r * k0 ** 2 - k0c ** 2).max()) / 0.95, 3.0)
+            V = self.sample.e_r * k0 ** 2 - k0c ** 2 - 1.0j * eps
+            V = V * self._edge_filter()
+            self._gamma_host = (1.0j / eps * V).astype(np.complex64)
         self.iterations_per_cycle = self.lambda_ / (2 * k0c / eps)
-        V = self.sample.e_r * k0 ** 2 - k0c ** 2 - 1.0j * eps
-        V = V * self._edge_filter()
-        self.gamma = (1.0j / eps * V).astype(np.complex64)
         self.k02e = np.complex64(k0c ** 2 / eps + 1.0j)
         self.epsilon = np.float32(eps)
         self.k0, self.k0c = k0, k0c
@@ -118,10 +125,11 @@ class WaveSim:
         self._solver = None
 
     # WaveSimBase.apply_edge_filters (WaveSimBase.m:217-258): separable ARL window
-    def _edge_filter(self):
-        F = np.ones(tuple(self.grid.N))
+    def _edge_windows(self):
+        """The three 1-D factors (y, x, z) of the ARL edge window."""
+        out = [np.ones(int(self.grid.N[d])) for d in range(3)]
         if self.sample.boundary_type != "ARL" or (self.sample.Bl == 0).all():
-            return F
+            return out
         bw = np.ravel(self.options["boundary_widths"])
         linear = bool((self.grid.N > 1).all())
         for d in range(3):
@@ -136,11 +144,51 @@ class WaveSim:
                 win = lambda B, nw=nw: nw[:B]  # noqa: E731
             step = np.concatenate([[0.0], win(L - 1)]) if bl == br else win(L)
             core = int(self.grid.N[d]) - bl - br
-            f = np.concatenate([np.zeros(bl - L), step, np.ones(core), step[::-1], np.zeros(br - L)])
-            shape = [1, 1, 1]
-            shape[d] = f.size
-            F = F * f.reshape(shape)
-        return F
+            out[d] = np.concatenate([np.zeros(bl - L), step, np.ones(core), step[::-1], np.zeros(br - L)])
+        return out
+
+    def _edge_filter(self):
+        fy, fx, fz = self._edge_windows()
+        return fy[:, None, None] * fx[None, :, None] * fz[None, None, :]
+
+    def _setup_on_device(self, k0, o):
+        """e_r statistics, epsilon and gamma on the GPU (ws_setup.cu); returns
+        (epsilon, k0c).  The same formulas as the host path, in double."""
+        import torch
+        dev = torch.device("cuda", self.device)
+        n = self.sample.n[..., 0] if self.sample.n.ndim == 4 else self.sample.n
+        cplx = bool(np.iscomplexobj(n))
+        flat = np.ascontiguousarray(np.ravel(n, order="F").astype(np.complex128 if cplx else np.float64))
+        nd = torch.from_numpy(flat.view(np.float64)).to(dev)
+        stats = (C.c_double * 3)()
+        L = _lib.lib
+        _lib.check_setup(L.ws_medium_reduce(nd.data_ptr(), int(cplx), n.size, 0.0, 0.0, stats, None))
+        s = self.sample
+        s.e_r_min, s.e_r_max = stats[0], stats[1]
+        s.e_r_center = 0.5 * (s.e_r_min + s.e_r_max)
+        k0c = np.sqrt(s.e_r_center) * k0
+        if "epsilon" in o:
+            eps = float(o["epsilon"])
+        else:  # WaveSimBase.m:201-215
+            _lib.check_setup(L.ws_medium_reduce(nd.data_ptr(), int(cplx), n.size, k0 ** 2, k0c ** 2, stats, None))
+            eps = max(stats[2] / 0.95, 3.0)
+        wins = [torch.from_numpy(w.astype(np.float32)).to(dev) for w in self._edge_windows()]
+        gamma = torch.empty(int(np.prod(self.grid.N)), dtype=torch.complex64, device=dev)
+        N3 = (C.c_int64 * 3)(*[int(v) for v in self.grid.N])
+        R3 = (C.c_int64 * 3)(*[int(v) for v in n.shape])
+        lo = (C.c_int64 * 3)(*[int(v) for v in self.sample.Bl])
+        _lib.check_setup(L.ws_build_gamma(nd.data_ptr(), int(cplx), R3, N3, lo, wins[0].data_ptr(), wins[1].data_ptr(),
+                                          wins[2].data_ptr(), k0 ** 2, k0c ** 2, eps, gamma.data_ptr(), None))
+        torch.cuda.synchronize(dev)
+        self._gamma_dev = gamma
+        return eps, k0c
+
+    @property
+    def gamma(self):
+        """gamma = (i/epsilon) V F on the full grid, [y, x, z] complex64 (host)."""
+        if self._gamma_host is None:
+            self._gamma_host = self._gamma_dev.cpu().numpy().reshape(tuple(int(v) for v in self.grid.N), order="F")
+        return self._gamma_host
 
     # WaveSimBase.compute_wiggles / wiggle_descriptor (WaveSimBase.m:272-316)
     def _wiggles(self, acc):
@@ -180,13 +228,30 @@ class WaveSim:
         """The ws_solver for this medium (created once; set-up uploaded once)."""
         if self._solver is None:
             N = (C.c_int64 * 4)(*[int(v) for v in self.N])
-            gamma = np.asfortranarray(self.gamma)
-            wig = self._wiggle_structs()
             h = C.c_void_p()
-            _lib.check(_lib.lib.ws_solver_create(
-                N, gamma.ctypes.data, len(self.wiggles), wig, C.c_float(self.epsilon),
-                _lib.ws_complex(self.k02e.real, self.k02e.imag), self._roi8(), _lib.WS_HOST, self.device,
-                C.byref(h)))
+            if self._gamma_dev is not None:
+                # everything from device memory: gamma stays where it was built
+                import torch
+                dev = self._gamma_dev.device
+                keep = []
+                wig = (_lib.ws_wiggle * len(self.wiggles))()
+                for i, w in enumerate(self.wiggles):
+                    parts = [torch.from_numpy(np.ascontiguousarray(a).view(np.float32)).to(dev)
+                             for a in (w.pxe, w.pye, w.pze, w.gx, w.gy, w.gz)]
+                    keep.extend(parts)
+                    wig[i] = _lib.ws_wiggle(*[t.data_ptr() for t in parts])
+                _lib.check(_lib.lib.ws_solver_create(
+                    N, self._gamma_dev.data_ptr(), len(self.wiggles), wig, C.c_float(self.epsilon),
+                    _lib.ws_complex(self.k02e.real, self.k02e.imag), self._roi8(), _lib.WS_DEVICE, self.device,
+                    C.byref(h)))
+                del keep
+            else:
+                gamma = np.asfortranarray(self.gamma)
+                wig = self._wiggle_structs()
+                _lib.check(_lib.lib.ws_solver_create(
+                    N, gamma.ctypes.data, len(self.wiggles), wig, C.c_float(self.epsilon),
+                    _lib.ws_complex(self.k02e.real, self.k02e.imag), self._roi8(), _lib.WS_HOST, self.device,
+                    C.byref(h)))
             self._solver = h
         return self._solver
 
