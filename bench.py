@@ -51,6 +51,7 @@ def parse():
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-warm", action="store_true", help="skip the learned warm-start leg")
     p.add_argument("--batch", type=int, default=4, help="right-hand sides of the batched leg (0: skip)")
+    p.add_argument("--media", type=int, default=8, help="media of mixed sizes in the concurrent leg (0: skip)")
     return p.parse_args()
 
 
@@ -150,7 +151,7 @@ def build_problem(config):
     import wavesim_b200 as ws
     n, opt, val, pos, vector = workloads.CONFIGS[config]()
     t = time.time()
-    sim = (ws.WaveSimVector if vector else ws.WaveSim)(n, opt)
+    sim = (ws.WaveSimVector if vector else ws.WaveSim)(n, dict(opt, device_setup=True))
     return sim, ws.Source(val, pos), time.time() - t, (n, opt, val, pos, vector)
 
 
@@ -307,6 +308,8 @@ def run_ours(args):
             legs["batched"] = run_batched(args, sim, h, stream, torch, dev, value)
         if not args.no_warm:
             legs["warm_start"] = run_warm(args, sim, h, s, blocks, opts, torch, dev, E_dev, value)
+        if args.media > 0:
+            legs["mixed_media"] = run_media(args)
 
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
@@ -448,6 +451,46 @@ def run_warm(args, sim, h, s, blocks, opts, torch, dev, E_plain, plain_ms):
             "note_iterations": "loop iterations plus the cold probe iteration of a warm start",
             "discarded": bool(disc.value), "first_cycle_energy_ratio": warm.value / cold.value,
             "rel_l2_vs_plain": diff, "speedup_vs_plain": plain_ms / ms, "checkpoint": os.path.relpath(DEFAULT_OUT, ROOT)}
+
+
+def run_media(args):
+    """args.media seeded media of mixed sizes (2-D 256^2-1024^2 Gaussian
+    random media with a Gaussian-beam edge source, 3-D 64^3-192^3 cubes of the
+    sphere distribution with a plane wave), set up on the device, solved one
+    at a time and then concurrently (wavesim_b200.batch.solve_many, one
+    solver stream per medium, 4 host threads); solves/s of both."""
+    import wavesim_b200 as ws
+    from wavesim_b200.batch import solve_many
+    from wavesim_b200.workloads import PPW, gaussian_random_field, sphere_medium
+    rng = np.random.default_rng(48)
+    probs, sizes = [], []
+    t0 = time.perf_counter()
+    for i in range(args.media):
+        if i % 2 == 0:
+            side = int(rng.choice([256, 384, 512, 768, 1024]))
+            n = np.clip(1.0 + 0.3 * gaussian_random_field((side, side), PPW, rng), 0.8, 1.6) + 0.01j
+            opt = {"lambda": 1.0, "pixel_size": 1.0 / PPW, "boundary_widths": [32, 32], "energy_threshold": 1e-3,
+                   "device_setup": True}
+            y = np.arange(side)
+            src = ws.Source(np.exp(-((y - side / 2) ** 2) / (4 * PPW) ** 2)[:, None], [1, 1])
+            sizes.append(f"2d {side}^2")
+        else:
+            side = int(rng.choice([64, 96, 128, 160, 192]))
+            n = sphere_medium(side, rng)
+            opt = {"lambda": 1.0, "pixel_size": 1.0 / PPW, "boundary_widths": [16, 16, 16], "energy_threshold": 1e-3,
+                   "device_setup": True}
+            src = ws.Source(np.ones((side, side)), [1, 1, 1])
+            sizes.append(f"3d {side}^3")
+        probs.append((ws.WaveSim(n, opt), src))
+    setup_s = time.perf_counter() - t0
+    solve_many(probs, workers=1)  # warm-up: solvers, graphs
+    _, st_seq, t_seq = solve_many(probs, workers=1)
+    _, st_par, t_par = solve_many(probs, workers=4)
+    for sim, _ in probs:
+        sim.close()
+    return {"media": sizes, "host_setup_s": setup_s, "iterations": [s.it - 1 for s in st_seq],
+            "sequential_solves_per_s": len(probs) / t_seq, "concurrent_solves_per_s": len(probs) / t_par,
+            "speedup": t_seq / t_par, "timing": "host wall clock around the solves (set-up excluded)"}
 
 
 def run_e2e(args, sim, s, keep, torch, dev):
