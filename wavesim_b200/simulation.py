@@ -291,8 +291,11 @@ class WaveSim:
     def roi_medium(self):
         """The (real) refractive index on the ROI, [y, x, z]."""
         r = self.roi
-        n = np.sqrt(np.asarray(self.sample.e_r))
-        return np.real(n[r[0, 0] - 1:r[1, 0], r[0, 1] - 1:r[1, 1], r[0, 2] - 1:r[1, 2]]).astype(np.float32)
+        lo = [int(r[0, d]) - 1 - int(self.sample.Bl[d]) for d in range(3)]  # into the medium as given
+        hi = [int(r[1, d]) - int(self.sample.Bl[d]) for d in range(3)]
+        n = np.asarray(self.sample.n)
+        n = n[..., 0] if n.ndim == 4 else n
+        return np.real(n[lo[0]:hi[0], lo[1]:hi[1], lo[2]:hi[2]]).astype(np.float32)
 
     def initial_field(self, psi0):
         """A starting field psi0 on the full grid (complex64, column-major, as
