@@ -58,6 +58,47 @@ __device__ __forceinline__ void prefetch_l2(const void* p, unsigned bytes) {
   asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(p), "r"(bytes) : "memory");
 }
 
+// Cluster exchange by push: st.async of a float2 into another block's shared
+// memory, completing on that block's mbarrier (bytes counted), so that the
+// sender never waits on a remote load and the receiver waits once.
+__device__ __forceinline__ uint32_t smem_addr(const void* p) {
+  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+__device__ __forceinline__ uint32_t map_rank(uint32_t addr, int rank) {
+  uint32_t r;
+  asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(r) : "r"(addr), "r"(rank));
+  return r;
+}
+__device__ __forceinline__ void st_async_f2(uint32_t raddr, float2 v, uint32_t rbar) {
+  asm volatile("st.async.shared::cluster.mbarrier::complete_tx::bytes.v2.f32 [%0], {%1, %2}, [%3];" ::"r"(raddr),
+               "f"(v.x), "f"(v.y), "r"(rbar)
+               : "memory");
+}
+__device__ __forceinline__ void mbar_init_expect(uint64_t* bar, uint32_t bytes) {
+  const uint32_t a = smem_addr(bar);
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(a));
+  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(a), "r"(bytes) : "memory");
+}
+// Waits for phase 0 of the barrier (the pushed bytes all arrived); gives up
+// after about 5e7 clocks and then returns false.
+__device__ __forceinline__ bool mbar_wait_cluster(uint64_t* bar) {
+  const uint32_t a = smem_addr(bar);
+  const long long t0 = clock64();
+  while (true) {
+    uint32_t done;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.acquire.cluster.shared::cta.b64 p, [%1], 0;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(done)
+        : "r"(a)
+        : "memory");
+    if (done) return true;
+    if (clock64() - t0 > 50000000LL) return false;
+  }
+}
+
 struct SyncWarp {
   __device__ __forceinline__ void operator()() const { __syncwarp(); }
 };
@@ -140,7 +181,11 @@ struct PlaneGeom {
   static constexpr int LPR = kThreads / P;     // lines per round
   static constexpr size_t smem_a = (size_t)(M + 1) * CS * sizeof(float2);  // + scratch column
   static constexpr size_t smem_b = (size_t)N * CS2 * sizeof(float2);
-  static constexpr size_t smem = (C > 1 && DO_X) ? (smem_a > smem_b ? smem_a : smem_b) : smem_a;
+  // K1 with a cluster: one round of column scratch + the received rows
+  static constexpr bool PUSH = C > 1 && DO_X;
+  static constexpr size_t smem_push = (size_t)(LPR + 1) * CS * sizeof(float2) + smem_b;
+  static constexpr size_t smem_max_ab = smem_a > smem_b ? smem_a : smem_b;
+  static constexpr size_t smem = PUSH ? (smem_push > smem_max_ab ? smem_push : smem_max_ab) : smem_a;
   static_assert(kThreads % P == 0 || P > kThreads, "threads per line");
 };
 
@@ -196,6 +241,14 @@ __global__ void __launch_bounds__(kThreads, 3)
       if (src) prefetch_l2(src + (fcol + c) * N, N * sizeof(float2));
     }
   }
+  constexpr bool PUSH = G::PUSH;
+  // PUSH: [one round of column scratch, LPR + 1 columns][rows received from the cluster]
+  float2* const smB = sm + (PUSH ? (LPR + 1) * G::CS : 0);
+  __shared__ __align__(8) uint64_t recv_bar;
+  if constexpr (PUSH) {
+    if (tid == 0) mbar_init_expect(&recv_bar, (uint32_t)(G::LR * N * sizeof(float2)));
+    cg::this_cluster().sync();  // every block's barrier is armed before anyone pushes
+  }
   const float2 gzz = a.w.gz[z];
   // phase A: y transform of each held column, straight from global memory
   for (int c0 = 0; c0 < ncol; c0 += LPR) {
@@ -219,13 +272,27 @@ __global__ void __launch_bounds__(kThreads, 3)
 #pragma unroll
       for (int r = 0; r < 16; ++r) v[r] = make_float2(0.f, 0.f);
     }
-    ColLine L{sm + (live ? cl : M) * G::CS};
+    ColLine L{sm + (PUSH ? (live ? cl - c0 : LPR) : (live ? cl : M)) * G::CS};
     if constexpr (P <= 32) {
       line_fft<N, false>(v, L, p, a.py.tw, SyncWarp{});
     } else {
       line_fft<N, false>(v, L, p, a.py.tw, SyncBlock{});
     }
-    if constexpr (DO_X) {
+    if constexpr (PUSH) {
+      // X[ky] of column x goes to the block holding row ky: rank ky / LR,
+      // at x * CS2 + kyl (padded) of its received tile
+      if (live) {
+        const int x = x0 + cl;
+        const uint32_t lbar = smem_addr(&recv_bar);
+#pragma unroll
+        for (int m = 0; m < 16; ++m) {
+          const int ky = p + P * m;
+          const int dst = ky / G::LR, kyl = ky - dst * G::LR;
+          const uint32_t la = smem_addr(smB + x * G::CS2 + kyl + (kyl >> 4));
+          st_async_f2(map_rank(la, dst), v[m], map_rank(lbar, dst));
+        }
+      }
+    } else if constexpr (DO_X) {
 #pragma unroll
       for (int m = 0; m < 16; ++m) L.at(p + P * m) = v[m];
     } else if (live) {
@@ -235,39 +302,23 @@ __global__ void __launch_bounds__(kThreads, 3)
     }
   }
   if constexpr (DO_X) {
-    __syncthreads();
     // rows of the x transform: C == 1 -> column-major tile as is;
-    // C > 1 -> transpose through the cluster so this block holds rows
-    // [rank*LR, (rank+1)*LR) of all N columns, column-major with stride CS2.
+    // C > 1 -> the rows [rank*LR, (rank+1)*LR) of all N columns the cluster
+    // pushed into smB, column-major with stride CS2.
     int xs = G::CS;
-    if constexpr (C > 1) {
-      cg::cluster_group cl = cg::this_cluster();
-      constexpr int PER = G::LR * N / kThreads;  // elements per thread
-      float2 hold[PER];
-      cl.sync();
-#pragma unroll
-      for (int i = 0; i < PER; ++i) {
-        const int e = tid + kThreads * i;
-        const int kyl = e % G::LR, x = e / G::LR;
-        const float2* rs = cl.map_shared_rank(sm, x / G::M);
-        const int ky = rank * G::LR + kyl;
-        hold[i] = rs[(x % G::M) * G::CS + ky + (ky >> 4)];
+    if constexpr (PUSH) {
+      if (!mbar_wait_cluster(&recv_bar)) {
+        if (a.err) atomicExch(a.err, 1);
       }
-      cl.sync();
-#pragma unroll
-      for (int i = 0; i < PER; ++i) {
-        const int e = tid + kThreads * i;
-        const int kyl = e % G::LR, x = e / G::LR;
-        sm[x * G::CS2 + kyl + (kyl >> 4)] = hold[i];
-      }
-      __syncthreads();
       xs = G::CS2;
+    } else {
+      __syncthreads();
     }
     constexpr int ROWS = C > 1 ? G::LR : N;
     constexpr int RPR = kThreads / P;  // rows per round
     for (int r0 = 0; r0 < ROWS; r0 += RPR) {
       const int rl = r0 + tid % RPR, p = tid / RPR;
-      RowLine L{sm + rl + (rl >> 4), xs};
+      RowLine L{smB + rl + (rl >> 4), xs};
       float2 v[16];
 #pragma unroll
       for (int r = 0; r < 16; ++r) v[r] = L.at(p + P * r);

@@ -97,6 +97,7 @@ struct InnerArgs {
   long long fstride;  // elements between the fields of consecutive right-hand sides
   int pf;       // fast kernels: block b pulls the inputs of block b + pf into L2 (0: off)
   int acc2;     // K3: E' += dE' in pairs, every second iteration (Nw even; 0: every iteration)
+  int* err;     // fast kernels: set to 1 when a cluster exchange wait gives up (may be null)
 };
 
 struct OuterArgs {

@@ -272,6 +272,7 @@ struct Solver {
   double* d_partials = nullptr;  // per-block ROI energy of K3
   long long partials_cap = 0;    // elements of d_partials
   float2* d_init = nullptr;      // warm starts: v = gamma psi0 / Nw per right-hand side (batch_cap of them)
+  int* d_err = nullptr;          // set by a fast kernel whose cluster exchange wait gave up
   int pf_inner = 0, pf_outer = 0;  // L2 prefetch distance of the fast kernels, in blocks (0: off)
   bool warm = false;             // the current solve starts from d_init
   LayoutChoice tuned{};          // the autotuner's choice (all zero: the heuristics)
@@ -297,7 +298,8 @@ static void destroy_solver(Solver* s) {
   cudaSetDevice(s->device);
   free_graph(s);
   void* ptrs[] = {s->d_wigf, s->d_wigc,  s->d_gamma,  s->d_E,        s->d_dE, s->d_T,   s->d_src,
-                  s->d_stage, s->d_out, s->d_state, s->d_hist, s->d_energy, s->d_tw, s->d_partials, s->d_init};
+                  s->d_stage, s->d_out, s->d_state, s->d_hist, s->d_energy, s->d_tw, s->d_partials, s->d_init,
+                  s->d_err};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   for (auto& e : s->ev)
@@ -481,6 +483,8 @@ static int create_solver(const int64_t N[4], const ws_complex* gamma, int64_t n_
     }                                \
   } while (0)
   WS_TRY(cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking));
+  WS_TRY(cudaMalloc(&s->d_err, sizeof(int)));
+  WS_TRY(cudaMemset(s->d_err, 0, sizeof(int)));
   for (auto& e : s->ev) WS_TRY(cudaEventCreate(&e));
   // plans and twiddle tables
   std::vector<float2> tw;
@@ -582,6 +586,7 @@ static InnerArgs inner_args(const Solver* s, int w) {
   a.ncols = s->lay.ncols;
   a.bpr = (int)s->lay.grid_inner;
   a.fstride = (long long)field_elems(s);
+  a.err = s->d_err;
   a.pf = 0;  // K3 (and the generic kernels) measured slower with it
   // E' += dE' in pairs when every stop (a multiple of Nw) falls after an even iteration
   a.acc2 = (s->nw % 2 == 0) ? 1 : 0;
@@ -1020,7 +1025,13 @@ static int solve_batch(Solver* s, int nrhs, const int64_t* counts, const ws_sour
     }
   }
   WS_CUDA(cudaMemcpyAsync(hs.data(), s->d_state, nrhs * sizeof(DevState), cudaMemcpyDeviceToHost, s->stream));
+  int kerr = 0;
+  WS_CUDA(cudaMemcpyAsync(&kerr, s->d_err, sizeof(int), cudaMemcpyDeviceToHost, s->stream));
   WS_CUDA(cudaStreamSynchronize(s->stream));
+  if (kerr) {
+    cudaMemset(s->d_err, 0, sizeof(int));
+    return fail(WS_ERR_CUDA, "a cluster exchange of the FFT kernels timed out");
+  }
   bool diverged = false;
   for (int r = 0; r < nrhs; ++r) {
     const long long n_iter = hs[r].it - 1;
