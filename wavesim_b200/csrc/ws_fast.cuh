@@ -74,6 +74,11 @@ __device__ __forceinline__ void st_async_f2(uint32_t raddr, float2 v, uint32_t r
                "f"(v.x), "f"(v.y), "r"(rbar)
                : "memory");
 }
+__device__ __forceinline__ void st_async_f4(uint32_t raddr, float2 u, float2 v, uint32_t rbar) {
+  asm volatile("st.async.shared::cluster.mbarrier::complete_tx::bytes.v4.f32 [%0], {%1, %2, %3, %4}, [%5];" ::"r"(raddr),
+               "f"(u.x), "f"(u.y), "f"(v.x), "f"(v.y), "r"(rbar)
+               : "memory");
+}
 __device__ __forceinline__ void mbar_init_expect(uint64_t* bar, uint32_t bytes) {
   const uint32_t a = smem_addr(bar);
   asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(a));
@@ -176,7 +181,9 @@ struct PlaneGeom {
   static constexpr int M = DO_X ? N / C : 0;   // columns held in phase A (2-D: a.ncols at run time)
   static constexpr int CS = N + N / 16 + 1;    // padded column stride (odd: row access conflict free)
   static constexpr int LR = N / C;             // rows held in the x phase (C > 1)
-  static constexpr int CS2 = LR + LR / 16 + 1; // column stride of the transposed tile
+  // transposed tile: row kyl of column x at x * CS2 + kyl + 2 (kyl / 16); CS2
+  // even, so that element pairs (kyl even) are 16-byte aligned
+  static constexpr int CS2 = LR + 2 * (LR / 16) + 2;
   static constexpr int P = N / 16;
   static constexpr int LPR = kThreads / P;     // lines per round
   static constexpr size_t smem_a = (size_t)(M + 1) * CS * sizeof(float2);  // + scratch column
@@ -281,15 +288,27 @@ __global__ void __launch_bounds__(kThreads, 3)
     if constexpr (PUSH) {
       // X[ky] of column x goes to the block holding row ky: rank ky / LR,
       // at x * CS2 + kyl (padded) of its received tile
+      // in 16-byte pairs (ky, ky + 1): the even thread of a lane pair sends
+      // the pairs of m < 8, the odd one those of m >= 8 (P is even, so the
+      // partner lane p ^ 1 works on the same column)
+      float2 w[16];
+#pragma unroll
+      for (int m = 0; m < 16; ++m) {
+        w[m].x = __shfl_xor_sync(0xffffffffu, v[m].x, 1);
+        w[m].y = __shfl_xor_sync(0xffffffffu, v[m].y, 1);
+      }
       if (live) {
         const int x = x0 + cl;
         const uint32_t lbar = smem_addr(&recv_bar);
+        const bool odd = p & 1;
 #pragma unroll
-        for (int m = 0; m < 16; ++m) {
-          const int ky = p + P * m;
+        for (int h = 0; h < 8; ++h) {
+          const int m = odd ? 8 + h : h;
+          const int ky = (p & ~1) + P * m;  // even
           const int dst = ky / G::LR, kyl = ky - dst * G::LR;
-          const uint32_t la = smem_addr(smB + x * G::CS2 + kyl + (kyl >> 4));
-          st_async_f2(map_rank(la, dst), v[m], map_rank(lbar, dst));
+          const uint32_t la = smem_addr(smB + x * G::CS2 + kyl + 2 * (kyl >> 4));
+          const float2 lo = odd ? w[8 + h] : v[h], hi = odd ? v[8 + h] : w[h];  // constant indices
+          st_async_f4(map_rank(la, dst), lo, hi, map_rank(lbar, dst));
         }
       }
     } else if constexpr (DO_X) {
@@ -318,7 +337,7 @@ __global__ void __launch_bounds__(kThreads, 3)
     constexpr int RPR = kThreads / P;  // rows per round
     for (int r0 = 0; r0 < ROWS; r0 += RPR) {
       const int rl = r0 + tid % RPR, p = tid / RPR;
-      RowLine L{smB + rl + (rl >> 4), xs};
+      RowLine L{smB + rl + (PUSH ? 2 : 1) * (rl >> 4), xs};
       float2 v[16];
 #pragma unroll
       for (int r = 0; r < 16; ++r) v[r] = L.at(p + P * r);

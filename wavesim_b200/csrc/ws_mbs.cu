@@ -76,7 +76,8 @@ struct FastInner {
   int n, c, do_x;
   const void* fwd;
   const void* inv;
-  size_t smem;      // bytes (3-D); 2-D: bytes per held column, one extra column of scratch
+  size_t smem;      // bytes (3-D, enough for both kernels); 2-D: bytes per held column, one extra column of scratch
+  size_t smem_fwd, smem_inv;  // 3-D: what each kernel needs
 };
 struct FastPencil {
   int no, ty;
@@ -87,7 +88,8 @@ template <int N, int C, bool DX>
 static FastInner fast_inner() {
   using G = fast::PlaneGeom<N, C, DX>;
   return FastInner{N, C, DX ? 1 : 0, (const void*)fast::kf_plane_fwd<N, C, DX>,
-                   (const void*)fast::kf_plane_inv<N, C, DX>, DX ? G::smem : (size_t)G::CS * sizeof(float2)};
+                   (const void*)fast::kf_plane_inv<N, C, DX>, DX ? G::smem : (size_t)G::CS * sizeof(float2),
+                   DX ? (G::PUSH ? G::smem_push : G::smem_a) : 0, DX ? G::smem_max_ab : 0};
 }
 template <int NO, int TY>
 static FastPencil fast_pencil() {
@@ -653,16 +655,16 @@ static cudaError_t launch_k3_t(const Solver* s, int w) {
                             s->d_E, (const float2*)s->d_gamma, (const DevState*)s->d_state, s->d_partials);
 }
 
-static size_t fast_inner_smem(const Solver* s) {
+static size_t fast_inner_smem(const Solver* s, bool fwd) {
   const FastInner* f = s->lay.fi;
-  return f->do_x ? f->smem : f->smem * (size_t)(s->lay.ncols + 1);
+  return f->do_x ? (fwd ? f->smem_fwd : f->smem_inv) : f->smem * (size_t)(s->lay.ncols + 1);
 }
 
 static cudaError_t launch_fast_inner(const Solver* s, const void* fn, void** args) {
   cudaLaunchConfig_t cfg{};
   cfg.gridDim = dim3((unsigned)(s->lay.grid_inner * s->nrhs));
   cfg.blockDim = dim3(fast::kThreads);
-  cfg.dynamicSmemBytes = fast_inner_smem(s);
+  cfg.dynamicSmemBytes = fast_inner_smem(s, fn == s->lay.fi->fwd);
   cfg.stream = s->stream;
   cudaLaunchAttribute attr[1];
   attr[0].id = cudaLaunchAttributeClusterDimension;
