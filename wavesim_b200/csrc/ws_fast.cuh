@@ -190,7 +190,8 @@ struct PlaneGeom {
   static constexpr size_t smem_b = (size_t)N * CS2 * sizeof(float2);
   // K1 with a cluster: one round of column scratch + the received rows
   static constexpr bool PUSH = C > 1 && DO_X;
-  static constexpr size_t smem_push = (size_t)(LPR + 1) * CS * sizeof(float2) + smem_b;
+  // (+ 16 bytes: the received tile starts on a 16-byte boundary for the pair pushes)
+  static constexpr size_t smem_push = (size_t)(LPR + 1) * CS * sizeof(float2) + 16 + smem_b;
   static constexpr size_t smem_max_ab = smem_a > smem_b ? smem_a : smem_b;
   static constexpr size_t smem = PUSH ? (smem_push > smem_max_ab ? smem_push : smem_max_ab) : smem_a;
   static_assert(kThreads % P == 0 || P > kThreads, "threads per line");
@@ -250,7 +251,8 @@ __global__ void __launch_bounds__(kThreads, 3)
   }
   constexpr bool PUSH = G::PUSH;
   // PUSH: [one round of column scratch, LPR + 1 columns][rows received from the cluster]
-  float2* const smB = sm + (PUSH ? (LPR + 1) * G::CS : 0);
+  float2* const smB =
+      PUSH ? reinterpret_cast<float2*>((reinterpret_cast<uintptr_t>(sm + (LPR + 1) * G::CS) + 15) & ~(uintptr_t)15) : sm;
   __shared__ __align__(8) uint64_t recv_bar;
   if constexpr (PUSH) {
     if (tid == 0) mbar_init_expect(&recv_bar, (uint32_t)(G::LR * N * sizeof(float2)));
