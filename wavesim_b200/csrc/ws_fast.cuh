@@ -193,13 +193,7 @@ struct PlaneGeom {
   // (+ 16 bytes: the received tile starts on a 16-byte boundary for the pair pushes)
   static constexpr size_t smem_push = (size_t)(LPR + 1) * CS * sizeof(float2) + 16 + smem_b;
   static constexpr size_t smem_max_ab = smem_a > smem_b ? smem_a : smem_b;
-  // K3 with a cluster: one round of row scratch (stride XS3) + the received columns (M + 1, stride CS)
-  static constexpr int RPR = kThreads / P;
-  static constexpr int XS3 = RPR + RPR / 16 + 1;
-  static constexpr size_t smem_inv_push = (size_t)N * XS3 * sizeof(float2) + 16 + smem_a;
-  static constexpr size_t smem_fwd = PUSH ? smem_push : smem_a;
-  static constexpr size_t smem_inv = PUSH ? smem_inv_push : smem_a;
-  static constexpr size_t smem = smem_fwd > smem_inv ? smem_fwd : smem_inv;
+  static constexpr size_t smem = PUSH ? (smem_push > smem_max_ab ? smem_push : smem_max_ab) : smem_a;
   static_assert(kThreads % P == 0 || P > kThreads, "threads per line");
 };
 
@@ -476,18 +470,10 @@ __global__ void __launch_bounds__(kThreads, 2)
       if (tid == 0 && fn > 0) prefetch_l2(T + fcol * N, (unsigned)fn * N * sizeof(float2));
     }
   }
-  constexpr bool PUSH = G::PUSH;
-  // PUSH: [one round of row scratch, N x XS3][columns received from the cluster, M + 1 slots of CS]
-  float2* const smC =
-      PUSH ? reinterpret_cast<float2*>((reinterpret_cast<uintptr_t>(sm + N * G::XS3) + 15) & ~(uintptr_t)15) : sm;
-  __shared__ __align__(8) uint64_t recv_bar;
-  if constexpr (PUSH) {
-    if (tid == 0) mbar_init_expect(&recv_bar, (uint32_t)(G::M * N * sizeof(float2)));
-    cg::this_cluster().sync();  // every block's barrier is armed before anyone pushes
-  }
   if constexpr (DO_X) {
     constexpr int ROWS = C > 1 ? G::LR : N;
     constexpr int RPR = kThreads / P;
+    const int xs = C > 1 ? G::CS2 : G::CS;
     for (int r0 = 0; r0 < ROWS; r0 += RPR) {
       const int rl = r0 + tid % RPR, p = tid / RPR;
       const int ky = (C > 1 ? rank * G::LR : 0) + rl;
@@ -495,30 +481,32 @@ __global__ void __launch_bounds__(kThreads, 2)
       float2 v[16];
 #pragma unroll
       for (int r = 0; r < 16; ++r) v[r] = s[(long long)(p + P * r) * N];
-      const int rr = PUSH ? rl - r0 : rl;
-      RowLine L{sm + rr + (rr >> 4), PUSH ? G::XS3 : G::CS};
+      RowLine L{sm + rl + (rl >> 4), xs};
       line_fft<N, true>(v, L, p, a.twx, SyncBlock{});
-      if constexpr (PUSH) {
-        // x-transformed row ky: element kx goes to the block holding column
-        // kx (rank kx / M), at (kx % M) * CS + ky (padded) of its received tile
-        const uint32_t lbar = smem_addr(&recv_bar);
 #pragma unroll
-        for (int m = 0; m < 16; ++m) {
-          const int kx = p + P * m;
-          const int dst = kx / G::M, c = kx - dst * G::M;
-          const uint32_t la = smem_addr(smC + c * G::CS + ky + (ky >> 4));
-          st_async_f2(map_rank(la, dst), v[m], map_rank(lbar, dst));
-        }
-      } else {
-#pragma unroll
-        for (int m = 0; m < 16; ++m) L.at(p + P * m) = v[m];
-      }
+      for (int m = 0; m < 16; ++m) L.at(p + P * m) = v[m];
     }
-    if constexpr (PUSH) {
-      if (!mbar_wait_cluster(&recv_bar)) {
-        if (a.err) atomicExch(a.err, 1);
+    __syncthreads();
+    if constexpr (C > 1) {
+      cg::cluster_group cl = cg::this_cluster();
+      constexpr int PER = G::M * N / kThreads;
+      float2 hold[PER];
+      cl.sync();
+#pragma unroll
+      for (int i = 0; i < PER; ++i) {
+        const int e = tid + kThreads * i;
+        const int ky = e % N, c = e / N;
+        const float2* rs = cl.map_shared_rank(sm, ky / G::LR);
+        const int kyl = ky % G::LR;
+        hold[i] = rs[(x0 + c) * G::CS2 + kyl + (kyl >> 4)];
       }
-    } else {
+      cl.sync();
+#pragma unroll
+      for (int i = 0; i < PER; ++i) {
+        const int e = tid + kThreads * i;
+        const int ky = e % N, c = e / N;
+        sm[c * G::CS + ky + (ky >> 4)] = hold[i];
+      }
       __syncthreads();
     }
   }
@@ -528,7 +516,7 @@ __global__ void __launch_bounds__(kThreads, 2)
     const int cl = c0 + tid / P, p = tid % P;
     const bool live = cl < ncol;
     float2 v[16];
-    ColLine L{smC + (live ? cl : M) * G::CS};
+    ColLine L{sm + (live ? cl : M) * G::CS};
     if constexpr (DO_X) {
 #pragma unroll
       for (int r = 0; r < 16; ++r) v[r] = L.at(p + P * r);

@@ -89,7 +89,7 @@ static FastInner fast_inner() {
   using G = fast::PlaneGeom<N, C, DX>;
   return FastInner{N, C, DX ? 1 : 0, (const void*)fast::kf_plane_fwd<N, C, DX>,
                    (const void*)fast::kf_plane_inv<N, C, DX>, DX ? G::smem : (size_t)G::CS * sizeof(float2),
-                   DX ? G::smem_fwd : 0, DX ? G::smem_inv : 0};
+                   DX ? (G::PUSH ? G::smem_push : G::smem_a) : 0, DX ? G::smem_max_ab : 0};
 }
 template <int NO, int TY>
 static FastPencil fast_pencil() {
