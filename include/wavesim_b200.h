@@ -91,6 +91,19 @@ typedef struct ws_source_block {
 typedef void (*ws_callback_fn)(const char* callback_type, const double* diff_energy, int64_t n_iterations,
                                double energy_threshold, void* user_data);
 
+/* A plane-wave source block (no counterpart in the reference, whose sources
+ * are dense arrays): value(a) = amplitude * exp(i (phase0 + phase[0] a_y +
+ * phase[1] a_x + phase[2] a_z)) over the block at the 1-based grid corner
+ * `position` (after the shift and crop of Simulation.exec), a the 0-based
+ * offset within the block.  Generated on the device. */
+typedef struct ws_plane_wave {
+  int64_t position[4];
+  int64_t size[4];
+  ws_complex amplitude;
+  double phase[3];
+  double phase0;
+} ws_plane_wave;
+
 typedef struct ws_solve_options {
   int64_t max_iterations;        /* >= 1; the MEX call uses max_iterations or 100000 (WaveSimBase.m:127-131) */
   double energy_threshold;       /* Simulation.energy_threshold (Simulation.m:53) */
@@ -196,6 +209,14 @@ int ws_solver_solve(ws_solver s, int64_t n_blocks, const ws_source_block* source
 int ws_solver_solve_batch(ws_solver s, int64_t n_rhs, const int64_t* block_counts, const ws_source_block* blocks,
                           int source_memory, const ws_solve_options* opts, ws_complex* E_out, int out_memory,
                           double* diff_energy_out, int64_t diff_capacity, int64_t* n_iterations, int* converged);
+
+/* ws_solver_solve_batch with one plane-wave block per right-hand side
+ * (waves[n_rhs]), generated on the device instead of uploaded: angle sweeps
+ * on one medium (e.g. examples/pulse2d.m:31-40). */
+int ws_solver_solve_plane_waves(ws_solver s, int64_t n_rhs, const ws_plane_wave* waves,
+                                const ws_solve_options* opts, ws_complex* E_out, int out_memory,
+                                double* diff_energy_out, int64_t diff_capacity, int64_t* n_iterations,
+                                int* converged);
 
 /* Device pointer of the solver's current E' buffer and the CUDA stream it
  * works on (both valid until ws_solver_destroy). */

@@ -50,6 +50,11 @@ class ws_source_block(C.Structure):
 CALLBACK = C.CFUNCTYPE(None, C.c_char_p, C.POINTER(C.c_double), C.c_int64, C.c_double, C.c_void_p)
 
 
+class ws_plane_wave(C.Structure):
+    _fields_ = [("position", C.c_int64 * 4), ("size", C.c_int64 * 4), ("amplitude", ws_complex),
+                ("phase", C.c_double * 3), ("phase0", C.c_double)]
+
+
 class ws_solve_options(C.Structure):
     _fields_ = [("max_iterations", C.c_int64), ("energy_threshold", C.c_double),
                 ("energy_interval", C.c_int64), ("stop_rule", C.c_int), ("output", C.c_int),
@@ -63,7 +68,8 @@ class ws_solve_options(C.Structure):
 EXPORTS = [
     "ws_default_options", "ws_version", "ws_last_error", "ws_size_supported", "ws_run_algorithm",
     "ws_run_algorithm_release",
-    "ws_solver_create", "ws_solver_solve", "ws_solver_solve_batch", "ws_solver_buffers", "ws_solver_time_kernels",
+    "ws_solver_create", "ws_solver_solve", "ws_solver_solve_batch", "ws_solver_solve_plane_waves", "ws_solver_buffers",
+    "ws_solver_time_kernels",
     "ws_solver_launches_per_iteration", "ws_solver_warm_report", "ws_solver_autotune", "ws_solver_destroy",
     "ws_run_algorithm_noalloc", "ws_medium_reduce", "ws_build_gamma", "ws_setup_last_error",
     "ws_noalloc_scratch_bytes", "ws_noalloc_last_error",
@@ -105,6 +111,9 @@ def _load():
                                           C.POINTER(ws_solve_options), P, C.c_int, C.POINTER(C.c_double), C.c_int64,
                                           i64p, C.POINTER(C.c_int)]
     lib.ws_solver_solve_batch.restype = C.c_int
+    lib.ws_solver_solve_plane_waves.argtypes = [P, C.c_int64, C.POINTER(ws_plane_wave), C.POINTER(ws_solve_options), P,
+                                                C.c_int, C.POINTER(C.c_double), C.c_int64, i64p, C.POINTER(C.c_int)]
+    lib.ws_solver_solve_plane_waves.restype = C.c_int
     lib.ws_solver_buffers.argtypes = [P, C.POINTER(C.c_void_p), C.POINTER(C.c_void_p)]
     lib.ws_solver_buffers.restype = C.c_int
     lib.ws_solver_time_kernels.argtypes = [P, C.c_int, C.POINTER(C.c_float), C.POINTER(C.c_double)]

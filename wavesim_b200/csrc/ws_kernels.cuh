@@ -596,6 +596,35 @@ static __global__ void k_scatter_source(float2* __restrict__ dst, const float2* 
   if ((threadIdx.x & 31) == 0) atomicAdd(energy, (double)esum);
 }
 
+// A plane-wave source block generated on the device: value(a) = amp exp(i
+// (phase0 + sum_d phase[d] a_d)) over the block at 0-based corner p, size sz
+// (no counterpart in the reference, whose sources are dense arrays).
+struct PlaneWaveArgs {
+  int p[4], sz[4];
+  double amp_re, amp_im, phase0, phase[3];
+};
+static __global__ void k_plane_wave_source(float2* __restrict__ dst, Geom g, PlaneWaveArgs w, double* energy) {
+  const long long n = (long long)w.sz[0] * w.sz[1] * w.sz[2] * w.sz[3];
+  double esum = 0.0;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    long long r = i;
+    const int a0 = (int)(r % w.sz[0]); r /= w.sz[0];
+    const int a1 = (int)(r % w.sz[1]); r /= w.sz[1];
+    const int a2 = (int)(r % w.sz[2]); r /= w.sz[2];
+    const int a3 = (int)r;
+    const long long gi = (w.p[0] + a0) +
+                         (long long)g.ny * ((w.p[1] + a1) + (long long)g.nx * ((w.p[2] + a2) + (long long)g.nz * (w.p[3] + a3)));
+    double sp, cp;
+    sincos(w.phase0 + w.phase[0] * a0 + w.phase[1] * a1 + w.phase[2] * a2, &sp, &cp);
+    const float2 v = make_float2((float)(w.amp_re * cp - w.amp_im * sp), (float)(w.amp_re * sp + w.amp_im * cp));
+    dst[gi] = cadd(dst[gi], v);
+    esum += (double)v.x * v.x + (double)v.y * v.y;
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) esum += __shfl_xor_sync(0xffffffffu, esum, o);
+  if ((threadIdx.x & 31) == 0) atomicAdd(energy, esum);
+}
+
 // E = E' ./ gamma on the roi (WaveSimBase.m:193,196), column-major output.
 static __global__ void k_finalize(const float2* __restrict__ Ep, const float2* __restrict__ gamma, Geom g,
                            float2* __restrict__ out) {

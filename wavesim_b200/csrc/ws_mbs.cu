@@ -923,6 +923,39 @@ static int upload_sources(Solver* s, int nrhs, const int64_t* counts, const ws_s
   return WS_OK;
 }
 
+// One plane-wave block per right-hand side into the dense source fields.
+static int generate_plane_waves(Solver* s, int nrhs, const ws_plane_wave* waves, std::vector<double>& energy) {
+  const Geom& g = s->g;
+  const size_t F = field_elems(s);
+  WS_CUDA(cudaMemsetAsync(s->d_src, 0, F * nrhs * sizeof(float2), s->stream));
+  WS_CUDA(cudaMemsetAsync(s->d_energy, 0, nrhs * sizeof(double), s->stream));
+  for (int r = 0; r < nrhs; ++r) {
+    const ws_plane_wave& W = waves[r];
+    PlaneWaveArgs a{};
+    long long n = 1;
+    for (int d = 0; d < 4; ++d) {
+      const int64_t lim = d == 0 ? g.ny : d == 1 ? g.nx : d == 2 ? g.nz : g.nc;
+      if (W.size[d] < 1 || W.position[d] < 1 || W.position[d] + W.size[d] - 1 > lim)
+        return fail(WS_ERR_INVALID_ARGUMENT, "plane-wave block outside the grid (crop it first, Source.m:81-103)");
+      a.p[d] = (int)W.position[d] - 1;
+      a.sz[d] = (int)W.size[d];
+      n *= W.size[d];
+    }
+    a.amp_re = W.amplitude.re;
+    a.amp_im = W.amplitude.im;
+    a.phase0 = W.phase0;
+    for (int d = 0; d < 3; ++d) a.phase[d] = W.phase[d];
+    const long long blocks = std::min<long long>((n + 255) / 256, 4096);
+    k_plane_wave_source<<<(unsigned)std::max(1LL, blocks), 256, 0, s->stream>>>(s->d_src + F * r, g, a,
+                                                                                s->d_energy + r);
+    WS_CUDA(cudaGetLastError());
+  }
+  energy.assign(nrhs, 0.0);
+  WS_CUDA(cudaMemcpyAsync(energy.data(), s->d_energy, nrhs * sizeof(double), cudaMemcpyDeviceToHost, s->stream));
+  WS_CUDA(cudaStreamSynchronize(s->stream));
+  return WS_OK;
+}
+
 static size_t roi_elems(const Geom& g) {
   return (size_t)(g.r1[0] - g.r0[0]) * (g.r1[1] - g.r0[1]) * (g.r1[2] - g.r0[2]) * (g.r1[3] - g.r0[3]);
 }
@@ -932,7 +965,7 @@ static size_t roi_elems(const Geom& g) {
 // while the others continue.
 static int solve_batch(Solver* s, int nrhs, const int64_t* counts, const ws_source_block* src, int source_memory,
                        const ws_solve_options* o, ws_complex* E_out, int out_memory, double* diff_out,
-                       int64_t diff_cap, int64_t* n_it, int* converged) {
+                       int64_t diff_cap, int64_t* n_it, int* converged, const ws_plane_wave* waves = nullptr) {
   WS_CUDA(cudaSetDevice(s->device));
   ws_solve_options opt;
   ws_default_options(&opt);
@@ -941,9 +974,11 @@ static int solve_batch(Solver* s, int nrhs, const int64_t* counts, const ws_sour
   if (opt.max_iterations < 1 || opt.max_iterations > 100000000LL)
     return fail(WS_ERR_INVALID_ARGUMENT, "max_iterations must be in [1, 1e8]");
   if (opt.energy_interval < 1) return fail(WS_ERR_INVALID_ARGUMENT, "energy_interval must be >= 1");
-  if (!counts || !src) return fail(WS_ERR_NO_SOURCE, "no source blocks");
-  for (int r = 0; r < nrhs; ++r)
-    if (counts[r] < 1) return fail(WS_ERR_NO_SOURCE, "a right-hand side has no source blocks");
+  if (!waves) {
+    if (!counts || !src) return fail(WS_ERR_NO_SOURCE, "no source blocks");
+    for (int r = 0; r < nrhs; ++r)
+      if (counts[r] < 1) return fail(WS_ERR_NO_SOURCE, "a right-hand side has no source blocks");
+  }
   const bool want_cb = opt.callback && opt.callback_type && std::strcmp(opt.callback_type, "NoCallback") != 0;
   if (want_cb && nrhs > 1) return fail(WS_ERR_INVALID_ARGUMENT, "callbacks need a single right-hand side");
   if (s->lay.grid_inner * (long long)nrhs > (1LL << 31) - 1 || s->lay.grid_outer * (long long)nrhs > (1LL << 31) - 1)
@@ -955,7 +990,8 @@ static int solve_batch(Solver* s, int nrhs, const int64_t* counts, const ws_sour
   if (s->nrhs != nrhs) free_graph(s);
   s->nrhs = nrhs;
   std::vector<double> src_energy;
-  rc = upload_sources(s, nrhs, counts, src, source_memory, src_energy);
+  rc = waves ? generate_plane_waves(s, nrhs, waves, src_energy)
+             : upload_sources(s, nrhs, counts, src, source_memory, src_energy);
   if (rc) return rc;
   for (int r = 0; r < nrhs; ++r)
     if (!(src_energy[r] > 0)) return fail(WS_ERR_NO_SOURCE, "There is no source inside the grid boundaries");
@@ -1157,6 +1193,15 @@ int ws_solver_solve_batch(ws_solver h, int64_t n_rhs, const int64_t* block_count
   if (!h) return fail(WS_ERR_INVALID_ARGUMENT, "null solver");
   return solve_batch(reinterpret_cast<Solver*>(h), (int)n_rhs, block_counts, blocks, source_memory, opts, E_out,
                      out_memory, diff_energy_out, diff_capacity, n_iterations, converged);
+}
+
+int ws_solver_solve_plane_waves(ws_solver h, int64_t n_rhs, const ws_plane_wave* waves, const ws_solve_options* opts,
+                                ws_complex* E_out, int out_memory, double* diff_energy_out, int64_t diff_capacity,
+                                int64_t* n_iterations, int* converged) {
+  if (!h) return fail(WS_ERR_INVALID_ARGUMENT, "null solver");
+  if (!waves) return fail(WS_ERR_NO_SOURCE, "no plane waves");
+  return solve_batch(reinterpret_cast<Solver*>(h), (int)n_rhs, nullptr, nullptr, WS_HOST, opts, E_out, out_memory,
+                     diff_energy_out, diff_capacity, n_iterations, converged, waves);
 }
 
 int ws_solver_buffers(ws_solver h, void** E_prime, void** stream) {

@@ -192,3 +192,40 @@ class Source:
             s.positions.append(a)
             s.values.append(v[sl])
         return s
+
+
+class PlaneWave:
+    """A plane-wave source block given by a few numbers instead of values (no
+    counterpart in the reference, whose Source holds dense arrays): value at
+    offset a from the block corner = amplitude exp(i (phase0 + phase . a)),
+    phase = phase advance per pixel along (y, x, z).  size and position as
+    the shape and position of Source (1-based, ROI coordinates, 4 entries
+    with the polarisation last).  Generated on the device
+    (ws_solver_solve_plane_waves)."""
+
+    def __init__(self, size, position=(1, 1, 1, 1), amplitude=1.0, phase=(0.0, 0.0, 0.0)):
+        self.size = _pad4(np.maximum(np.asarray(size, dtype=np.int64), 1))
+        self.position = _pad4(position)
+        self.amplitude = complex(amplitude)
+        self.phase = np.asarray(list(phase) + [0.0] * (3 - len(phase)), dtype=float)[:3]
+        self.phase0 = 0.0
+
+    def values(self):
+        """The dense block (for checks and for the host path)."""
+        a = [np.arange(int(n)) for n in self.size]
+        ph = (self.phase0 + self.phase[0] * a[0][:, None, None, None] + self.phase[1] * a[1][None, :, None, None]
+              + self.phase[2] * a[2][None, None, :, None]) + 0 * a[3][None, None, None, :]
+        return self.amplitude * np.exp(1j * ph)
+
+    def placed(self, roi0, N):
+        """The block shifted to grid coordinates (by the ROI origin roi0, 1-based)
+        and cropped to the grid [1, N]; the phase follows the crop.  None if
+        nothing is left."""
+        pos = self.position + _pad4(roi0) - 1
+        lo = np.maximum(pos, 1)
+        hi = np.minimum(pos + self.size - 1, _pad4(N))
+        if (lo > hi).any():
+            return None
+        w = PlaneWave(hi - lo + 1, lo, self.amplitude, self.phase)
+        w.phase0 = self.phase0 + float(np.dot(self.phase, (lo - pos)[:3]))
+        return w

@@ -27,7 +27,7 @@ from types import SimpleNamespace
 import numpy as np
 
 from . import _lib
-from .problem import Medium, Source, _pad4
+from .problem import Medium, PlaneWave, Source, _pad4
 
 ALPHA = 0.7  # private/f_mix.m:3
 
@@ -437,6 +437,8 @@ class WaveSim:
         the ROI or the full grid), see exec; a discarded start is rerun cold
         on its own.  Returns (list of E, list of state)."""
         t0 = time.perf_counter()
+        if sources and all(isinstance(s, PlaneWave) for s in sources):
+            return self._exec_plane_waves(sources, warm_starts, t0)
         groups, keep, counts = [], [], []
         for src in sources:
             s, blocks, k = self.source_blocks(src)
@@ -498,6 +500,45 @@ class WaveSim:
                     st.warm_cycle_energy = states[i].warm_cycle_energy
                     st.time += dt
                     states[i] = st
+        return outs, states
+
+
+    def _exec_plane_waves(self, waves, warm_starts, t0):
+        """exec_batch for PlaneWave sources: the blocks are generated on the
+        device (ws_solver_solve_plane_waves)."""
+        if warm_starts is not None:
+            raise ValueError("warm starts with plane-wave descriptors: use Source blocks")
+        R = len(waves)
+        arr = (_lib.ws_plane_wave * R)()
+        for i, w in enumerate(waves):
+            pw = w.placed(self.roi[0], self.N)
+            if pw is None:
+                raise ValueError("a source has no part inside the grid boundaries")
+            arr[i] = _lib.ws_plane_wave((C.c_int64 * 4)(*[int(a) for a in pw.position]),
+                                        (C.c_int64 * 4)(*[int(a) for a in pw.size]),
+                                        _lib.ws_complex(pw.amplitude.real, pw.amplitude.imag),
+                                        (C.c_double * 3)(*[float(a) for a in pw.phase]), pw.phase0)
+        h = self.solver()
+        o = self._options()
+        r = self.roi
+        shape = tuple(int(r[1, d] - r[0, d] + 1) for d in range(4))
+        E = np.empty((R,) + shape[::-1], dtype=np.complex64)
+        cap = o.max_iterations + len(self.wiggles) + 1
+        hist = np.zeros((R, cap))
+        n_it = np.zeros(R, dtype=np.int64)
+        conv = np.zeros(R, dtype=np.int32)
+        _lib.check(_lib.lib.ws_solver_solve_plane_waves(
+            h, R, arr, C.byref(o), E.ctypes.data, _lib.WS_HOST, hist.ctypes.data_as(C.POINTER(C.c_double)), cap,
+            n_it.ctypes.data_as(C.POINTER(C.c_int64)), conv.ctypes.data_as(C.POINTER(C.c_int))))
+        dt = time.perf_counter() - t0
+        outs, states = [], []
+        for i in range(R):
+            Ei = np.ascontiguousarray(E[i].transpose(3, 2, 1, 0))
+            if not self.vector:
+                Ei = Ei[..., 0]
+            outs.append(Ei)
+            states.append(SimpleNamespace(source=waves[i], it=int(n_it[i]) + 1, converged=bool(conv[i]),
+                                          diff_energy=hist[i, :n_it[i]].copy(), time=dt))
         return outs, states
 
 
