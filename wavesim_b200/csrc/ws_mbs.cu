@@ -20,6 +20,7 @@
 #include "wavesim_b200.h"
 #include "ws_fast.cuh"
 #include "ws_kernels.cuh"
+#include "ws_tma.cuh"
 
 namespace ws {
 
@@ -103,6 +104,25 @@ static const std::vector<FastInner>& fast_inner_table() {
       fast_inner<512, 1, false>(),   fast_inner<1024, 1, false>(),  fast_inner<2048, 1, false>()};
   return t;
 }
+// Persistent TMA-pipelined K2 (ws_tma.cuh) for z pencils of a 3-D grid.
+struct TmaPencil {
+  int no, ty, stages;
+  const void* fn;
+  size_t smem;
+  int threads;
+};
+template <int NO, int TY, int S>
+static TmaPencil tma_pencil() {
+  using PT = tma::PencilTile<NO, TY, S>;
+  return TmaPencil{NO, TY, S, (const void*)tma::kt_pencil<NO, TY, S>, PT::smem, PT::kThreads};
+}
+static const std::vector<TmaPencil>& tma_pencil_table() {
+  // the first match of (no, ty) is the default; the autotuner tries the rest
+  static const std::vector<TmaPencil> t = {tma_pencil<64, 16, 3>(), tma_pencil<128, 16, 3>(),
+                                           tma_pencil<256, 16, 3>(), tma_pencil<256, 16, 2>()};
+  return t;
+}
+
 static const std::vector<FastPencil>& fast_pencil_table() {
   static const std::vector<FastPencil> t = {fast_pencil<32, 16>(),  fast_pencil<64, 16>(),  fast_pencil<128, 16>(),
                                             fast_pencil<256, 16>(), fast_pencil<512, 8>(),  fast_pencil<1024, 4>()};
@@ -112,6 +132,7 @@ static const std::vector<FastPencil>& fast_pencil_table() {
 struct Layout {
   const FastInner* fi = nullptr;   // fast K1/K3, or null (generic)
   const FastPencil* fp = nullptr;  // fast K2, or null (generic)
+  const TmaPencil* tp = nullptr;   // persistent TMA K2 (takes precedence over fp), or null
   int rset = kPow2;  // radix set of every plan of the solver
   int mode3d = 0;
   int csize = 1;     // 3-D: blocks (cluster) per plane
@@ -127,7 +148,7 @@ static bool is_pow2(long long n) { return n >= 1 && (n & (n - 1)) == 0; }
 // Overrides of the layout heuristics, for the autotuner (0 = heuristic).
 struct LayoutChoice {
   int inner = 0;  // 1: fast inner kernels when a shape matches, 2: generic
-  int outer = 0;  // 1: fast pencil when a shape matches, 2: generic
+  int outer = 0;  // 1: fast pencil when a shape matches, 2: generic, 3 + k: TMA pencil of k stages
   int csize = 0;  // 3-D generic: smallest blocks per plane to try
   int ncols = 0;  // 2-D generic: columns per block
   int ty = 0;     // generic outer: consecutive y per block
@@ -229,6 +250,17 @@ static int make_layout(const Geom& g, Layout& L, std::string& why, const LayoutC
       if (f.no == no && g.ny % f.ty == 0) L.fp = &f;
   }
   if (L.fp) L.grid_outer = (long long)(g.ny / L.fp->ty) * mids;  // blocks of the fast pencil kernel
+  // the TMA pencil where a shape matches: by default (WAVESIM_B200_K2=plain keeps kf_pencil), or the
+  // autotuner's choice of stages
+  const char* k2 = std::getenv("WAVESIM_B200_K2");
+  const bool tma_ok = L.mode3d && g.nc == 1 && (ch.outer == 0 || ch.outer >= 3) &&
+                      !(ch.outer == 0 && k2 && std::strcmp(k2, "plain") == 0);
+  if (tma_ok)
+    for (const TmaPencil& f : tma_pencil_table())
+      if (f.no == no && g.ny % f.ty == 0 && (ch.outer < 3 || f.stages == ch.outer - 3)) {
+        L.tp = &f;
+        break;
+      }
   return WS_OK;
 }
 
@@ -274,7 +306,12 @@ struct Solver {
   double* d_partials = nullptr;  // per-block ROI energy of K3
   long long partials_cap = 0;    // elements of d_partials
   float2* d_init = nullptr;      // warm starts: v = gamma psi0 / Nw per right-hand side (batch_cap of them)
-  int* d_err = nullptr;          // set by a fast kernel whose cluster exchange wait gave up
+  int* d_err = nullptr;          // set by a fast kernel whose cluster exchange or TMA wait gave up
+  CUtensorMap tmap_T{};          // T as {2 Ny floats, Nx, Nz * tmap_nrhs}, for the TMA pencil
+  const void* tmap_base = nullptr;
+  int tmap_nrhs = 0;
+  const void* tmap_kernel = nullptr;  // the TMA pencil the map and tma_blocks were made for
+  int tma_blocks = 0;            // resident blocks of the TMA pencil (its persistent grid)
   int pf_inner = 0, pf_outer = 0;  // L2 prefetch distance of the fast kernels, in blocks (0: off)
   bool warm = false;             // the current solve starts from d_init
   LayoutChoice tuned{};          // the autotuner's choice (all zero: the heuristics)
@@ -364,6 +401,7 @@ static int set_kernel_attributes() {
     WS_CUDA(cudaFuncSetAttribute(f.inv, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
   }
   for (const FastPencil& f : fast_pencil_table()) WS_CUDA(allow_dynamic_smem(f.fn, optin));
+  for (const TmaPencil& f : tma_pencil_table()) WS_CUDA(allow_dynamic_smem(f.fn, optin));
   if (dev < 31) done_mask |= 1 << dev;
   return WS_OK;
 }
@@ -691,7 +729,70 @@ static cudaError_t launch_k1(const Solver* s, int w, bool with_source) {
   }
   return s->lay.rset == kPow2 ? launch_k1_t<kPow2>(s, w, with_source) : launch_k1_t<kMixed>(s, w, with_source);
 }
+// cuTensorMapEncodeTiled through the runtime's driver entry point (no link
+// against libcuda)
+typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                  const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                  CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+static EncodeTiledFn encode_tiled() {
+  static EncodeTiledFn fn = [] {
+    void* f = nullptr;
+    cudaDriverEntryPointQueryResult q{};
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &f, cudaEnableDefault, &q) != cudaSuccess ||
+        q != cudaDriverEntryPointSuccess)
+      f = nullptr;
+    return reinterpret_cast<EncodeTiledFn>(f);
+  }();
+  return fn;
+}
+
+// T of the current batch as a 3-D float tensor {2 Ny, Nx, Nz nrhs}, box
+// {2 TY, 1, Nz}: every x coordinate the kernel issues is 2 TY yt floats, a
+// multiple of 32 floats, so each copy starts on a 128-byte boundary.
+static cudaError_t ensure_tmap(Solver* s) {
+  const TmaPencil* f = s->lay.tp;
+  if (s->tmap_base == s->d_T && s->tmap_nrhs == s->nrhs && s->tmap_kernel == f->fn) return cudaSuccess;
+  s->tmap_kernel = nullptr;
+  s->tma_blocks = 0;
+  EncodeTiledFn enc = encode_tiled();
+  if (!enc) return cudaErrorNotSupported;
+  const Geom& g = s->g;
+  const cuuint64_t dims[3] = {(cuuint64_t)2 * g.ny, (cuuint64_t)g.nx, (cuuint64_t)g.nz * s->nrhs};
+  const cuuint64_t strides[2] = {(cuuint64_t)g.ny * sizeof(float2), (cuuint64_t)g.ny * g.nx * sizeof(float2)};
+  const cuuint32_t box[3] = {(cuuint32_t)(2 * f->ty), 1u, (cuuint32_t)f->no};
+  const cuuint32_t estr[3] = {1u, 1u, 1u};
+  if (enc(&s->tmap_T, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, s->d_T, dims, strides, box, estr,
+          CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+          CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+    return cudaErrorInvalidValue;
+  s->tmap_base = s->d_T;
+  s->tmap_nrhs = s->nrhs;
+  s->tmap_kernel = f->fn;
+  return cudaSuccess;
+}
+
+static cudaError_t launch_k2_tma(const Solver* cs, int w) {
+  Solver* s = const_cast<Solver*>(cs);  // the tensor-map cache only
+  const TmaPencil* f = s->lay.tp;
+  cudaError_t e = ensure_tmap(s);
+  if (e != cudaSuccess) return e;
+  if (s->tma_blocks <= 0) {
+    int per_sm = 0;
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, f->fn, f->threads, f->smem);
+    if (e != cudaSuccess) return e;
+    s->tma_blocks = std::max(1, per_sm) * kNumSms;
+  }
+  OuterArgs a = outer_args(s, w);
+  int ntiles = s->nrhs * s->g.nx * (s->g.ny / f->ty);
+  const unsigned grid = (unsigned)std::min(ntiles, s->tma_blocks);
+  const DevState* st = s->d_state;
+  int* err = s->d_err;
+  void* args[] = {&s->tmap_T, &a, &st, &ntiles, &err};
+  return cudaLaunchKernel(f->fn, dim3(grid), dim3(f->threads), args, f->smem, s->stream);
+}
+
 static cudaError_t launch_k2(const Solver* s, int w) {
+  if (s->lay.tp) return launch_k2_tma(s, w);
   if (s->lay.fp) {
     OuterArgs a = outer_args(s, w);
     const FastPencil* f = s->lay.fp;
@@ -1390,6 +1491,7 @@ int ws_solver_autotune(ws_solver h, int n_iterations, int* n_tried, float* ms_be
     for (int f : {4, 2, -2})
       inner_c.push_back(LayoutChoice{2, 0, 0, f > 0 ? std::max(1, base.ncols / f) : base.ncols * 2, 0});
   outer_c.push_back(LayoutChoice{0, 1, 0, 0, 0});
+  for (int k : {2, 3}) outer_c.push_back(LayoutChoice{0, 3 + k, 0, 0, 0});
   for (int t : {1, 2, 4, 8, 16}) outer_c.push_back(LayoutChoice{0, 2, 0, 0, t});
   int tried = 0;
   LayoutChoice best_in{}, best_out{};

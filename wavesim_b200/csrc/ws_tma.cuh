@@ -1,0 +1,186 @@
+// K2 as a persistent, TMA-pipelined kernel (sm_100a): the outer-dimension
+// (z) pencils of a 3-D grid, TY consecutive y per tile.  Each block walks
+// its tiles t = blockIdx.x, blockIdx.x + gridDim.x, ...; while it
+// transforms one tile (FFT along z, Green's function, inverse FFT; registers
+// plus an in-place exchange in the tile's own buffer), the tensor-memory
+// access unit holds the loads of the next S - 2 tiles (S - 1 in the second
+// half) and the store of the previous one, so that HBM never waits for the
+// arithmetic.
+//   load:  cp.async.bulk.tensor.3d, box {2 TY floats, 1, NO} of the map
+//          {2 Ny floats, Nx, Nz * nrhs} over T, completing on the buffer's
+//          mbarrier with the byte count
+//   store: cp.async.bulk.tensor.3d from the same buffer, bulk group; a buffer
+//          is reloaded only after the store that reads it has read it
+//          (cp.async.bulk.wait_group.read)
+// The tensor map spans this GPU's own T only (no multicast).  Every wait is
+// bounded: a block whose load does not arrive in ~5e7 clocks sets *err,
+// drains its copies (bounded again) and returns.
+#pragma once
+#include <cuda.h>
+
+#include "ws_fast.cuh"
+
+namespace ws {
+namespace tma {
+
+__device__ __forceinline__ void load_3d(uint32_t dst, const CUtensorMap* map, int c0, int c1, int c2, uint32_t bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], [%5];" ::"r"(
+          dst),
+      "l"(map), "r"(c0), "r"(c1), "r"(c2), "r"(bar)
+      : "memory");
+}
+__device__ __forceinline__ void store_3d(const CUtensorMap* map, int c0, int c1, int c2, uint32_t src) {
+  asm volatile("cp.async.bulk.tensor.3d.global.shared::cta.bulk_group [%0, {%1, %2, %3}], [%4];" ::"l"(map), "r"(c0),
+               "r"(c1), "r"(c2), "r"(src)
+               : "memory");
+}
+__device__ __forceinline__ void bulk_commit() { asm volatile("cp.async.bulk.commit_group;" ::: "memory"); }
+// every committed store group has read its shared memory
+__device__ __forceinline__ void bulk_wait_read_0() { asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory"); }
+__device__ __forceinline__ void bulk_wait_all() { asm volatile("cp.async.bulk.wait_group 0;" ::: "memory"); }
+__device__ __forceinline__ void expect_bytes(uint64_t* bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(fast::smem_addr(bar)), "r"(bytes)
+               : "memory");
+}
+// phase with parity `parity` of the barrier complete; false after ~5e7 clocks
+__device__ __forceinline__ bool wait_parity(uint64_t* bar, uint32_t parity) {
+  const uint32_t a = fast::smem_addr(bar);
+  const long long t0 = clock64();
+  while (true) {
+    uint32_t done;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(done)
+        : "r"(a), "r"(parity)
+        : "memory");
+    if (done) return true;
+    if (clock64() - t0 > 50000000LL) return false;
+  }
+}
+
+template <int NO, int TY, int S>
+struct PencilTile {
+  static_assert(NO >= 32 && NO <= 256, "a TMA box dimension holds at most 256 elements");
+  static_assert(2 * TY * 4 % 16 == 0 && 2 * TY <= 256, "inner box extent");
+  static constexpr int P = NO / 16;
+  static constexpr int kThreads = TY * P;
+  static constexpr unsigned kTileBytes = NO * TY * sizeof(float2);
+  // S tile buffers, [z][y] as the TMA box lands (128-byte aligned)
+  static constexpr size_t smem = S * (size_t)kTileBytes + 128;
+};
+
+template <int NO, int TY, int S>
+__global__ void __launch_bounds__(PencilTile<NO, TY, S>::kThreads, 2)
+    kt_pencil(const __grid_constant__ CUtensorMap tmap, OuterArgs a, const DevState* __restrict__ st, int ntiles,
+              int* __restrict__ err) {
+  using PT = PencilTile<NO, TY, S>;
+  constexpr int P = PT::P;
+  extern __shared__ uint8_t smem_raw[];
+  float2* const buf0 = reinterpret_cast<float2*>((reinterpret_cast<uintptr_t>(smem_raw) + 127) & ~(uintptr_t)127);
+  __shared__ __align__(8) uint64_t full[S];
+  const Geom& g = a.g;
+  const int tid = threadIdx.x;
+  const int yl = tid % TY, p = tid / TY;
+  const int nyt = g.ny / TY;
+  const int per_rhs = nyt * g.nx;
+  if (tid == 0) {
+#pragma unroll
+    for (int b = 0; b < S; ++b) asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(fast::smem_addr(&full[b])));
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  __syncthreads();
+  // tile t -> (rhs, x = mid, y tile)
+  auto coords = [&](int t, int& rhs, int& mid, int& yt) {
+    rhs = t / per_rhs;
+    const int r = t - rhs * per_rhs;
+    mid = r / nyt;
+    yt = r - mid * nyt;
+  };
+  auto issue = [&](int t, int b) {
+    int rhs, mid, yt;
+    coords(t, rhs, mid, yt);
+    expect_bytes(&full[b], PT::kTileBytes);
+    load_3d(fast::smem_addr(buf0 + b * NO * TY), &tmap, 2 * TY * yt, mid, rhs * g.nz, fast::smem_addr(&full[b]));
+  };
+  const int G = gridDim.x;
+  const int mine = blockIdx.x < ntiles ? (ntiles - 1 - blockIdx.x) / G + 1 : 0;  // tiles of this block
+  if (tid == 0)
+    for (int i = 0; i < S - 1 && i < mine; ++i) issue(blockIdx.x + i * G, i);
+  // this thread's part of the Green's function: pz^2 - Re(k0^2 + i eps) for its 16 z
+  float pz2[16];
+#pragma unroll
+  for (int m = 0; m < 16; ++m) {
+    const float po = a.w.pze[p + P * m];
+    pz2[m] = fmaf(po, po, -a.k02e.x);
+  }
+  const float di = -a.k02e.y;
+  int i = 0;
+  bool ok = true;
+  for (; i < mine; ++i) {
+    const int b = i % S;
+    const int t = blockIdx.x + i * G;
+    float2* const buf = buf0 + b * NO * TY;
+    ok = wait_parity(&full[b], (uint32_t)((i / S) & 1));
+    if (__syncthreads_or(!ok)) {
+      ok = false;
+      break;
+    }
+    // tile i + S - 1 goes into the buffer of tile i - 1 (no thread reads it
+    // any more), once the store of tile i - 1 has read it: issued half way
+    // through tile i, so that the load overlaps the inverse transform too
+    auto refill = [&]() {
+      const int nxt = i + S - 1;
+      if (tid == 0 && nxt < mine) {
+        bulk_wait_read_0();
+        issue(blockIdx.x + nxt * G, nxt % S);
+      }
+    };
+    int rhs, mid, yt;
+    coords(t, rhs, mid, yt);
+    const bool live = !load_done(st + rhs);
+    if (!live) refill();
+    if (live) {
+      float2 v[16];
+#pragma unroll
+      for (int q = 0; q < 16; ++q) v[q] = buf[(p + P * q) * TY + yl];
+      // the exchanges go through the tile's own buffer (each starts with a
+      // block barrier, so every input has been read before it is overwritten)
+      fast::RowLine L{buf + yl, TY};
+      fast::line_fft<NO, false>(v, L, p, a.po.tw, fast::SyncBlock{});
+      // f_g0_scalar with the 1/N of ifftn: E ./ (px^2 + py^2 + (pz^2 - k02e))
+      const float py = a.w.pye[yt * TY + yl];
+      const float pxm = a.w.pxe[mid];
+      const float base2 = fmaf(pxm, pxm, py * py);
+#pragma unroll
+      for (int m = 0; m < 16; ++m) {
+        const float dr = base2 + pz2[m];
+        const float inv = __fdividef(a.norm, fmaf(dr, dr, di * di));
+        v[m] = cmul(v[m], make_float2(dr * inv, -di * inv));
+      }
+      refill();
+      fast::line_fft<NO, true>(v, L, p, a.po.tw, fast::SyncBlock{});
+      // thread (p, yl) wrote back exactly the elements it read last
+#pragma unroll
+      for (int m = 0; m < 16; ++m) buf[(p + P * m) * TY + yl] = v[m];
+      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");  // visible to the TMA store
+    }
+    __syncthreads();
+    if (tid == 0 && live) {
+      store_3d(&tmap, 2 * TY * yt, mid, rhs * g.nz, fast::smem_addr(buf));
+      bulk_commit();
+    }
+  }
+  if (!ok) {
+    if (tid == 0) atomicExch(err, 1);
+    // drain the loads still in flight: tiles i .. min(i + S - 2, mine - 1); a
+    // load that never arrives is abandoned after the same bound
+    for (int j = i; j < mine && j < i + S - 1; ++j) (void)wait_parity(&full[j % S], (uint32_t)((j / S) & 1));
+  }
+  if (tid == 0) bulk_wait_all();
+}
+
+}  // namespace tma
+}  // namespace ws
