@@ -45,6 +45,12 @@ CASES = {
     "3d_128_cluster2": ((96, 96, 96), [16, 16, 16], 16, False),
     "3d_256_cluster8": ((224, 224, 16), [16, 16, 8], 16, False),
     "3d_64_vector": ((32, 32, 32), [16, 16, 16], 16, True),
+    # mixed-radix kernels (192 = 12 x 4 x 4): planes on a cluster of 6, z pencils
+    "3d_192_cluster6": ((160, 160, 8), [16, 16, 4], 16, False),
+    "3d_192_cluster6_vector": ((160, 160, 4), [16, 16, 2], 16, True),
+    "3d_pencil_192": ((16, 16, 160), [8, 8, 16], 16, False),
+    "3d_pencil_192_vector": ((16, 16, 160), [8, 8, 16], 16, True),
+    "3d_128_vector": ((96, 96, 96), [16, 16, 16], 8, True),
 }
 
 

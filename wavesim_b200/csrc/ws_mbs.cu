@@ -20,6 +20,7 @@
 #include "wavesim_b200.h"
 #include "ws_fast.cuh"
 #include "ws_kernels.cuh"
+#include "ws_mixed.cuh"
 #include "ws_tma.cuh"
 
 namespace ws {
@@ -83,6 +84,10 @@ struct FastInner {
 struct FastPencil {
   int no, ty;
   const void* fn;
+  int nc;        // components it transforms together (1, or 3 with the dyadic Green's function)
+  int threads;
+  size_t smem;
+  int only3d;    // z pencils of a 3-D grid only
 };
 
 template <int N, int C, bool DX>
@@ -94,14 +99,29 @@ static FastInner fast_inner() {
 }
 template <int NO, int TY>
 static FastPencil fast_pencil() {
-  return FastPencil{NO, TY, (const void*)fast::kf_pencil<NO, TY>};
+  return FastPencil{NO, TY, (const void*)fast::kf_pencil<NO, TY>, 1, TY * (NO / 16),
+                    (size_t)(TY + 1) * NO * sizeof(float2), 0};
+}
+// mixed-radix / vector kernels (ws_mixed.cuh)
+using Plan192 = mixed::Plan<192, 12, 12, 4, 4>;
+template <class PL, int C>
+static FastInner mixed_inner() {
+  using G = mixed::MGeom<PL, C>;
+  return FastInner{PL::N, C, 1, (const void*)mixed::km_plane_fwd<PL, C>, (const void*)mixed::km_plane_inv<PL, C>,
+                   G::smem, G::smem, G::smem};
+}
+template <class PL, int TY, int NC>
+static FastPencil mixed_pencil() {
+  return FastPencil{PL::N, TY, (const void*)mixed::km_pencil<PL, TY, NC>, NC, TY * PL::P,
+                    (size_t)(TY + 1) * PL::N * sizeof(float2), 1};
 }
 
 static const std::vector<FastInner>& fast_inner_table() {
   static const std::vector<FastInner> t = {
       fast_inner<64, 1, true>(),     fast_inner<128, 2, true>(),    fast_inner<256, 8, true>(),
       fast_inner<64, 1, false>(),    fast_inner<128, 1, false>(),   fast_inner<256, 1, false>(),
-      fast_inner<512, 1, false>(),   fast_inner<1024, 1, false>(),  fast_inner<2048, 1, false>()};
+      fast_inner<512, 1, false>(),   fast_inner<1024, 1, false>(),  fast_inner<2048, 1, false>(),
+      mixed_inner<Plan192, 6>()};
   return t;
 }
 // Persistent TMA-pipelined K2 (ws_tma.cuh) for z pencils of a 3-D grid.
@@ -124,8 +144,14 @@ static const std::vector<TmaPencil>& tma_pencil_table() {
 }
 
 static const std::vector<FastPencil>& fast_pencil_table() {
-  static const std::vector<FastPencil> t = {fast_pencil<32, 16>(),  fast_pencil<64, 16>(),  fast_pencil<128, 16>(),
-                                            fast_pencil<256, 16>(), fast_pencil<512, 8>(),  fast_pencil<1024, 4>()};
+  static const std::vector<FastPencil> t = {
+      fast_pencil<32, 16>(),  fast_pencil<64, 16>(),  fast_pencil<128, 16>(),
+      fast_pencil<256, 16>(), fast_pencil<512, 8>(),  fast_pencil<1024, 4>(),
+      mixed_pencil<Plan192, 16, 1>(),
+      mixed_pencil<Plan192, 16, 3>(),
+      mixed_pencil<mixed::Plan<64, 16, 16, 4>, 16, 3>(),
+      mixed_pencil<mixed::Plan<128, 16, 16, 8>, 16, 3>(),
+      mixed_pencil<mixed::Plan<256, 16, 16, 16>, 16, 3>()};
   return t;
 }
 
@@ -245,9 +271,9 @@ static int make_layout(const Geom& g, Layout& L, std::string& why, const LayoutC
     L.grid_inner = (total_cols + want - 1) / want;
   }
   if (L.fi && L.mode3d) L.grid_inner = (long long)g.nz * g.nc * L.fi->c;
-  if (g.nc == 1 && ch.outer != 2) {
+  if (ch.outer != 2) {
     for (const FastPencil& f : fast_pencil_table())
-      if (f.no == no && g.ny % f.ty == 0) L.fp = &f;
+      if (f.no == no && g.ny % f.ty == 0 && f.nc == g.nc && (L.mode3d || !f.only3d)) L.fp = &f;
   }
   if (L.fp) L.grid_outer = (long long)(g.ny / L.fp->ty) * mids;  // blocks of the fast pencil kernel
   // the TMA pencil where a shape matches: by default (WAVESIM_B200_K2=plain keeps kf_pencil), or the
@@ -796,15 +822,11 @@ static cudaError_t launch_k2(const Solver* s, int w) {
   if (s->lay.fp) {
     OuterArgs a = outer_args(s, w);
     const FastPencil* f = s->lay.fp;
-    const int th = f->ty * (f->no / 16);
-    const long long mids = s->lay.mode3d ? s->g.nx : 1;
     const unsigned grid = (unsigned)(s->lay.grid_outer * s->nrhs);
-    (void)mids;
-    const size_t smem = (size_t)(f->ty + 1) * f->no * sizeof(float2);
     float2* T = s->d_T;
     const DevState* st = s->d_state;
     void* args[] = {&a, &T, &st};
-    return cudaLaunchKernel(f->fn, dim3(grid), dim3(th), args, smem, s->stream);
+    return cudaLaunchKernel(f->fn, dim3(grid), dim3(f->threads), args, f->smem, s->stream);
   }
   return s->lay.rset == kPow2 ? launch_k2_t<kPow2>(s, w) : launch_k2_t<kMixed>(s, w);
 }

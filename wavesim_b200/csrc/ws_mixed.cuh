@@ -1,0 +1,377 @@
+// Register-resident fused MBS kernels for line lengths that are not powers
+// of two (and for the vector Green's function), e.g. the 192^3 x 3 grid of
+// a WaveSimVector problem with a 16-pixel boundary.
+//
+// A line of N points is held by P = N / E threads with E elements each, and
+// transformed by a Stockham schedule fixed at compile time: radices
+// R0 = E, R1, R2 with R0 R1 R2 = N and R1, R2 dividing E (192 = 12 x 4 x 4,
+// E = 12).  Thread p enters with v[r] = x[p + P r] and leaves with
+// v[m] = X[p + P m], as in the power-of-two kernels; stage s > 0 reads the
+// R inputs x[j + r N/R] of its butterflies j = p + P q, multiplies them by
+// W_{Ns R}^{(j mod Ns) r} (Ns = product of the earlier radices), applies the
+// radix-R DFT and writes output r to (j - j mod Ns) R + j mod Ns + r Ns.
+//
+//   km_plane_fwd<PL, C>  K1: (y, x) planes on a cluster of C blocks; y
+//                        transforms of N / C columns per block, then each
+//                        block pulls its N / C rows from the cluster
+//                        (distributed shared memory) for the x transforms.
+//   km_pencil<PL, TY, NC> K2: z pencils of NC components, scalar or dyadic
+//                        Green's function (f_g0_scalar.m / f_g0_vector.m).
+//   km_plane_inv<PL, C>  K3: the inverse of K1, then the epilogue of the
+//                        power-of-two K3 (unwiggle, f_mix, E' += dE', ROI energy).
+#pragma once
+#include "ws_fast.cuh"
+
+namespace ws {
+namespace mixed {
+
+constexpr int kThreads = 256;
+
+template <int N_, int E_, int R0, int R1, int R2 = 1>
+struct Plan {
+  static constexpr int N = N_, E = E_, P = N_ / E_;
+  static constexpr int NST = R2 > 1 ? 3 : (R1 > 1 ? 2 : 1);
+  __host__ __device__ static constexpr int radix(int s) { return s == 0 ? R0 : (s == 1 ? R1 : R2); }
+  __host__ __device__ static constexpr int span(int s) { return s == 0 ? 1 : (s == 1 ? R0 : R0 * R1); }
+  static_assert(R0 * R1 * R2 == N_, "the radices multiply to N");
+  static_assert(R0 == E_ && E_ % R1 == 0 && E_ % R2 == 0, "first radix = elements per thread, the others divide it");
+};
+
+template <int R, bool INV, int E>
+__device__ __forceinline__ void dft_at(float2 (&v)[E], int off) {
+  float2 u[R];
+#pragma unroll
+  for (int r = 0; r < R; ++r) u[r] = v[off + r];
+  Dft<R, INV>::run(u);
+#pragma unroll
+  for (int r = 0; r < R; ++r) v[off + r] = u[r];
+}
+
+template <class PL, bool INV, int S, class Line, class Sync>
+__device__ __forceinline__ void stage(float2 (&v)[PL::E], const Line& L, int p, const float2* __restrict__ tw,
+                                      Sync sync) {
+  constexpr int E = PL::E, N = PL::N, P = PL::P;
+  constexpr int R = PL::radix(S), Ns = PL::span(S), B = E / R, NR = N / R, TS = N / (Ns * R);
+  if constexpr (S > 0) {
+#pragma unroll
+    for (int q = 0; q < B; ++q) {
+      const int j = p + P * q;
+#pragma unroll
+      for (int r = 0; r < R; ++r) v[q * R + r] = L.at(j + r * NR);
+      const int jm = j % Ns;
+#pragma unroll
+      for (int r = 1; r < R; ++r) {
+        float2 w = __ldg(&tw[jm * r * TS]);
+        if (INV) w.y = -w.y;
+        v[q * R + r] = cmul(v[q * R + r], w);
+      }
+    }
+  }
+#pragma unroll
+  for (int q = 0; q < B; ++q) dft_at<R, INV>(v, q * R);
+  if constexpr (S < PL::NST - 1) {
+    sync();
+#pragma unroll
+    for (int q = 0; q < B; ++q) {
+      const int j = p + P * q;
+      const int jm = j % Ns;
+      const int base = (j - jm) * R + jm;
+#pragma unroll
+      for (int r = 0; r < R; ++r) L.at(base + r * Ns) = v[q * R + r];
+    }
+    sync();
+  } else if constexpr (B > 1) {
+    float2 t[E];
+#pragma unroll
+    for (int q = 0; q < B; ++q)
+#pragma unroll
+      for (int r = 0; r < R; ++r) t[q + B * r] = v[q * R + r];
+#pragma unroll
+    for (int m = 0; m < E; ++m) v[m] = t[m];
+  }
+}
+
+// In: v[r] = x[p + P r].  Out: v[m] = X[p + P m] (unnormalised; INV: sign +1).
+template <class PL, bool INV, class Line, class Sync>
+__device__ __forceinline__ void line_fft(float2 (&v)[PL::E], const Line& L, int p, const float2* __restrict__ tw,
+                                         Sync sync) {
+  stage<PL, INV, 0>(v, L, p, tw, sync);
+  if constexpr (PL::NST > 1) stage<PL, INV, 1>(v, L, p, tw, sync);
+  if constexpr (PL::NST > 2) stage<PL, INV, 2>(v, L, p, tw, sync);
+}
+
+// Shared-memory tiles of the plane kernels (one buffer, used twice):
+//   column tile: column cl of the block at cl * CS, element y at y + y / 16
+//   row tile:    element (row kyl, x) at x * RS + kyl
+template <class PL, int C>
+struct MGeom {
+  static constexpr int N = PL::N, P = PL::P;
+  static constexpr int M = N / C;   // columns per block
+  static constexpr int LR = N / C;  // rows per block
+  static constexpr int CS = N + N / 16 + 1;
+  static constexpr int RS = LR + 1;
+  static constexpr int LPR = kThreads / P;  // lines per round
+  static constexpr int PER = LR * N / kThreads;  // elements each thread carries across the cluster
+  static constexpr size_t smem = sizeof(float2) * (size_t)(M * CS > N * RS ? M * CS : N * RS);
+  static_assert(N % C == 0 && M % LPR == 0 && (LR * N) % kThreads == 0, "plane split");
+  static_assert(kThreads % P == 0 && (P <= 32 ? 32 % P == 0 : true), "threads per line");
+};
+
+template <int P>
+struct LineSync {
+  using type = fast::SyncBlock;
+};
+template <>
+struct LineSync<16> {
+  using type = fast::SyncWarp;
+};
+template <>
+struct LineSync<8> {
+  using type = fast::SyncWarp;
+};
+
+// K1 --------------------------------------------------------------------------
+template <class PL, int C>
+__global__ void __launch_bounds__(kThreads, 3)
+    km_plane_fwd(InnerArgs a, const float2* __restrict__ dE, const float2* __restrict__ src, float2 A,
+                 float2* __restrict__ T, const DevState* __restrict__ st) {
+  using G = MGeom<PL, C>;
+  constexpr int N = PL::N, E = PL::E, P = PL::P, M = G::M, LR = G::LR, LPR = G::LPR;
+  const int rhs = blockIdx.x / a.bpr, bid = blockIdx.x - rhs * a.bpr;
+  st += rhs;
+  if (load_done(st)) return;  // the same for every block of a cluster (one right-hand side)
+  dE += rhs * a.fstride;
+  if (src) src += rhs * a.fstride;
+  T += rhs * a.fstride;
+  extern __shared__ float2 sm[];
+  const int tid = threadIdx.x;
+  const Geom& g = a.g;
+  const int rank = bid % C, plane = bid / C, z = plane % g.nz;
+  const int x0 = rank * M;
+  const long long colbase = (long long)plane * N + x0;
+  const float2 gzz = a.w.gz[z];
+  // y transforms of the block's columns, straight from global memory
+  for (int c0 = 0; c0 < M; c0 += LPR) {
+    const int cl = c0 + tid / P, p = tid % P;
+    const long long col = colbase + cl;
+    const float2 gxz = cmul(a.w.gx[x0 + cl], gzz);
+    const float2* __restrict__ s = dE + col * N;
+    const float2* __restrict__ sr = src ? src + col * N : nullptr;
+    float2 v[E];
+#pragma unroll
+    for (int r = 0; r < E; ++r) {
+      const int y = p + P * r;
+      float2 e = s[y];
+      if (sr) e = cadd(e, cmul(A, sr[y]));
+      v[r] = cmul(cmul(e, gxz), a.w.gy[y]);
+    }
+    fast::ColLine L{sm + cl * G::CS};
+    line_fft<PL, false>(v, L, p, a.py.tw, typename LineSync<P>::type{});
+#pragma unroll
+    for (int m = 0; m < E; ++m) L.at(p + P * m) = v[m];
+  }
+  cg::cluster_group cluster = cg::this_cluster();
+  cluster.sync();
+  // rows [rank LR, rank LR + LR) of all N columns, from the blocks holding them
+  float2 hold[G::PER];
+#pragma unroll
+  for (int i = 0; i < G::PER; ++i) {
+    const int e = tid + kThreads * i;
+    const int kyl = e % LR, x = e / LR;
+    const int ky = rank * LR + kyl;
+    const float2* rs = cluster.map_shared_rank(sm, x / M);
+    hold[i] = rs[(x % M) * G::CS + ky + (ky >> 4)];
+  }
+  cluster.sync();
+#pragma unroll
+  for (int i = 0; i < G::PER; ++i) {
+    const int e = tid + kThreads * i;
+    sm[(e / LR) * G::RS + e % LR] = hold[i];
+  }
+  __syncthreads();
+  constexpr int RPR = kThreads / P;
+  for (int r0 = 0; r0 < LR; r0 += RPR) {
+    const int rl = r0 + tid % RPR, p = tid / RPR;
+    fast::RowLine L{sm + rl, G::RS};
+    float2 v[E];
+#pragma unroll
+    for (int r = 0; r < E; ++r) v[r] = L.at(p + P * r);
+    line_fft<PL, false>(v, L, p, a.twx, fast::SyncBlock{});
+    float2* __restrict__ d = T + (long long)plane * N * N + rank * LR + rl;
+#pragma unroll
+    for (int m = 0; m < E; ++m) d[(long long)(p + P * m) * N] = v[m];
+  }
+}
+
+// K2 --------------------------------------------------------------------------
+template <class PL, int TY, int NC>
+__global__ void __launch_bounds__(TY* PL::P, NC == 1 ? 2 : 1)
+    km_pencil(OuterArgs a, float2* __restrict__ T, const DevState* __restrict__ st) {
+  constexpr int E = PL::E, P = PL::P, TYS = TY + 1;
+  const int rhs = blockIdx.x / a.bpr, bid = blockIdx.x - rhs * a.bpr;
+  st += rhs;
+  if (load_done(st)) return;
+  T += rhs * a.fstride;
+  extern __shared__ float2 sm[];
+  const Geom& g = a.g;
+  const int tid = threadIdx.x;
+  const int yl = tid % TY, p = tid / TY;
+  const int nyt = g.ny / TY;
+  const int yt = bid % nyt, mid = bid / nyt;
+  const int ky = yt * TY + yl;
+  const long long ps = (long long)g.ny * g.nx;
+  float2* __restrict__ base = T + ky + (long long)g.ny * mid;
+  float2 v[NC][E];
+#pragma unroll
+  for (int c = 0; c < NC; ++c)
+#pragma unroll
+    for (int r = 0; r < E; ++r) v[c][r] = base[ps * (p + P * r) + g.npts * c];
+  fast::RowLine L{sm + yl, TYS};
+#pragma unroll
+  for (int c = 0; c < NC; ++c) line_fft<PL, false>(v[c], L, p, a.po.tw, fast::SyncBlock{});
+  const float px = a.w.pxe[mid], py = a.w.pye[ky];
+  const float di = -a.k02e.y;
+#pragma unroll
+  for (int m = 0; m < E; ++m) {
+    const float pz = a.w.pze[p + P * m];
+    const float dr = fmaf(px, px, fmaf(py, py, pz * pz)) - a.k02e.x;
+    const float inv = __fdividef(a.norm, fmaf(dr, dr, di * di));
+    const float2 g0 = make_float2(dr * inv, -di * inv);
+    if constexpr (NC == 1) {
+      // f_g0_scalar with the 1/N of ifftn: E ./ (px^2 + py^2 + (pz^2 - k02e))
+      v[0][m] = cmul(v[0][m], g0);
+    } else {
+      // f_g0_vector: div = (p . E) / k02e; E_i <- (E_i - p_i div) / (|p|^2 - k02e)
+      const float2 ex = v[0][m], ey = v[1][m], ez = v[2][m];
+      const float2 pe =
+          make_float2(fmaf(px, ex.x, fmaf(py, ey.x, pz * ez.x)), fmaf(px, ex.y, fmaf(py, ey.y, pz * ez.y)));
+      const float kk = fmaf(a.k02e.x, a.k02e.x, a.k02e.y * a.k02e.y);
+      const float2 dv =
+          make_float2((pe.x * a.k02e.x + pe.y * a.k02e.y) / kk, (pe.y * a.k02e.x - pe.x * a.k02e.y) / kk);
+      v[0][m] = cmul(g0, make_float2(ex.x - px * dv.x, ex.y - px * dv.y));
+      v[1][m] = cmul(g0, make_float2(ey.x - py * dv.x, ey.y - py * dv.y));
+      v[2][m] = cmul(g0, make_float2(ez.x - pz * dv.x, ez.y - pz * dv.y));
+    }
+  }
+#pragma unroll
+  for (int c = 0; c < NC; ++c) line_fft<PL, true>(v[c], L, p, a.po.tw, fast::SyncBlock{});
+#pragma unroll
+  for (int c = 0; c < NC; ++c)
+#pragma unroll
+    for (int m = 0; m < E; ++m) base[ps * (p + P * m) + g.npts * c] = v[c][m];
+}
+
+// K3 --------------------------------------------------------------------------
+template <class PL, int C>
+__global__ void __launch_bounds__(kThreads, 2)
+    km_plane_inv(InnerArgs a, const float2* __restrict__ T, float2* __restrict__ dE, float2* __restrict__ E,
+                 const float2* __restrict__ gamma, const DevState* __restrict__ st, double* __restrict__ partials) {
+  using G = MGeom<PL, C>;
+  constexpr int N = PL::N, EL = PL::E, P = PL::P, M = G::M, LR = G::LR, LPR = G::LPR;
+  const int rhs = blockIdx.x / a.bpr, bid = blockIdx.x - rhs * a.bpr;
+  st += rhs;
+  if (load_done(st)) return;
+  // with a.acc2, E' takes dE'_{k-1} + dE'_k after even iterations k only
+  const bool acc_now = !a.acc2 || (__ldcg(&st->it) & 1) == 0;
+  T += rhs * a.fstride;
+  dE += rhs * a.fstride;
+  E += rhs * a.fstride;
+  partials += (long long)rhs * a.bpr;
+  extern __shared__ float2 sm[];
+  __shared__ float red[kThreads / 32];
+  const int tid = threadIdx.x;
+  const Geom& g = a.g;
+  const int rank = bid % C, plane = bid / C, z = plane % g.nz, comp = plane / g.nz;
+  const int x0 = rank * M;
+  const long long colbase = (long long)plane * N + x0;
+  // inverse x transforms of the block's rows, straight from global memory
+  constexpr int RPR = kThreads / P;
+  for (int r0 = 0; r0 < LR; r0 += RPR) {
+    const int rl = r0 + tid % RPR, p = tid / RPR;
+    const float2* __restrict__ s = T + (long long)plane * N * N + rank * LR + rl;
+    float2 v[EL];
+#pragma unroll
+    for (int r = 0; r < EL; ++r) v[r] = s[(long long)(p + P * r) * N];
+    fast::RowLine L{sm + rl, G::RS};
+    line_fft<PL, true>(v, L, p, a.twx, fast::SyncBlock{});
+#pragma unroll
+    for (int m = 0; m < EL; ++m) L.at(p + P * m) = v[m];
+  }
+  cg::cluster_group cluster = cg::this_cluster();
+  cluster.sync();
+  // columns [x0, x0 + M) of all N rows, from the blocks holding them
+  float2 hold[G::PER];
+#pragma unroll
+  for (int i = 0; i < G::PER; ++i) {
+    const int e = tid + kThreads * i;
+    const int ky = e % N, c = e / N;
+    const float2* rs = cluster.map_shared_rank(sm, ky / LR);
+    hold[i] = rs[(x0 + c) * G::RS + ky % LR];
+  }
+  cluster.sync();
+#pragma unroll
+  for (int i = 0; i < G::PER; ++i) {
+    const int e = tid + kThreads * i;
+    const int ky = e % N, c = e / N;
+    sm[c * G::CS + ky + (ky >> 4)] = hold[i];
+  }
+  __syncthreads();
+  const float2 gzz = a.w.gz[z];
+  float esum = 0.f;
+  for (int c0 = 0; c0 < M; c0 += LPR) {
+    const int cl = c0 + tid / P, p = tid % P;
+    fast::ColLine L{sm + cl * G::CS};
+    float2 v[EL];
+#pragma unroll
+    for (int r = 0; r < EL; ++r) v[r] = L.at(p + P * r);
+    line_fft<PL, true>(v, L, p, a.py.tw, typename LineSync<P>::type{});
+    const int x = x0 + cl;
+    const long long col = colbase + cl;
+    const float2 gxz = cmul(a.w.gx[x], gzz);
+    const bool in_xzc =
+        x >= g.r0[1] && x < g.r1[1] && z >= g.r0[2] && z < g.r1[2] && comp >= g.r0[3] && comp < g.r1[3];
+    const long long gcol = col * N;
+    const float2* __restrict__ gmc = gamma + (gcol - (long long)comp * g.npts);
+    float2* __restrict__ dEc = dE + gcol;
+    float2* __restrict__ Ec = E + gcol;
+    // Eprop after the conjugate ramps (WaveSim.m:55), then f_mix (f_mix.m:3-4)
+    // and E += dE; the loads of a half are issued together.
+    constexpr int H = EL / 2;
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      float2 gm[H], d0[H], e0[H];
+#pragma unroll
+      for (int i = 0; i < H; ++i) {
+        const int y = p + P * (H * h + i);
+        gm[i] = gmc[y];
+        d0[i] = dEc[y];
+        e0[i] = acc_now ? Ec[y] : make_float2(0.f, 0.f);
+      }
+#pragma unroll
+      for (int i = 0; i < H; ++i) {
+        const int m = H * h + i;
+        const int y = p + P * m;
+        const float2 ep = cmul_conj(cmul_conj(v[m], gxz), a.w.gy[y]);
+        const float2 one_m = make_float2(1.f - kAlpha * gm[i].x, -kAlpha * gm[i].y);
+        const float2 t = cmul(cmul(gm[i], gm[i]), ep);
+        const float2 dn = cadd(cmul(one_m, d0[i]), make_float2(kAlpha * t.y, -kAlpha * t.x));
+        dEc[y] = dn;
+        if (acc_now) Ec[y] = cadd(e0[i], a.acc2 ? cadd(d0[i], dn) : dn);
+        if (in_xzc && y >= g.r0[0] && y < g.r1[0]) esum = fmaf(dn.x, dn.x, fmaf(dn.y, dn.y, esum));
+      }
+    }
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) esum += __shfl_xor_sync(0xffffffffu, esum, o);
+  if ((tid & 31) == 0) red[tid >> 5] = esum;
+  __syncthreads();
+  if (tid < 32) {
+    float v = tid < kThreads / 32 ? red[tid] : 0.f;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    if (tid == 0) partials[bid] = (double)v;
+  }
+}
+
+}  // namespace mixed
+}  // namespace ws
