@@ -258,6 +258,47 @@ int ws_solver_autotune(ws_solver s, int n_iterations, int* n_tried, float* ms_be
 
 int ws_solver_destroy(ws_solver s);
 
+/* ------------------------------------------------------------------------
+ * PSTD: the reference's pseudo-spectral time-domain comparison solver
+ * (PSTD.m:22-137) on the same FFT kernels.  Replaces PSTD.run_algorithm
+ * (PSTD.m:79-127); the constructor's set-up (time step, coefficient maps,
+ * Fourier ranges, PSTD.m:22-77) stays with the caller.
+ * ------------------------------------------------------------------------ */
+typedef struct ws_pstd_s* ws_pstd;
+
+/* A(Ncycle), the source amplitude of PSTD.source_amplitude (PSTD.m:10). */
+typedef void (*ws_amplitude_fn)(double ncycle, double* re, double* im, void* user_data);
+
+typedef struct ws_pstd_options {
+  int64_t max_iterations;        /* ceil(max_cycles * iterations_per_cycle) (Simulation.m:165); as in
+                                    Simulation.next the run stops there only on a step with real(A) > 0.9 */
+  double energy_threshold;       /* Simulation.energy_threshold */
+  int64_t energy_interval;       /* Simulation.energy_calculation_interval */
+  double iterations_per_cycle;   /* lambda / dt (PSTD.m:55); step it runs at Ncycle = it / this */
+  ws_amplitude_fn amplitude;     /* NULL: PSTD.default_source (PSTD.m:130-137) */
+  void* user_data;
+} ws_pstd_options;
+
+void ws_pstd_default_options(ws_pstd_options* opts);
+
+/* N = grid (Ny, Nx, Nz); c1, c2, c3 = the real coefficient maps of the damped
+ * leapfrog (PSTD.m:57-63, N(1) N(2) N(3) floats, column-major, host);
+ * px, py, pz = SimulationGrid px_range (Nx), py_range (Ny), pz_range (Nz);
+ * roi = 1-based [first; last] per dimension as in ws_solver_create. */
+int ws_pstd_create(const int64_t N[3], const float* c1, const float* c2, const float* c3, const float* px,
+                   const float* py, const float* pz, const int64_t roi[8], int device, ws_pstd* out);
+
+/* Runs PSTD.run_algorithm for the source blocks (positions on the grid,
+ * 1-based, cropped).  E_out (host) receives the ROI field times
+ * exp(-i arg A(it_final / iterations_per_cycle)) (PSTD.m:125-126),
+ * diff_energy_out (host, may be NULL) the first diff_capacity entries of
+ * state.diff_energy. */
+int ws_pstd_run(ws_pstd h, int64_t n_blocks, const ws_source_block* source, int source_memory,
+                const ws_pstd_options* opts, ws_complex* E_out, double* diff_energy_out, int64_t diff_capacity,
+                int64_t* n_iterations, int* converged);
+
+int ws_pstd_destroy(ws_pstd h);
+
 /*
  * Medium set-up on the device (no counterpart in the reference, which builds
  * gamma in MATLAB on the host; WaveSimBase.m:58-81, 201-258, Medium.m:44-62).

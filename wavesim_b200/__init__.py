@@ -9,6 +9,7 @@ if it has not been built.
 from ._lib import WaveSimError, lib  # noqa: F401  (fails loudly if the library is missing)
 from .problem import Medium, PlaneWave, SimulationGrid, Source, efficient_size, symrange  # noqa: F401
 from .simulation import WaveSim, WaveSimVector, nuttallwin, wiggle_perm  # noqa: F401
+from .pstd import PSTD  # noqa: F401
 
 __all__ = ["WaveSim", "WaveSimVector", "Source", "Medium", "SimulationGrid", "WaveSimError",
            "efficient_size", "symrange", "nuttallwin", "wiggle_perm"]

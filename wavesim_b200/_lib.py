@@ -73,7 +73,16 @@ EXPORTS = [
     "ws_solver_launches_per_iteration", "ws_solver_warm_report", "ws_solver_autotune", "ws_solver_destroy",
     "ws_run_algorithm_noalloc", "ws_medium_reduce", "ws_build_gamma", "ws_setup_last_error",
     "ws_noalloc_scratch_bytes", "ws_noalloc_last_error",
+    "ws_pstd_default_options", "ws_pstd_create", "ws_pstd_run", "ws_pstd_destroy",
 ]
+
+
+AMPLITUDE = C.CFUNCTYPE(None, C.c_double, C.POINTER(C.c_double), C.POINTER(C.c_double), C.c_void_p)
+
+
+class ws_pstd_options(C.Structure):
+    _fields_ = [("max_iterations", C.c_int64), ("energy_threshold", C.c_double), ("energy_interval", C.c_int64),
+                ("iterations_per_cycle", C.c_double), ("amplitude", AMPLITUDE), ("user_data", C.c_void_p)]
 
 
 class WaveSimError(RuntimeError):
@@ -138,6 +147,15 @@ def _load():
                                              C.POINTER(C.c_int), P]
     lib.ws_run_algorithm_noalloc.restype = C.c_int
     lib.ws_noalloc_scratch_bytes.restype = C.c_int64
+    lib.ws_pstd_default_options.argtypes = [C.POINTER(ws_pstd_options)]
+    lib.ws_pstd_default_options.restype = None
+    lib.ws_pstd_create.argtypes = [i64p, P, P, P, P, P, P, i64p, C.c_int, C.POINTER(C.c_void_p)]
+    lib.ws_pstd_create.restype = C.c_int
+    lib.ws_pstd_run.argtypes = [P, C.c_int64, C.POINTER(ws_source_block), C.c_int, C.POINTER(ws_pstd_options), P,
+                                C.POINTER(C.c_double), C.c_int64, i64p, C.POINTER(C.c_int)]
+    lib.ws_pstd_run.restype = C.c_int
+    lib.ws_pstd_destroy.argtypes = [P]
+    lib.ws_pstd_destroy.restype = C.c_int
     lib.ws_gemm_bf16.argtypes = [P, P, P, P, P, C.c_int64, C.c_int64, C.c_int64, C.c_int64, C.c_int64, C.c_int64,
                                  C.c_int, P, P]
     lib.ws_gemm_bf16.restype = C.c_int

@@ -390,15 +390,28 @@ __global__ void __launch_bounds__(TY*(NO / 16) < 1024 ? TY*(NO / 16) : 1024, 3)
   const float pxm = a.mode3d ? a.w.pxe[mid] : 0.f;
   const float base2 = a.mode3d ? fmaf(pxm, pxm, py * py) : fmaf(py, py, a.w.pze[0] * a.w.pze[0]);
   const float di = -a.k02e.y;
+  if (a.pstd) {
 #pragma unroll
-  for (int m = 0; m < 16; ++m) {
-    const int ko = p + P * m;
-    const float po = a.mode3d ? a.w.pze[ko] : a.w.pxe[ko];
-    const float dr = fmaf(po, po, base2) - a.k02e.x;
-    const float inv = __fdividef(a.norm, fmaf(dr, dr, di * di));
-    v[m] = cmul(v[m], make_float2(dr * inv, -di * inv));
+    for (int m = 0; m < 16; ++m) {  // PSTD Laplacian -|p|^2 / N (k02e = 0)
+      const int ko = p + P * m;
+      const float po = a.mode3d ? a.w.pze[ko] : a.w.pxe[ko];
+      const float f = -fmaf(po, po, base2) * a.norm;
+      v[m] = make_float2(f * v[m].x, f * v[m].y);
+    }
+  } else {
+#pragma unroll
+    for (int m = 0; m < 16; ++m) {
+      const int ko = p + P * m;
+      const float po = a.mode3d ? a.w.pze[ko] : a.w.pxe[ko];
+      const float dr = fmaf(po, po, base2) - a.k02e.x;
+      const float inv = __fdividef(a.norm, fmaf(dr, dr, di * di));
+      v[m] = cmul(v[m], make_float2(dr * inv, -di * inv));
+    }
   }
   line_fft<NO, true>(v, L, p, a.po.tw, SyncBlock{});
+  if (a.pstd)
+#pragma unroll
+    for (int m = 0; m < 16; ++m) v[m].y = -v[m].y;
 #pragma unroll
   for (int m = 0; m < 16; ++m) base[ps * (p + P * m)] = v[m];
 }

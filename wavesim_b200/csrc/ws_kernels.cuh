@@ -111,6 +111,8 @@ struct OuterArgs {
   int bpr;
   long long fstride;
   int pf;       // fast kernels: block b pulls the inputs of block b + pf into L2 (0: off)
+  int pstd;     // 1: PSTD Laplacian -(px^2 + py^2 + pz^2) / N instead of the Green's function
+                // (k02e = 0), and the output conjugated (scalar fields only)
 };
 
 __device__ __forceinline__ int load_done(const DevState* st) { return __ldcg(&st->done); }
@@ -257,9 +259,13 @@ __global__ void __launch_bounds__(512, 1) k_outer(OuterArgs a, float2* __restric
       // f_g0_scalar: E ./ (px^2 + py^2 + (pz^2 - k02e))
       const float dr = fmaf(px, px, fmaf(py, py, pz * pz)) - a.k02e.x;
       const float di = -a.k02e.y;
-      const float inv = a.norm / fmaf(dr, dr, di * di);
       const int ad = o * RS + yl + (yl >> 4);
-      sm[ad] = cmul(sm[ad], make_float2(dr * inv, -di * inv));
+      if (a.pstd) {
+        sm[ad] = make_float2(-dr * a.norm * sm[ad].x, -dr * a.norm * sm[ad].y);  // PSTD.m:68
+      } else {
+        const float inv = a.norm / fmaf(dr, dr, di * di);
+        sm[ad] = cmul(sm[ad], make_float2(dr * inv, -di * inv));
+      }
     } else {
       // f_g0_vector: div = (p . E) / k02e; E_i <- (E_i - p_i div) / (|p|^2 - k02e)
       const int l0 = yl, l1 = ty + yl, l2 = 2 * ty + yl;
@@ -283,7 +289,11 @@ __global__ void __launch_bounds__(512, 1) k_outer(OuterArgs a, float2* __restric
     const int yl = e % ty, r = e / ty;
     const int c = r % nc, o = r / nc;
     const int l = c * ty + yl;
-    if (y0 + yl < g.ny) T[base + yl + ps * o + g.npts * c] = sm[o * RS + l + (l >> 4)];
+    if (y0 + yl < g.ny) {
+      float2 v = sm[o * RS + l + (l >> 4)];
+      if (a.pstd) v.y = -v.y;
+      T[base + yl + ps * o + g.npts * c] = v;
+    }
   }
 }
 

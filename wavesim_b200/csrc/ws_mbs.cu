@@ -340,6 +340,7 @@ struct Solver {
   int tma_blocks = 0;            // resident blocks of the TMA pencil (its persistent grid)
   int pf_inner = 0, pf_outer = 0;  // L2 prefetch distance of the fast kernels, in blocks (0: off)
   bool warm = false;             // the current solve starts from d_init
+  int pstd = 0;                  // a PSTD stepper's solver: K2 applies the Laplacian (see ws_pstd_*)
   LayoutChoice tuned{};          // the autotuner's choice (all zero: the heuristics)
   double warm_ratio = 0.0;       // discard threshold of the current solve
   float2* d_tw = nullptr;
@@ -671,11 +672,12 @@ static OuterArgs outer_args(const Solver* s, int w) {
   a.bpr = (int)s->lay.grid_outer;
   a.fstride = (long long)field_elems(s);
   a.pf = 0;  // K2 measured slower with it
+  a.pstd = s->pstd;
   return a;
 }
 
 template <int RS>
-static cudaError_t launch_k1_t(const Solver* s, int w, bool with_source) {
+static cudaError_t launch_k1_t(const Solver* s, int w, const float2* in, const float2* src, float2* out) {
   const float2 A = make_float2(0.f, (float)(1.0f / s->eps / (float)s->nw));  // 1i/epsilon/Nwiggles
   cudaLaunchConfig_t cfg{};
   cfg.gridDim = dim3((unsigned)(s->lay.grid_inner * s->nrhs));
@@ -689,8 +691,7 @@ static cudaError_t launch_k1_t(const Solver* s, int w, bool with_source) {
   attr[0].val.clusterDim.z = 1;
   cfg.attrs = attr;
   cfg.numAttrs = 1;
-  return cudaLaunchKernelEx(&cfg, k_fwd_inner<kEmax, RS>, inner_args(s, w), (const float2*)s->d_dE,
-                            (const float2*)(with_source ? s->d_src : nullptr), A, s->d_T,
+  return cudaLaunchKernelEx(&cfg, k_fwd_inner<kEmax, RS>, inner_args(s, w), in, src, A, out,
                             (const DevState*)s->d_state);
 }
 
@@ -740,20 +741,21 @@ static cudaError_t launch_fast_inner(const Solver* s, const void* fn, void** arg
   return cudaLaunchKernelExC(&cfg, fn, args);
 }
 
-static cudaError_t launch_k1(const Solver* s, int w, bool with_source) {
+// K1 on explicit buffers: out = inner FFT of (in + A src) times the ramps of wiggle w
+static cudaError_t launch_k1_io(const Solver* s, int w, const float2* in, const float2* src, float2* out) {
   if (s->lay.fi) {
     InnerArgs a = inner_args(s, w);
     a.ncols = s->lay.ncols;
     a.pf = s->pf_inner;  // K1 only: its loads come first, so the next wave's columns are worth pulling early
-    const float2* dE = s->d_dE;
-    const float2* src = with_source ? s->d_src : nullptr;
     float2 A = make_float2(0.f, (float)(1.0f / s->eps / (float)s->nw));
-    float2* T = s->d_T;
     const DevState* st = s->d_state;
-    void* args[] = {&a, &dE, &src, &A, &T, &st};
+    void* args[] = {&a, &in, &src, &A, &out, &st};
     return launch_fast_inner(s, s->lay.fi->fwd, args);
   }
-  return s->lay.rset == kPow2 ? launch_k1_t<kPow2>(s, w, with_source) : launch_k1_t<kMixed>(s, w, with_source);
+  return s->lay.rset == kPow2 ? launch_k1_t<kPow2>(s, w, in, src, out) : launch_k1_t<kMixed>(s, w, in, src, out);
+}
+static cudaError_t launch_k1(const Solver* s, int w, bool with_source) {
+  return launch_k1_io(s, w, s->d_dE, with_source ? s->d_src : nullptr, s->d_T);
 }
 // cuTensorMapEncodeTiled through the runtime's driver entry point (no link
 // against libcuda)
@@ -1633,6 +1635,318 @@ void ws_run_algorithm_release(void) {
     destroy_solver(s);
     s = nullptr;
   }
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// PSTD (PSTD.m): the reference's pseudo-spectral time-domain comparison
+// solver, on the same FFT kernels.  One step (PSTD.m:103-117):
+//   Etmp   = ifftn(-(px^2 + py^2 + pz^2) .* fftn(E)) + A(it) S
+//   E_next = c2 E + c1 E_prev + c3 Etmp
+// runs as K1 (inner FFT of E, unit ramps) -> K2 (outer FFT, Laplacian / N,
+// inverse outer FFT, conjugate) -> K1 again (inner FFT of the conjugate, so
+// that conj of its output is the inverse inner FFT) -> k_pstd_update (the
+// leapfrog, the source, the step energy |E_next - E e^{i(arg A - arg A_prev)}|^2
+// on the ROI) -> k_pstd_finish (Simulation.next with can_terminate =
+// real(A) > 0.9, energy / |A|^2).  E and E_prev swap buffers every step; the
+// source amplitudes A(it) of a chunk of steps come from the host.
+// ---------------------------------------------------------------------------
+namespace ws {
+
+struct PstdStep {
+  Geom g;
+  const float2* T2;    // inner FFT of conj(W): conj(T2) = ifftn(k fftn(E))
+  const float2* E;
+  const float2* Eprev;
+  float2* Enext;       // the buffer of Eprev
+  const float2* c12;   // (c1, c2) per point
+  const float* c3;
+  const float2* src;   // dense source field
+  const double2* amp;  // amp[k] = A at step it0 - 1 + k
+  long long it0;
+};
+
+struct PstdRule {
+  double threshold;
+  long long max_iter;
+  int interval;
+};
+
+static __global__ void __launch_bounds__(256) k_pstd_update(PstdStep a, const DevState* __restrict__ st,
+                                                            double* __restrict__ partials) {
+  if (load_done(st)) return;
+  const long long k = (long long)__ldcg(&st->it) - a.it0 + 1;
+  const double2 A = a.amp[k], Ap = a.amp[k - 1];
+  const double dphi = atan2(A.y, A.x) - atan2(Ap.y, Ap.x);
+  const float2 ps = make_float2((float)cos(dphi), (float)sin(dphi));
+  const float2 Af = make_float2((float)A.x, (float)A.y);
+  const Geom& g = a.g;
+  float esum = 0.f;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < g.npts;
+       i += (long long)gridDim.x * blockDim.x) {
+    float2 t = a.T2[i];
+    t.y = -t.y;
+    t = cadd(t, cmul(Af, a.src[i]));  // Source.add_to (Source.m:167-169)
+    const float2 c12 = a.c12[i];
+    const float c3 = a.c3[i];
+    const float2 e = a.E[i], ep = a.Eprev[i];
+    const float2 en = make_float2(c12.y * e.x + c12.x * ep.x + c3 * t.x, c12.y * e.y + c12.x * ep.y + c3 * t.y);
+    a.Enext[i] = en;
+    const int y = (int)(i % g.ny);
+    const long long r = i / g.ny;
+    const int x = (int)(r % g.nx), z = (int)(r / g.nx);
+    if (y >= g.r0[0] && y < g.r1[0] && x >= g.r0[1] && x < g.r1[1] && z >= g.r0[2] && z < g.r1[2]) {
+      const float2 d = make_float2(en.x - (e.x * ps.x - e.y * ps.y), en.y - (e.x * ps.y + e.y * ps.x));
+      esum = fmaf(d.x, d.x, fmaf(d.y, d.y, esum));
+    }
+  }
+  __shared__ float red[8];
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) esum += __shfl_xor_sync(0xffffffffu, esum, o);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = esum;
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    float v = threadIdx.x < blockDim.x / 32 ? red[threadIdx.x] : 0.f;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    if (threadIdx.x == 0) partials[blockIdx.x] = (double)v;
+  }
+}
+
+// Simulation.next (Simulation.m:193-217) for PSTD.run_algorithm (PSTD.m:108-124)
+static __global__ void k_pstd_finish(DevState* st, const double* __restrict__ partials, int nparts,
+                                     const double2* __restrict__ amp, long long it0, PstdRule rule,
+                                     double* __restrict__ hist, long long hist_cap) {
+  __shared__ double red[32];
+  if (load_done(st)) return;
+  double e = 0.0;
+  for (int i = threadIdx.x; i < nparts; i += blockDim.x) e += partials[i];
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) e += __shfl_xor_sync(0xffffffffu, e, o);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = e;
+  __syncthreads();
+  if (threadIdx.x != 0) return;
+  e = 0.0;
+  for (int w = 0; w < (int)(blockDim.x + 31) / 32; ++w) e += red[w];
+  const int it = st->it;
+  const double2 A = amp[it - it0 + 1];
+  if (st->calc_energy) st->last_step_energy = e / (A.x * A.x + A.y * A.y);
+  const double d = st->last_step_energy;
+  if (it - 1 < hist_cap) hist[it - 1] = d;
+  if (it == 1) st->diff1 = d;
+  const bool can_terminate = A.x > 0.9;  // MATLAB's A > 0.9 compares the real part
+  if (can_terminate && d / st->diff1 < rule.threshold) {
+    st->done = 1;
+    st->converged = 1;
+  } else if (can_terminate && it >= rule.max_iter) {
+    st->done = 1;
+    st->converged = 0;
+  }
+  st->calc_energy = ((it - 1) % rule.interval) == 0;
+  st->it = it + 1;
+}
+
+// ROI crop times a phase factor (PSTD.m:126)
+static __global__ void k_pstd_output(const float2* __restrict__ E, Geom g, float2 phase, float2* __restrict__ out) {
+  const int ry = g.r1[0] - g.r0[0], rx = g.r1[1] - g.r0[1], rz = g.r1[2] - g.r0[2];
+  const long long n = (long long)ry * rx * rz;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    long long r = i;
+    const int y = (int)(r % ry) + g.r0[0];
+    r /= ry;
+    const int x = (int)(r % rx) + g.r0[1];
+    const int z = (int)(r / rx) + g.r0[2];
+    out[i] = cmul(E[y + (long long)g.ny * (x + (long long)g.nx * z)], phase);
+  }
+}
+
+struct Pstd {
+  Solver* s = nullptr;       // layout, twiddles, T, source, state, stream (K2 in Laplacian mode)
+  float2* d_Ebuf = nullptr;  // two fields: step it reads E from (it - 1) % 2, writes E_next to it % 2
+  float2* d_T2 = nullptr;
+  float* d_c3 = nullptr;
+  double2* d_amp = nullptr;
+  double* d_hist = nullptr;
+  long long hist_cap = 0;
+  double* d_part = nullptr;
+  int nparts = 0;
+};
+
+static void pstd_free(Pstd* p) {
+  if (!p) return;
+  if (p->s) {
+    cudaSetDevice(p->s->device);
+    void* ptrs[] = {p->d_Ebuf, p->d_T2, p->d_c3, p->d_amp, p->d_hist, p->d_part};
+    for (void* q : ptrs)
+      if (q) cudaFree(q);
+    destroy_solver(p->s);
+  }
+  delete p;
+}
+
+static void pstd_default_amplitude(double ncycle, double* re, double* im, void*) {
+  // PSTD.m:130-137
+  const double env = 0.5 - 0.5 * std::cos(M_PI * std::min(ncycle / 100.0, 1.0));
+  *re = std::cos(-2.0 * M_PI * ncycle) * env;
+  *im = std::sin(-2.0 * M_PI * ncycle) * env;
+}
+
+constexpr int kPstdChunk = 256;  // steps launched between host checks of the stop flag
+
+}  // namespace ws
+
+extern "C" {
+
+int ws_pstd_create(const int64_t N[3], const float* c1, const float* c2, const float* c3, const float* px,
+                   const float* py, const float* pz, const int64_t roi[8], int device, ws_pstd* out) {
+  if (!N || !c1 || !c2 || !c3 || !px || !py || !pz || !roi || !out)
+    return fail(WS_ERR_INVALID_ARGUMENT, "null argument");
+  *out = nullptr;
+  const int64_t N4[4] = {N[0], N[1], N[2], 1};
+  for (int d = 0; d < 3; ++d)
+    if (N[d] < 1) return fail(WS_ERR_INVALID_ARGUMENT, "N must be positive");
+  const size_t npts = (size_t)N[0] * N[1] * N[2];
+  // the solver's gamma buffer holds (c1, c2); one wiggle with unit ramps and the plain Fourier ranges
+  std::vector<float2> c12(npts);
+  for (size_t i = 0; i < npts; ++i) c12[i] = make_float2(c1[i], c2[i]);
+  std::vector<float2> one((size_t)std::max(N[0], std::max(N[1], N[2])), make_float2(1.f, 0.f));
+  ws_wiggle w{px, py, pz, (const ws_complex*)one.data(), (const ws_complex*)one.data(),
+              (const ws_complex*)one.data()};
+  Pstd* p = new Pstd();
+  int rc = create_solver(N4, (const ws_complex*)c12.data(), 1, &w, 1.0f, ws_complex{0.f, 0.f}, roi, WS_HOST, device,
+                         &p->s);
+  if (rc) {
+    delete p;
+    return rc;
+  }
+  Solver* s = p->s;
+  s->pstd = 1;
+  p->nparts = (int)std::min<long long>(((long long)npts + 255) / 256, 8LL * kNumSms);
+  cudaError_t e = cudaSuccess;
+  if (e == cudaSuccess) e = cudaMalloc(&p->d_Ebuf, 2 * npts * sizeof(float2));
+  if (e == cudaSuccess) e = cudaMalloc(&p->d_T2, npts * sizeof(float2));
+  if (e == cudaSuccess) e = cudaMalloc(&p->d_c3, npts * sizeof(float));
+  if (e == cudaSuccess) e = cudaMalloc(&p->d_amp, (kPstdChunk + 1) * sizeof(double2));
+  if (e == cudaSuccess) e = cudaMalloc(&p->d_part, p->nparts * sizeof(double));
+  if (e == cudaSuccess) e = cudaMemcpy(p->d_c3, c3, npts * sizeof(float), cudaMemcpyHostToDevice);
+  if (e != cudaSuccess) {
+    pstd_free(p);
+    return fail(e == cudaErrorMemoryAllocation ? WS_ERR_OUT_OF_MEMORY : WS_ERR_CUDA, cudaGetErrorString(e));
+  }
+  *out = reinterpret_cast<ws_pstd>(p);
+  return WS_OK;
+}
+
+void ws_pstd_default_options(ws_pstd_options* o) {
+  if (!o) return;
+  std::memset(o, 0, sizeof(*o));
+  o->max_iterations = 100000;
+  o->energy_threshold = 1e-2;
+  o->energy_interval = 8;
+  o->iterations_per_cycle = 1.0;
+}
+
+int ws_pstd_run(ws_pstd h, int64_t n_blocks, const ws_source_block* source, int source_memory,
+                const ws_pstd_options* opts, ws_complex* E_out, double* diff_energy_out, int64_t diff_capacity,
+                int64_t* n_iterations, int* converged) {
+  if (!h || !opts || !E_out) return fail(WS_ERR_INVALID_ARGUMENT, "null argument");
+  if (opts->max_iterations < 1 || opts->energy_interval < 1 || !(opts->iterations_per_cycle > 0))
+    return fail(WS_ERR_INVALID_ARGUMENT, "bad options");
+  Pstd* p = reinterpret_cast<Pstd*>(h);
+  Solver* s = p->s;
+  WS_CUDA(cudaSetDevice(s->device));
+  const Geom& g = s->g;
+  if (n_blocks < 1 || !source) return fail(WS_ERR_NO_SOURCE, "There is no source inside the grid boundaries");
+  std::vector<double> energy;
+  int rc = upload_sources(s, 1, &n_blocks, source, source_memory, energy);
+  if (rc) return rc;
+  if (!(energy[0] > 0)) return fail(WS_ERR_NO_SOURCE, "There is no source inside the grid boundaries");
+  const long long cap = std::max<long long>(0, diff_capacity);
+  if (cap > p->hist_cap) {
+    if (p->d_hist) cudaFree(p->d_hist);
+    p->d_hist = nullptr;
+    p->hist_cap = 0;
+    WS_CUDA(cudaMalloc(&p->d_hist, cap * sizeof(double)));
+    p->hist_cap = cap;
+  }
+  const size_t npts = (size_t)g.npts;
+  WS_CUDA(cudaMemsetAsync(p->d_Ebuf, 0, 2 * npts * sizeof(float2), s->stream));
+  DevState st0{};
+  st0.it = 1;
+  st0.calc_energy = 1;
+  st0.last_step_energy = INFINITY;
+  WS_CUDA(cudaMemcpyAsync(s->d_state, &st0, sizeof(st0), cudaMemcpyHostToDevice, s->stream));
+  ws_amplitude_fn amp = opts->amplitude ? opts->amplitude : pstd_default_amplitude;
+  const PstdRule rule{opts->energy_threshold, (long long)opts->max_iterations, (int)opts->energy_interval};
+  std::vector<double2> hamp(kPstdChunk + 1);
+  double2 a_last = make_double2(1.0, 0.0);  // PSTD.m:83: A = 1 before the first step
+  long long it0 = 1;
+  DevState hst{};
+  const unsigned ublocks = (unsigned)p->nparts;
+  // Simulation.next stops at max_iterations only on a step that may terminate
+  // (real(A) > 0.9), as the reference does; past max_iterations plus a margin
+  // of max(1000, 2 iterations_per_cycle) steps the run ends unconverged.
+  const long long hard_stop =
+      opts->max_iterations + std::max<long long>(1000, (long long)std::ceil(2 * opts->iterations_per_cycle));
+  while (true) {
+    const long long K = kPstdChunk;
+    hamp[0] = a_last;
+    for (long long k = 1; k <= K; ++k)
+      amp((double)(it0 - 1 + k) / opts->iterations_per_cycle, &hamp[k].x, &hamp[k].y, opts->user_data);
+    WS_CUDA(cudaMemcpyAsync(p->d_amp, hamp.data(), (K + 1) * sizeof(double2), cudaMemcpyHostToDevice, s->stream));
+    for (long long k = 0; k < K; ++k) {
+      const long long it = it0 + k;
+      float2* E = p->d_Ebuf + (size_t)((it - 1) & 1) * npts;
+      float2* Ep = p->d_Ebuf + (size_t)(it & 1) * npts;
+      WS_CUDA(launch_k1_io(s, 0, E, nullptr, s->d_T));
+      WS_CUDA(launch_k2(s, 0));
+      WS_CUDA(launch_k1_io(s, 0, s->d_T, nullptr, p->d_T2));
+      PstdStep a{g, p->d_T2, E, Ep, Ep, (const float2*)s->d_gamma, p->d_c3, s->d_src, p->d_amp, it0};
+      k_pstd_update<<<ublocks, 256, 0, s->stream>>>(a, s->d_state, p->d_part);
+      WS_CUDA(cudaGetLastError());
+      k_pstd_finish<<<1, 256, 0, s->stream>>>(s->d_state, p->d_part, p->nparts, p->d_amp, it0, rule, p->d_hist,
+                                              p->hist_cap < cap ? p->hist_cap : cap);
+      WS_CUDA(cudaGetLastError());
+    }
+    WS_CUDA(cudaMemcpyAsync(&hst, s->d_state, sizeof(hst), cudaMemcpyDeviceToHost, s->stream));
+    WS_CUDA(cudaStreamSynchronize(s->stream));
+    if (hst.done || it0 + K > hard_stop) break;
+    a_last = hamp[K];
+    it0 += K;
+  }
+  int kerr = 0;
+  WS_CUDA(cudaMemcpy(&kerr, s->d_err, sizeof(int), cudaMemcpyDeviceToHost));
+  if (kerr) return fail(WS_ERR_CUDA, "a kernel's bounded wait gave up (cluster exchange or TMA load)");
+  const long long last = hst.it - 1;  // the last step run
+  double are = 1.0, aim = 0.0;
+  amp((double)hst.it / opts->iterations_per_cycle, &are, &aim, opts->user_data);  // PSTD.m:125
+  const double ph = -std::atan2(aim, are);
+  const float2 phase = make_float2((float)std::cos(ph), (float)std::sin(ph));
+  const long long nroi = (long long)(g.r1[0] - g.r0[0]) * (g.r1[1] - g.r0[1]) * (g.r1[2] - g.r0[2]);
+  if (s->out_cap < (size_t)nroi) {
+    if (s->d_out) cudaFree(s->d_out);
+    s->d_out = nullptr;
+    s->out_cap = 0;
+    WS_CUDA(cudaMalloc(&s->d_out, nroi * sizeof(float2)));
+    s->out_cap = nroi;
+  }
+  k_pstd_output<<<(unsigned)std::min<long long>((nroi + 255) / 256, 8LL * kNumSms), 256, 0, s->stream>>>(
+      p->d_Ebuf + (size_t)(last & 1) * npts, g, phase, s->d_out);
+  WS_CUDA(cudaGetLastError());
+  WS_CUDA(cudaMemcpyAsync(E_out, s->d_out, nroi * sizeof(float2), cudaMemcpyDeviceToHost, s->stream));
+  const long long nh = std::min<long long>(last, cap);
+  if (diff_energy_out && nh > 0)
+    WS_CUDA(cudaMemcpyAsync(diff_energy_out, p->d_hist, nh * sizeof(double), cudaMemcpyDeviceToHost, s->stream));
+  WS_CUDA(cudaStreamSynchronize(s->stream));
+  if (n_iterations) *n_iterations = last;
+  if (converged) *converged = hst.converged;
+  return WS_OK;
+}
+
+int ws_pstd_destroy(ws_pstd h) {
+  pstd_free(reinterpret_cast<Pstd*>(h));
+  return WS_OK;
 }
 
 }  // extern "C"

@@ -238,8 +238,9 @@ __global__ void __launch_bounds__(TY* PL::P, NC == 1 ? 2 : 1)
     const float inv = __fdividef(a.norm, fmaf(dr, dr, di * di));
     const float2 g0 = make_float2(dr * inv, -di * inv);
     if constexpr (NC == 1) {
-      // f_g0_scalar with the 1/N of ifftn: E ./ (px^2 + py^2 + (pz^2 - k02e))
-      v[0][m] = cmul(v[0][m], g0);
+      // f_g0_scalar with the 1/N of ifftn: E ./ (px^2 + py^2 + (pz^2 - k02e)),
+      // or the PSTD Laplacian (k02e = 0)
+      v[0][m] = a.pstd ? make_float2(-dr * a.norm * v[0][m].x, -dr * a.norm * v[0][m].y) : cmul(v[0][m], g0);
     } else {
       // f_g0_vector: div = (p . E) / k02e; E_i <- (E_i - p_i div) / (|p|^2 - k02e)
       const float2 ex = v[0][m], ey = v[1][m], ez = v[2][m];
@@ -255,6 +256,9 @@ __global__ void __launch_bounds__(TY* PL::P, NC == 1 ? 2 : 1)
   }
 #pragma unroll
   for (int c = 0; c < NC; ++c) line_fft<PL, true>(v[c], L, p, a.po.tw, fast::SyncBlock{});
+  if (NC == 1 && a.pstd)
+#pragma unroll
+    for (int m = 0; m < E; ++m) v[0][m].y = -v[0][m].y;
 #pragma unroll
   for (int c = 0; c < NC; ++c)
 #pragma unroll

@@ -157,11 +157,18 @@ __global__ void __launch_bounds__(PencilTile<NO, TY, S>::kThreads, 2)
 #pragma unroll
       for (int m = 0; m < 16; ++m) {
         const float dr = base2 + pz2[m];
-        const float inv = __fdividef(a.norm, fmaf(dr, dr, di * di));
-        v[m] = cmul(v[m], make_float2(dr * inv, -di * inv));
+        if (a.pstd) {
+          v[m] = make_float2(-dr * a.norm * v[m].x, -dr * a.norm * v[m].y);  // PSTD Laplacian (k02e = 0)
+        } else {
+          const float inv = __fdividef(a.norm, fmaf(dr, dr, di * di));
+          v[m] = cmul(v[m], make_float2(dr * inv, -di * inv));
+        }
       }
       refill();
       fast::line_fft<NO, true>(v, L, p, a.po.tw, fast::SyncBlock{});
+      if (a.pstd)
+#pragma unroll
+        for (int m = 0; m < 16; ++m) v[m].y = -v[m].y;
       // thread (p, yl) wrote back exactly the elements it read last
 #pragma unroll
       for (int m = 0; m < 16; ++m) buf[(p + P * m) * TY + yl] = v[m];
