@@ -132,7 +132,9 @@ def measured_peaks():
 
 def profile_traffic(kernel):
     """DRAM bytes per launch of `kernel` on this workload from the committed ncu
-    summary (profiles/*.md, line 'dram_bytes_per_launch[<kernel>]: N')."""
+    summary (profiles/*.md, line 'dram_bytes_per_launch[<kernel>]: N'; the
+    256^3 workload's kernels are keyed K1/K2/K3, other workloads prefix their
+    config, e.g. c4:K3)."""
     pdir = os.path.join(ROOT, "profiles")
     if not os.path.isdir(pdir):
         return None
@@ -336,7 +338,8 @@ def run_ours(args):
             "kernels": kern,
             "roofline": {"bound": "hbm", "kernel": dom["kernel"], "achieved": dom["achieved_gbs"], "peak": peak,
                          "peak_kind": peak_kind, "unit": "GB/s", "frac": dom["achieved_gbs"] / peak,
-                         "traffic": profile_traffic(dom["kernel"]),
+                         "traffic": profile_traffic(dom["kernel"] if args.config == "c3"
+                                                    else "%s:%s" % (args.config, dom["kernel"])),
                          "algorithmic_bytes_per_launch": dom["algorithmic_bytes"]},
             "plain_vs_warm_start_batched": dict(legs, plain_ms_per_solve=value),
             "e2e": e2e, "gpu_launches": launches_per_solve * args.steps, "cpu_baseline": cpu,
