@@ -17,23 +17,27 @@ def rel(a, b):
     return float(np.linalg.norm(np.ravel(a) - np.ravel(b)) / np.linalg.norm(np.ravel(b)))
 
 
-def run_product(n, opt, val, pos, vector, path):
+def run_product(n, opt, val, pos, vector, path, env=None):
     import wavesim_b200 as ws
-    old = os.environ.get("WAVESIM_B200_PATH")
+    env = dict(env or {})
+    env["WAVESIM_B200_PATH"] = "generic" if path == "generic" else None
+    old = {k: os.environ.get(k) for k in env}
     try:
-        if path == "generic":
-            os.environ["WAVESIM_B200_PATH"] = "generic"
-        else:
-            os.environ.pop("WAVESIM_B200_PATH", None)
+        for k, v in env.items():
+            if v is None:
+                os.environ.pop(k, None)
+            else:
+                os.environ[k] = v
         sim = (ws.WaveSimVector if vector else ws.WaveSim)(n, opt)
         E, st = sim.exec(ws.Source(val, pos))
         sim.close()
         return E, st
     finally:
-        if old is None:
-            os.environ.pop("WAVESIM_B200_PATH", None)
-        else:
-            os.environ["WAVESIM_B200_PATH"] = old
+        for k, v in old.items():
+            if v is None:
+                os.environ.pop(k, None)
+            else:
+                os.environ[k] = v
 
 
 CASES = {
@@ -51,12 +55,18 @@ CASES = {
     "3d_pencil_192": ((16, 16, 160), [8, 8, 16], 16, False),
     "3d_pencil_192_vector": ((16, 16, 160), [8, 8, 16], 16, True),
     "3d_128_vector": ((96, 96, 96), [16, 16, 16], 8, True),
+    # layout variants the autotuner may choose
+    "3d_256_cluster16": ((224, 224, 16), [16, 16, 8], 16, False, {"WAVESIM_B200_CLUSTER": "16"}),
+    "3d_pencil_192_vector_ty8": ((16, 16, 160), [8, 8, 16], 16, True, {"WAVESIM_B200_PENCIL_TY": "8"}),
+    "3d_256_pencil_tma": ((16, 16, 224), [8, 8, 16], 16, False),
+    "3d_256_pencil_plain": ((16, 16, 224), [8, 8, 16], 16, False, {"WAVESIM_B200_K2": "plain"}),
 }
 
 
 @pytest.mark.parametrize("name", list(CASES))
 def test_fast_matches_generic_and_oracle(gpu, name):
-    shape, bw, iters, vector = CASES[name]
+    shape, bw, iters, vector = CASES[name][:4]
+    env = CASES[name][4] if len(CASES[name]) > 4 else None
     rng = np.random.default_rng(7)
     n = 1.2 + 0.2 * rng.random(shape) + 0.005j
     opt = {"lambda": 1.0, "pixel_size": 0.25, "boundary_widths": bw, "energy_threshold": 1e-99,
@@ -65,7 +75,7 @@ def test_fast_matches_generic_and_oracle(gpu, name):
         opt.update(pixel_size=0.125)
     val = rng.standard_normal(shape[:2]) + 1j * rng.standard_normal(shape[:2])
     pos = [1] * len(shape) + ([2] if vector else [])
-    Ef, sf = run_product(n, opt, val, pos, vector, "fast")
+    Ef, sf = run_product(n, opt, val, pos, vector, "fast", env)
     Eg, sg = run_product(n, opt, val, pos, vector, "generic")
     sim = (ref.WaveSimVector if vector else ref.WaveSim)(n, opt)
     Eo, so = sim.exec(ref.Source(val, pos), max_iterations=iters)

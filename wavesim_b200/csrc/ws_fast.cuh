@@ -183,15 +183,18 @@ struct PlaneGeom {
   static constexpr int LR = N / C;             // rows held in the x phase (C > 1)
   // transposed tile: row kyl of column x at x * CS2 + kyl + 2 (kyl / 16); CS2
   // even, so that element pairs (kyl even) are 16-byte aligned
-  static constexpr int CS2 = LR + 2 * (LR / 16) + 2;
+  static constexpr int CS2 = LR + 2 * (LR / 16) + (LR >= 32 ? 2 : 0);
   static constexpr int P = N / 16;
   static constexpr int LPR = kThreads / P;     // lines per round
+  // K1's column scratch: one round of lines, plus a slot for idle lanes when
+  // the block's columns are not a whole number of rounds
+  static constexpr int SCR = (DO_X && M % LPR == 0) ? LPR : LPR + 1;
   static constexpr size_t smem_a = (size_t)(M + 1) * CS * sizeof(float2);  // + scratch column
   static constexpr size_t smem_b = (size_t)N * CS2 * sizeof(float2);
   // K1 with a cluster: one round of column scratch + the received rows
   static constexpr bool PUSH = C > 1 && DO_X;
   // (+ 16 bytes: the received tile starts on a 16-byte boundary for the pair pushes)
-  static constexpr size_t smem_push = (size_t)(LPR + 1) * CS * sizeof(float2) + 16 + smem_b;
+  static constexpr size_t smem_push = (size_t)SCR * CS * sizeof(float2) + 16 + smem_b;
   static constexpr size_t smem_max_ab = smem_a > smem_b ? smem_a : smem_b;
   static constexpr size_t smem = PUSH ? (smem_push > smem_max_ab ? smem_push : smem_max_ab) : smem_a;
   static_assert(kThreads % P == 0 || P > kThreads, "threads per line");
@@ -252,7 +255,7 @@ __global__ void __launch_bounds__(kThreads, 3)
   constexpr bool PUSH = G::PUSH;
   // PUSH: [one round of column scratch, LPR + 1 columns][rows received from the cluster]
   float2* const smB =
-      PUSH ? reinterpret_cast<float2*>((reinterpret_cast<uintptr_t>(sm + (LPR + 1) * G::CS) + 15) & ~(uintptr_t)15) : sm;
+      PUSH ? reinterpret_cast<float2*>((reinterpret_cast<uintptr_t>(sm + G::SCR * G::CS) + 15) & ~(uintptr_t)15) : sm;
   __shared__ __align__(8) uint64_t recv_bar;
   if constexpr (PUSH) {
     if (tid == 0) mbar_init_expect(&recv_bar, (uint32_t)(G::LR * N * sizeof(float2)));
@@ -420,7 +423,7 @@ __global__ void __launch_bounds__(TY*(NO / 16) < 1024 ? TY*(NO / 16) : 1024, 3)
 // K3
 // ----------------------------------------------------------------------------
 template <int N, int C, bool DO_X>
-__global__ void __launch_bounds__(kThreads, 2)
+__global__ void __launch_bounds__(kThreads, C >= 16 ? 3 : 2)
     kf_plane_inv(InnerArgs a, const float2* __restrict__ T, float2* __restrict__ dE, float2* __restrict__ E,
                  const float2* __restrict__ gamma, const DevState* __restrict__ st, double* __restrict__ partials) {
   using G = PlaneGeom<N, C, DO_X>;

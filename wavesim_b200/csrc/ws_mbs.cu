@@ -119,6 +119,7 @@ static FastPencil mixed_pencil() {
 static const std::vector<FastInner>& fast_inner_table() {
   static const std::vector<FastInner> t = {
       fast_inner<64, 1, true>(),     fast_inner<128, 2, true>(),    fast_inner<256, 8, true>(),
+      fast_inner<256, 16, true>(),
       fast_inner<64, 1, false>(),    fast_inner<128, 1, false>(),   fast_inner<256, 1, false>(),
       fast_inner<512, 1, false>(),   fast_inner<1024, 1, false>(),  fast_inner<2048, 1, false>(),
       mixed_inner<Plan192, 6>()};
@@ -147,6 +148,7 @@ static const std::vector<FastPencil>& fast_pencil_table() {
   static const std::vector<FastPencil> t = {
       fast_pencil<32, 16>(),  fast_pencil<64, 16>(),  fast_pencil<128, 16>(),
       fast_pencil<256, 16>(), fast_pencil<512, 8>(),  fast_pencil<1024, 4>(),
+      mixed_pencil<Plan192, 8, 3>(),   // (a TY = 8 variant first: the later TY = 16 is the default)
       mixed_pencil<Plan192, 16, 1>(),
       mixed_pencil<Plan192, 16, 3>(),
       mixed_pencil<mixed::Plan<64, 16, 16, 4>, 16, 3>(),
@@ -258,11 +260,22 @@ static int make_layout(const Geom& g, Layout& L, std::string& why, const LayoutC
   // fast power-of-two kernels where a shape matches
   const char* path = std::getenv("WAVESIM_B200_PATH");
   if (path && std::strcmp(path, "generic") == 0) return WS_OK;
+  // 3-D: the first plane kernel of the grid's size, or the one with the
+  // cluster size asked for (autotuner: ch.csize; WAVESIM_B200_CLUSTER)
+  int want_c = ch.csize;
+  if (!want_c)
+    if (const char* e = std::getenv("WAVESIM_B200_CLUSTER")) want_c = std::atoi(e);
+  const FastInner* first3 = nullptr;
+  const FastInner* pick3 = nullptr;
   for (const FastInner& f : fast_inner_table()) {
     if (ch.inner == 2) break;
-    if (L.mode3d && f.do_x && g.ny == f.n && g.nx == f.n) L.fi = &f;
+    if (L.mode3d && f.do_x && g.ny == f.n && g.nx == f.n) {
+      if (!first3) first3 = &f;
+      if (want_c && f.c == want_c) pick3 = &f;
+    }
     if (!L.mode3d && !f.do_x && g.ny == f.n) L.fi = &f;
   }
+  if (L.mode3d) L.fi = pick3 ? pick3 : first3;
   if (L.fi && !L.mode3d) {
     // one round of lines per block: 256 threads, 16 elements each
     const long long total_cols = (long long)g.nx * g.nc;
@@ -272,8 +285,14 @@ static int make_layout(const Geom& g, Layout& L, std::string& why, const LayoutC
   }
   if (L.fi && L.mode3d) L.grid_inner = (long long)g.nz * g.nc * L.fi->c;
   if (ch.outer != 2) {
+    // the last pencil of the shape, or the one with the y tile asked for
+    // (autotuner: outer = 1 with ty; WAVESIM_B200_PENCIL_TY)
+    int want_ty = ch.outer == 1 ? ch.ty : 0;
+    if (!want_ty)
+      if (const char* e = std::getenv("WAVESIM_B200_PENCIL_TY")) want_ty = std::atoi(e);
     for (const FastPencil& f : fast_pencil_table())
-      if (f.no == no && g.ny % f.ty == 0 && f.nc == g.nc && (L.mode3d || !f.only3d)) L.fp = &f;
+      if (f.no == no && g.ny % f.ty == 0 && f.nc == g.nc && (L.mode3d || !f.only3d) && (!want_ty || f.ty == want_ty))
+        L.fp = &f;
   }
   if (L.fp) L.grid_outer = (long long)(g.ny / L.fp->ty) * mids;  // blocks of the fast pencil kernel
   // the TMA pencil where a shape matches: by default (WAVESIM_B200_K2=plain keeps kf_pencil), or the
@@ -1511,10 +1530,13 @@ int ws_solver_autotune(ws_solver h, int n_iterations, int* n_tried, float* ms_be
   std::vector<LayoutChoice> inner_c, outer_c;
   inner_c.push_back(LayoutChoice{1, 0, 0, 0, 0});
   inner_c.push_back(LayoutChoice{2, 0, 0, 0, 0});
+  if (base.mode3d)
+    for (int c : {8, 16}) inner_c.push_back(LayoutChoice{1, 0, c, 0, 0});  // fast planes on other cluster sizes
   if (!base.mode3d)
     for (int f : {4, 2, -2})
       inner_c.push_back(LayoutChoice{2, 0, 0, f > 0 ? std::max(1, base.ncols / f) : base.ncols * 2, 0});
   outer_c.push_back(LayoutChoice{0, 1, 0, 0, 0});
+  outer_c.push_back(LayoutChoice{0, 1, 0, 0, 8});  // fast pencil with 8 y per block, where one exists
   for (int k : {2, 3}) outer_c.push_back(LayoutChoice{0, 3 + k, 0, 0, 0});
   for (int t : {1, 2, 4, 8, 16}) outer_c.push_back(LayoutChoice{0, 2, 0, 0, t});
   int tried = 0;
