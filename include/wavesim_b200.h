@@ -237,6 +237,12 @@ int ws_solver_time_kernels(ws_solver s, int n_iterations, float ms_out[3], doubl
 /* Number of kernel launches one iteration makes. */
 int ws_solver_launches_per_iteration(ws_solver s);
 
+/* Where the loop fuses K3 of an iteration with K1 of the next (3-D fast
+ * planes on a cluster), the mean CUDA-event time of that kernel and its
+ * algorithmic bytes per launch (K3's plus the write of T); otherwise
+ * WS_ERR_UNSUPPORTED. */
+int ws_solver_time_fused(ws_solver s, int n_iterations, float* ms_out, double* bytes_out);
+
 /* After a warm-started solve of right-hand side `rhs`: the ROI energy of the
  * cold first increment (diff_energy(1), from the probe iteration), the ROI
  * energy of the true increment at the end of the warm first wiggle cycle,

@@ -1,0 +1,88 @@
+"""The fused loop (K3 of each iteration and K1 of the next in one kernel, on
+3-D planes split over a cluster) against the three separate kernels
+(WAVESIM_B200_FUSE=0).  The fused kernel does the same arithmetic in the same
+order, so the fields must agree bit for bit: cold, warm, batched, with the
+host loop and with the CUDA graph."""
+import os
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def solve(fuse, fn):
+    import wavesim_b200 as ws
+    old = os.environ.get("WAVESIM_B200_FUSE")
+    try:
+        if fuse:
+            os.environ.pop("WAVESIM_B200_FUSE", None)
+        else:
+            os.environ["WAVESIM_B200_FUSE"] = "0"
+        return fn(ws)
+    finally:
+        if old is None:
+            os.environ.pop("WAVESIM_B200_FUSE", None)
+        else:
+            os.environ["WAVESIM_B200_FUSE"] = old
+
+
+def medium(shape, seed=3):
+    rng = np.random.default_rng(seed)
+    return 1.3 + 0.15 * rng.random(shape) + 0.002j
+
+
+CASES = {
+    "128_cluster2": ((96, 96, 96), [16, 16, 16]),
+    "256_cluster8": ((224, 224, 16), [16, 16, 8]),
+}
+
+
+@pytest.mark.parametrize("name", list(CASES))
+@pytest.mark.parametrize("use_graph", [True, False])
+def test_fused_loop_is_bit_identical(gpu, name, use_graph):
+    shape, bw = CASES[name]
+    n = medium(shape)
+    opt = {"lambda": 1.0, "pixel_size": 0.25, "boundary_widths": bw, "energy_threshold": 1e-3,
+           "max_iterations": 48, "use_graph": use_graph}
+    val = np.ones(shape[:2]) + 0.3j
+
+    def run(ws):
+        sim = ws.WaveSim(n, opt)
+        from wavesim_b200 import _lib
+        fused = _lib.lib.ws_solver_launches_per_iteration(sim.solver()) == 3
+        E, st = sim.exec(ws.Source(val, [1, 1, 1]))
+        sim.close()
+        return E, st, fused
+
+    Ef, sf, fused = solve(True, run)
+    Eu, su, unfused = solve(False, run)
+    assert fused and not unfused
+    assert sf.it == su.it
+    np.testing.assert_array_equal(sf.diff_energy, su.diff_energy)
+    np.testing.assert_array_equal(Ef, Eu)
+
+
+def test_fused_warm_and_batched(gpu):
+    shape, bw = CASES["128_cluster2"]
+    n = medium(shape, 5)
+    opt = {"lambda": 1.0, "pixel_size": 0.25, "boundary_widths": bw, "energy_threshold": 1e-3,
+           "max_iterations": 64}
+    rng = np.random.default_rng(9)
+    start = (rng.standard_normal(shape) + 1j * rng.standard_normal(shape)).astype(np.complex64) * 0.05
+
+    def run(ws):
+        sim = ws.WaveSim(n, opt)
+        src = ws.Source(np.ones(shape[:2]), [1, 1, 1])
+        Ew, sw = sim.exec(src, warm_start=start)
+        Eb, sb = sim.exec_batch([src, ws.Source(np.ones((8, 8)), [40, 40, 30])])
+        sim.close()
+        return Ew, sw, Eb, sb
+
+    Ewf, swf, Ebf, sbf = solve(True, run)
+    Ewu, swu, Ebu, sbu = solve(False, run)
+    assert swf.it == swu.it and swf.warm_discarded == swu.warm_discarded
+    np.testing.assert_array_equal(Ewf, Ewu)
+    for a, b in zip(Ebf, Ebu):
+        np.testing.assert_array_equal(a, b)
+    assert [s.it for s in sbf] == [s.it for s in sbu]

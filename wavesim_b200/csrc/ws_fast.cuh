@@ -606,5 +606,195 @@ __global__ void __launch_bounds__(kThreads, C >= 16 ? 3 : 2)
   }
 }
 
+
+// ----------------------------------------------------------------------------
+// K3 of iteration k fused with K1 of iteration k + 1 (3-D planes on a cluster)
+// ----------------------------------------------------------------------------
+// The new increment dE'_k of a column, which K3's epilogue holds in registers
+// as v[m] = dE'(y = p + P m), is exactly the input K1 of the next iteration
+// loads for that column.  So after the epilogue the block adds the source of
+// iteration k + 1 (if any), applies the next wiggle's ramps and runs the y
+// transform in place in the column tile; the cluster then exchanges rows by
+// pulling (two cluster barriers), and each block transforms its rows along x
+// and writes them to T: the very slab it read at the start.  dE' is not read
+// again, so an iteration moves 64 instead of 72 bytes per point, and the
+// K1 launch disappears from the loop.
+template <int N, int C>
+__global__ void __launch_bounds__(kThreads, 2)
+    kf_plane_fused(InnerArgs a, Wig w1, const float2* __restrict__ src1, float2 A, float2* __restrict__ T,
+                   float2* __restrict__ dE, float2* __restrict__ E, const float2* __restrict__ gamma,
+                   const DevState* __restrict__ st, double* __restrict__ partials) {
+  static_assert(C > 1, "cluster planes only");
+  using G = PlaneGeom<N, C, true>;
+  constexpr int P = G::P, LPR = G::LPR, M = G::M, LR = G::LR;
+  constexpr int RPR = kThreads / P;
+  const int rhs = blockIdx.x / a.bpr, bid = blockIdx.x - rhs * a.bpr;
+  st += rhs;
+  if (load_done(st)) return;  // the same for every block of a cluster
+  const bool acc_now = !a.acc2 || (__ldcg(&st->it) & 1) == 0;
+  T += rhs * a.fstride;
+  dE += rhs * a.fstride;
+  E += rhs * a.fstride;
+  if (src1) src1 += rhs * a.fstride;
+  partials += (long long)rhs * a.bpr;
+  extern __shared__ float2 sm[];
+  __shared__ float red[kThreads / 32];
+  const int tid = threadIdx.x;
+  const Geom& g = a.g;
+  const int nx = g.nx;
+  const int rank = (int)(bid % C), plane = bid / C;
+  const int x0 = rank * M, z = plane % g.nz, comp = plane / g.nz;
+  const long long colbase = (long long)plane * nx + x0;
+  float2* __restrict__ slab = T + (long long)plane * nx * N + rank * LR;  // rows [rank LR, +LR) of the plane
+  if (tid == 0) {
+    const unsigned bytes = (unsigned)M * N * sizeof(float2);
+    prefetch_l2(dE + colbase * N, bytes);
+    if (acc_now) prefetch_l2(E + colbase * N, bytes);
+    prefetch_l2(gamma + colbase * N - (long long)comp * g.npts, bytes);
+    if (src1) prefetch_l2(src1 + colbase * N, bytes);
+  }
+  cg::cluster_group cl = cg::this_cluster();
+  // K3: inverse x transform of the block's rows
+  for (int r0 = 0; r0 < LR; r0 += RPR) {
+    const int rl = r0 + tid % RPR, p = tid / RPR;
+    float2 v[16];
+#pragma unroll
+    for (int r = 0; r < 16; ++r) v[r] = slab[(long long)(p + P * r) * N + rl];
+    RowLine L{sm + rl + (rl >> 4), G::CS2};
+    line_fft<N, true>(v, L, p, a.twx, SyncBlock{});
+#pragma unroll
+    for (int m = 0; m < 16; ++m) L.at(p + P * m) = v[m];
+  }
+  {
+    constexpr int PER = M * N / kThreads;
+    float2 hold[PER];
+    cl.sync();
+#pragma unroll
+    for (int i = 0; i < PER; ++i) {
+      const int e = tid + kThreads * i;
+      const int ky = e % N, c = e / N;
+      const float2* rs = cl.map_shared_rank(sm, ky / LR);
+      const int kyl = ky % LR;
+      hold[i] = rs[(x0 + c) * G::CS2 + kyl + (kyl >> 4)];
+    }
+    cl.sync();
+#pragma unroll
+    for (int i = 0; i < PER; ++i) {
+      const int e = tid + kThreads * i;
+      const int ky = e % N, c = e / N;
+      sm[c * G::CS + ky + (ky >> 4)] = hold[i];
+    }
+  }
+  __syncthreads();
+  const float2 gzz = a.w.gz[z];
+  const float2 gzz1 = w1.gz[z];
+  float esum = 0.f;
+  for (int c0 = 0; c0 < M; c0 += LPR) {
+    const int cc = c0 + tid / P, p = tid % P;
+    float2 v[16];
+    ColLine L{sm + cc * G::CS};
+#pragma unroll
+    for (int r = 0; r < 16; ++r) v[r] = L.at(p + P * r);
+    if constexpr (P <= 32) {
+      line_fft<N, true>(v, L, p, a.py.tw, SyncWarp{});
+    } else {
+      line_fft<N, true>(v, L, p, a.py.tw, SyncBlock{});
+    }
+    const int x = x0 + cc;
+    const long long col = colbase + cc;
+    const float2 gxz = cmul(a.w.gx[x], gzz);
+    const bool in_xzc = x >= g.r0[1] && x < g.r1[1] && z >= g.r0[2] && z < g.r1[2] && comp >= g.r0[3] && comp < g.r1[3];
+    const long long gcol = col * N;
+    const float2* __restrict__ gmc = gamma + (gcol - (long long)comp * g.npts);
+    float2* __restrict__ dEc = dE + gcol;
+    float2* __restrict__ Ec = E + gcol;
+    // K3's epilogue (unwiggle, f_mix, E' += dE', ROI energy); v[m] becomes dE'_k(y)
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      float2 gm[8], d0[8], e0[8];
+#pragma unroll
+      for (int i = 0; i < 8; ++i) {
+        const int y = p + P * (8 * h + i);
+        gm[i] = gmc[y];
+        d0[i] = dEc[y];
+        e0[i] = acc_now ? Ec[y] : make_float2(0.f, 0.f);
+      }
+#pragma unroll
+      for (int i = 0; i < 8; ++i) {
+        const int m = 8 * h + i;
+        const int y = p + P * m;
+        const float2 ep = cmul_conj(cmul_conj(v[m], gxz), a.w.gy[y]);
+        const float2 one_m = make_float2(1.f - kAlpha * gm[i].x, -kAlpha * gm[i].y);
+        const float2 t = cmul(cmul(gm[i], gm[i]), ep);
+        const float2 dn = cadd(cmul(one_m, d0[i]), make_float2(kAlpha * t.y, -kAlpha * t.x));
+        dEc[y] = dn;
+        if (acc_now) Ec[y] = cadd(e0[i], a.acc2 ? cadd(d0[i], dn) : dn);
+        if (in_xzc && y >= g.r0[0] && y < g.r1[0]) esum = fmaf(dn.x, dn.x, fmaf(dn.y, dn.y, esum));
+        v[m] = dn;
+      }
+    }
+    // K1 of iteration k + 1 on the same column: source, next ramps, y transform
+    const float2 gxz1 = cmul(w1.gx[x], gzz1);
+    const float2* __restrict__ sr = src1 ? src1 + gcol : nullptr;
+#pragma unroll
+    for (int m = 0; m < 16; ++m) {
+      const int y = p + P * m;
+      float2 e = v[m];
+      if (sr) e = cadd(e, cmul(A, sr[y]));
+      v[m] = cmul(cmul(e, gxz1), w1.gy[y]);
+    }
+    if constexpr (P <= 32) {
+      line_fft<N, false>(v, L, p, a.py.tw, SyncWarp{});
+    } else {
+      line_fft<N, false>(v, L, p, a.py.tw, SyncBlock{});
+    }
+#pragma unroll
+    for (int m = 0; m < 16; ++m) L.at(p + P * m) = v[m];
+  }
+  // the ROI energy of dE'_k
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) esum += __shfl_xor_sync(0xffffffffu, esum, o);
+  if ((tid & 31) == 0) red[tid >> 5] = esum;
+  // rows [rank LR, +LR) of all N transformed columns, from the blocks holding them
+  {
+    constexpr int PER = LR * N / kThreads;
+    float2 hold[PER];
+    cl.sync();
+#pragma unroll
+    for (int i = 0; i < PER; ++i) {
+      const int e = tid + kThreads * i;
+      const int kyl = e % LR, x = e / LR;
+      const int ky = rank * LR + kyl;
+      const float2* rs = cl.map_shared_rank(sm, x / M);
+      hold[i] = rs[(x % M) * G::CS + ky + (ky >> 4)];
+    }
+    cl.sync();
+#pragma unroll
+    for (int i = 0; i < PER; ++i) {
+      const int e = tid + kThreads * i;
+      const int kyl = e % LR, x = e / LR;
+      sm[x * G::CS2 + kyl + (kyl >> 4)] = hold[i];
+    }
+  }
+  __syncthreads();
+  if (tid < 32) {
+    float v = tid < kThreads / 32 ? red[tid] : 0.f;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    if (tid == 0) partials[bid] = (double)v;
+  }
+  // K1's x transform of the block's rows, written over the slab K3 read
+  for (int r0 = 0; r0 < LR; r0 += RPR) {
+    const int rl = r0 + tid % RPR, p = tid / RPR;
+    RowLine L{sm + rl + (rl >> 4), G::CS2};
+    float2 v[16];
+#pragma unroll
+    for (int r = 0; r < 16; ++r) v[r] = L.at(p + P * r);
+    line_fft<N, false>(v, L, p, a.twx, SyncBlock{});
+#pragma unroll
+    for (int m = 0; m < 16; ++m) slab[(long long)(p + P * m) * N + rl] = v[m];
+  }
+}
+
 }  // namespace fast
 }  // namespace ws

@@ -80,6 +80,7 @@ struct FastInner {
   const void* inv;
   size_t smem;      // bytes (3-D, enough for both kernels); 2-D: bytes per held column, one extra column of scratch
   size_t smem_fwd, smem_inv;  // 3-D: what each kernel needs
+  const void* fused = nullptr;  // K3 of one iteration + K1 of the next (3-D planes on a cluster), or null
 };
 struct FastPencil {
   int no, ty;
@@ -93,9 +94,11 @@ struct FastPencil {
 template <int N, int C, bool DX>
 static FastInner fast_inner() {
   using G = fast::PlaneGeom<N, C, DX>;
-  return FastInner{N, C, DX ? 1 : 0, (const void*)fast::kf_plane_fwd<N, C, DX>,
-                   (const void*)fast::kf_plane_inv<N, C, DX>, DX ? G::smem : (size_t)G::CS * sizeof(float2),
-                   DX ? (G::PUSH ? G::smem_push : G::smem_a) : 0, DX ? G::smem_max_ab : 0};
+  FastInner f{N, C, DX ? 1 : 0, (const void*)fast::kf_plane_fwd<N, C, DX>,
+              (const void*)fast::kf_plane_inv<N, C, DX>, DX ? G::smem : (size_t)G::CS * sizeof(float2),
+              DX ? (G::PUSH ? G::smem_push : G::smem_a) : 0, DX ? G::smem_max_ab : 0};
+  if constexpr (DX && C > 1) f.fused = (const void*)fast::kf_plane_fused<N, C>;
+  return f;
 }
 template <int NO, int TY>
 static FastPencil fast_pencil() {
@@ -360,6 +363,7 @@ struct Solver {
   int pf_inner = 0, pf_outer = 0;  // L2 prefetch distance of the fast kernels, in blocks (0: off)
   bool warm = false;             // the current solve starts from d_init
   int pstd = 0;                  // a PSTD stepper's solver: K2 applies the Laplacian (see ws_pstd_*)
+  int fuse = 0;                  // the loop runs K3 of each iteration fused with K1 of the next
   LayoutChoice tuned{};          // the autotuner's choice (all zero: the heuristics)
   double warm_ratio = 0.0;       // discard threshold of the current solve
   float2* d_tw = nullptr;
@@ -376,6 +380,16 @@ static void free_graph(Solver* s) {
   if (s->graph) cudaGraphDestroy(s->graph);
   s->gexec = nullptr;
   s->graph = nullptr;
+}
+
+// The fused K3 + K1 step is used where the layout has one (3-D fast planes on
+// a cluster); WAVESIM_B200_FUSE=0 keeps the three kernels separate.
+static void update_fuse(Solver* s) {
+  const char* e = std::getenv("WAVESIM_B200_FUSE");
+  const int f = (s->lay.fi && s->lay.fi->fused && s->lay.mode3d && !s->pstd && !(e && std::strcmp(e, "0") == 0))
+                    ? 1 : 0;
+  if (f != s->fuse) free_graph(s);
+  s->fuse = f;
 }
 
 static void destroy_solver(Solver* s) {
@@ -445,6 +459,10 @@ static int set_kernel_attributes() {
     WS_CUDA(allow_dynamic_smem(f.inv, optin));
     WS_CUDA(cudaFuncSetAttribute(f.fwd, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
     WS_CUDA(cudaFuncSetAttribute(f.inv, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
+    if (f.fused) {
+      WS_CUDA(allow_dynamic_smem(f.fused, optin));
+      WS_CUDA(cudaFuncSetAttribute(f.fused, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
+    }
   }
   for (const FastPencil& f : fast_pencil_table()) WS_CUDA(allow_dynamic_smem(f.fn, optin));
   for (const TmaPencil& f : tma_pencil_table()) WS_CUDA(allow_dynamic_smem(f.fn, optin));
@@ -549,6 +567,7 @@ static int create_solver(const int64_t N[4], const ws_complex* gamma, int64_t n_
     destroy_solver(s);
     return fail(rc, why);
   }
+  update_fuse(s);
   {
     // L2 prefetch distance of the fast kernels: about one wave of resident
     // blocks (2 per SM), a whole number of clusters.  WAVESIM_B200_PREFETCH
@@ -882,6 +901,54 @@ static cudaError_t launch_k3(const Solver* s, int w, const StopRule& rule, const
 }
 
 static cudaError_t launch_iteration(const Solver* s, int it0, bool with_source, const StopRule& rule,
+                                    const Hist& h);
+
+// K3 of the iteration with wiggle w fused with K1 of the next (wiggle w1,
+// with the source when that iteration is one of the first Nw)
+static cudaError_t launch_k3k1(const Solver* s, int w, int w1, bool src_next) {
+  InnerArgs a = inner_args(s, w);
+  a.ncols = s->lay.ncols;
+  Wig W1 = s->wig[w1];
+  const float2* src1 = src_next ? s->d_src : nullptr;
+  float2 A = make_float2(0.f, (float)(1.0f / s->eps / (float)s->nw));
+  float2* T = s->d_T;
+  float2* dE = s->d_dE;
+  float2* E = s->d_E;
+  const float2* gamma = s->d_gamma;
+  const DevState* st = s->d_state;
+  double* partials = s->d_partials;
+  void* args[] = {&a, &W1, &src1, &A, &T, &dE, &E, &gamma, &st, &partials};
+  cudaLaunchConfig_t cfg{};
+  cfg.gridDim = dim3((unsigned)(s->lay.grid_inner * s->nrhs));
+  cfg.blockDim = dim3(fast::kThreads);
+  cfg.dynamicSmemBytes = s->lay.fi->smem_inv;
+  cfg.stream = s->stream;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeClusterDimension;
+  attr[0].val.clusterDim.x = s->lay.fi->c;
+  attr[0].val.clusterDim.y = 1;
+  attr[0].val.clusterDim.z = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelExC(&cfg, s->lay.fi->fused, args);
+}
+
+// One iteration of the fused loop: T already holds K1's output for it.
+static cudaError_t launch_iteration_fused(const Solver* s, int i, bool src_next, const StopRule& rule,
+                                          const Hist& h) {
+  const int w = i % s->nw, w1 = (i + 1) % s->nw;
+  cudaError_t e = launch_k2(s, w);
+  if (e != cudaSuccess) return e;
+  if ((e = launch_k3k1(s, w, w1, src_next)) != cudaSuccess) return e;
+  return launch_finish(s, rule, h);
+}
+
+// A steady iteration (no source) of the loop, fused or not.
+static cudaError_t launch_steady(const Solver* s, int i, const StopRule& rule, const Hist& h) {
+  return s->fuse ? launch_iteration_fused(s, i, false, rule, h) : launch_iteration(s, i, false, rule, h);
+}
+
+static cudaError_t launch_iteration(const Solver* s, int it0, bool with_source, const StopRule& rule,
                                     const Hist& h) {
   const int w = it0 % s->nw;
   cudaError_t e = launch_k1(s, w, with_source);
@@ -923,14 +990,24 @@ static cudaError_t launch_prologue(const Solver* s, const StopRule& rule, const 
     k_warm_restart<<<1, 256, 0, s->stream>>>(s->d_state, s->nrhs);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
   }
-  for (int i = 0; i < s->nw; ++i)
-    if ((e = launch_iteration(s, i, true, rule, h)) != cudaSuccess) return e;
+  if (s->fuse) {
+    // K1 of the first iteration, then each fused step also computes K1 of the
+    // next iteration (with the source while that one is among the first Nw)
+    if ((e = launch_k1(s, 0, true)) != cudaSuccess) return e;
+    for (int i = 0; i < s->nw; ++i)
+      if ((e = launch_iteration_fused(s, i, i + 1 < s->nw, rule, h)) != cudaSuccess) return e;
+  } else {
+    for (int i = 0; i < s->nw; ++i)
+      if ((e = launch_iteration(s, i, true, rule, h)) != cudaSuccess) return e;
+  }
   if (s->warm) {
     const long long fe = (long long)field_elems(s);
     const unsigned bpr = (unsigned)std::max<long long>(1, std::min<long long>((fe + 255) / 256, 4 * kNumSms));
     k_warm_shift<<<dim3(bpr, s->nrhs), 256, 0, s->stream>>>(s->d_dE, s->d_init, s->g, fe, s->d_state);
     k_warm_check<<<1, 256, 0, s->stream>>>(s->d_state, s->nrhs, s->warm_ratio);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    // the shift changed dE': the fused loop's T is recomputed from it
+    if (s->fuse && (e = launch_k1(s, 0, false)) != cudaSuccess) return e;
   }
   return cudaSuccess;
 }
@@ -989,7 +1066,7 @@ static int build_graph(Solver* s, const StopRule& rule, const Hist& h) {
   cudaGraph_t body = cp.conditional.phGraph_out[0];
   e = cudaStreamBeginCaptureToGraph(s->stream, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal);
   if (e == cudaSuccess) {
-    for (int i = 0; i < s->nw && e == cudaSuccess; ++i) e = launch_iteration(s, i, false, rule, h);
+    for (int i = 0; i < s->nw && e == cudaSuccess; ++i) e = launch_steady(s, i, rule, h);
     if (e == cudaSuccess) {
       k_cycle_guard<<<1, 32, 0, s->stream>>>(s->d_state, s->nrhs, cond, max_cycles);
       e = cudaGetLastError();
@@ -1187,7 +1264,7 @@ static int solve_batch(Solver* s, int nrhs, const int64_t* counts, const ws_sour
         it += s->nw;
       } else {
         for (int i = 0; i < s->nw; ++i) {
-          WS_CUDA(launch_iteration(s, (int)(it % s->nw), false, rule, h));
+          WS_CUDA(launch_steady(s, (int)(it % s->nw), rule, h));
           ++it;
         }
       }
@@ -1356,7 +1433,47 @@ int ws_solver_buffers(ws_solver h, void** E_prime, void** stream) {
   return WS_OK;
 }
 
-int ws_solver_launches_per_iteration(ws_solver h) { return h ? 4 : 0; }
+int ws_solver_launches_per_iteration(ws_solver h) {
+  if (!h) return 0;
+  return reinterpret_cast<Solver*>(h)->fuse ? 3 : 4;  // (K1,) K2, K3 or K3 + next K1, stop rule
+}
+
+int ws_solver_time_fused(ws_solver h, int n_iterations, float* ms_out, double* bytes_out) {
+  if (!h || !ms_out || n_iterations < 1) return fail(WS_ERR_INVALID_ARGUMENT, "bad argument");
+  Solver* s = reinterpret_cast<Solver*>(h);
+  if (!s->fuse) return fail(WS_ERR_UNSUPPORTED, "this solver's loop does not fuse K3 with K1");
+  WS_CUDA(cudaSetDevice(s->device));
+  const long long cap = n_iterations + 1;
+  if (s->hist_cap < cap) {
+    const int rc = ensure_hist(s, cap);
+    if (rc) return rc;
+  }
+  StopRule rule{s->nw, 1, 0, 1, (long long)1 << 62, -1.0};
+  Hist hh{s->d_hist, s->d_hist + s->hist_cap, 0, 0};  // cap 0: history untouched
+  s->nrhs = 1;
+  k_resume_state<<<1, 32, 0, s->stream>>>(s->d_state);
+  WS_CUDA(launch_k1(s, 0, false));
+  float acc = 0.f;
+  for (int i = 0; i < n_iterations; ++i) {
+    const int w = i % s->nw;
+    WS_CUDA(launch_k2(s, w));
+    WS_CUDA(cudaEventRecord(s->ev[0], s->stream));
+    WS_CUDA(launch_k3k1(s, w, (i + 1) % s->nw, false));
+    WS_CUDA(cudaEventRecord(s->ev[1], s->stream));
+    WS_CUDA(launch_finish(s, rule, hh));
+    WS_CUDA(cudaEventSynchronize(s->ev[1]));
+    float t;
+    WS_CUDA(cudaEventElapsedTime(&t, s->ev[0], s->ev[1]));
+    acc += t;
+  }
+  *ms_out = acc / n_iterations;
+  if (bytes_out) {
+    const double n = (double)s->g.npts * s->g.nc;
+    // K3's bytes (as ws_solver_time_kernels) plus the write of T for the next iteration
+    *bytes_out = (s->nw % 2 == 0 ? 40.0 : 48.0) * n + 8.0 * (double)s->g.npts;
+  }
+  return WS_OK;
+}
 
 int ws_solver_time_kernels(ws_solver h, int n_iterations, float ms_out[3], double bytes_out[3]) {
   if (!h || !ms_out || n_iterations < 1) return fail(WS_ERR_INVALID_ARGUMENT, "bad argument");
@@ -1597,6 +1714,7 @@ int ws_solver_autotune(ws_solver h, int n_iterations, int* n_tried, float* ms_be
     }
   }
   s->tuned = fin;
+  update_fuse(s);
   cleanup();
   if (n_tried) *n_tried = tried;
   if (ms_before) *ms_before = base_ms[0] + base_ms[1] + base_ms[2];
@@ -1844,6 +1962,7 @@ int ws_pstd_create(const int64_t N[3], const float* c1, const float* c2, const f
   }
   Solver* s = p->s;
   s->pstd = 1;
+  s->fuse = 0;
   p->nparts = (int)std::min<long long>(((long long)npts + 255) / 256, 8LL * kNumSms);
   cudaError_t e = cudaSuccess;
   if (e == cudaSuccess) e = cudaMalloc(&p->d_Ebuf, 2 * npts * sizeof(float2));
