@@ -11,20 +11,24 @@ import pytest
 pytestmark = pytest.mark.gpu
 
 
-def solve(fuse, fn):
+def solve(fuse, fn, env=None):
     import wavesim_b200 as ws
-    old = os.environ.get("WAVESIM_B200_FUSE")
+    env = dict(env or {})
+    env["WAVESIM_B200_FUSE"] = None if fuse else "0"
+    old = {k: os.environ.get(k) for k in env}
     try:
-        if fuse:
-            os.environ.pop("WAVESIM_B200_FUSE", None)
-        else:
-            os.environ["WAVESIM_B200_FUSE"] = "0"
+        for k, v in env.items():
+            if v is None:
+                os.environ.pop(k, None)
+            else:
+                os.environ[k] = v
         return fn(ws)
     finally:
-        if old is None:
-            os.environ.pop("WAVESIM_B200_FUSE", None)
-        else:
-            os.environ["WAVESIM_B200_FUSE"] = old
+        for k, v in old.items():
+            if v is None:
+                os.environ.pop(k, None)
+            else:
+                os.environ[k] = v
 
 
 def medium(shape, seed=3):
@@ -33,15 +37,17 @@ def medium(shape, seed=3):
 
 
 CASES = {
-    "128_cluster2": ((96, 96, 96), [16, 16, 16]),
-    "256_cluster8": ((224, 224, 16), [16, 16, 8]),
+    "128_cluster2": ((96, 96, 96), [16, 16, 16], None),
+    "256_cluster8": ((224, 224, 16), [16, 16, 8], None),
+    # 16-block clusters: K1's half of the exchange pushed (kf_plane_fused_push)
+    "256_cluster16": ((224, 224, 16), [16, 16, 8], {"WAVESIM_B200_CLUSTER": "16"}),
 }
 
 
 @pytest.mark.parametrize("name", list(CASES))
 @pytest.mark.parametrize("use_graph", [True, False])
 def test_fused_loop_is_bit_identical(gpu, name, use_graph):
-    shape, bw = CASES[name]
+    shape, bw, env = CASES[name]
     n = medium(shape)
     opt = {"lambda": 1.0, "pixel_size": 0.25, "boundary_widths": bw, "energy_threshold": 1e-3,
            "max_iterations": 48, "use_graph": use_graph}
@@ -55,8 +61,8 @@ def test_fused_loop_is_bit_identical(gpu, name, use_graph):
         sim.close()
         return E, st, fused
 
-    Ef, sf, fused = solve(True, run)
-    Eu, su, unfused = solve(False, run)
+    Ef, sf, fused = solve(True, run, env)
+    Eu, su, unfused = solve(False, run, env)
     assert fused and not unfused
     assert sf.it == su.it
     np.testing.assert_array_equal(sf.diff_energy, su.diff_energy)
@@ -64,7 +70,7 @@ def test_fused_loop_is_bit_identical(gpu, name, use_graph):
 
 
 def test_fused_warm_and_batched(gpu):
-    shape, bw = CASES["128_cluster2"]
+    shape, bw, _ = CASES["128_cluster2"]
     n = medium(shape, 5)
     opt = {"lambda": 1.0, "pixel_size": 0.25, "boundary_widths": bw, "energy_threshold": 1e-3,
            "max_iterations": 64}

@@ -796,5 +796,200 @@ __global__ void __launch_bounds__(kThreads, 2)
   }
 }
 
+
+// The same fused step with K1's half of the plane exchange pushed: each block
+// sends its transformed columns to the row owners with st.async, completion
+// counted in bytes on the receiver's mbarrier (as in kf_plane_fwd), instead of
+// two more cluster barriers, whose release would wait for the epilogue's
+// global stores.  The received rows land in the region that held K3's rows,
+// dead after K3's exchange; the column tile is separate, so the tiles must be
+// small: 256^2 planes on 16 blocks (16 columns and 16 rows each).
+template <int N, int C>
+struct FusedPushGeom {
+  using G = PlaneGeom<N, C, true>;
+  static constexpr size_t col_bytes = (size_t)G::M * G::CS * sizeof(float2);  // one round of columns
+  static constexpr size_t row_bytes = (size_t)N * G::CS2 * sizeof(float2);
+  static constexpr size_t smem = col_bytes + row_bytes;
+  static_assert(G::M == G::LPR, "one round of columns");
+  static_assert(col_bytes % 16 == 0, "the row tile starts on a 16-byte boundary");
+};
+
+template <int N, int C>
+__global__ void __launch_bounds__(kThreads, 2)
+    kf_plane_fused_push(InnerArgs a, Wig w1, const float2* __restrict__ src1, float2 A, float2* __restrict__ T,
+                        float2* __restrict__ dE, float2* __restrict__ E, const float2* __restrict__ gamma,
+                        const DevState* __restrict__ st, double* __restrict__ partials) {
+  using G = PlaneGeom<N, C, true>;
+  using F = FusedPushGeom<N, C>;
+  constexpr int P = G::P, M = G::M, LR = G::LR;
+  constexpr int RPR = kThreads / P;
+  const int rhs = blockIdx.x / a.bpr, bid = blockIdx.x - rhs * a.bpr;
+  st += rhs;
+  if (load_done(st)) return;  // the same for every block of a cluster
+  const bool acc_now = !a.acc2 || (__ldcg(&st->it) & 1) == 0;
+  T += rhs * a.fstride;
+  dE += rhs * a.fstride;
+  E += rhs * a.fstride;
+  if (src1) src1 += rhs * a.fstride;
+  partials += (long long)rhs * a.bpr;
+  extern __shared__ float2 sm[];
+  float2* const ct = sm;                                       // columns [x0, x0 + M), stride CS
+  float2* const rt = sm + F::col_bytes / sizeof(float2);       // rows: K3's, then the pushed ones; stride CS2
+  __shared__ float red[kThreads / 32];
+  __shared__ __align__(8) uint64_t recv_bar;
+  const int tid = threadIdx.x;
+  const Geom& g = a.g;
+  const int nx = g.nx;
+  const int rank = (int)(bid % C), plane = bid / C;
+  const int x0 = rank * M, z = plane % g.nz, comp = plane / g.nz;
+  const long long colbase = (long long)plane * nx + x0;
+  float2* __restrict__ slab = T + (long long)plane * nx * N + rank * LR;
+  if (tid == 0) {
+    mbar_init_expect(&recv_bar, (uint32_t)(LR * N * sizeof(float2)));
+    const unsigned bytes = (unsigned)M * N * sizeof(float2);
+    prefetch_l2(dE + colbase * N, bytes);
+    if (acc_now) prefetch_l2(E + colbase * N, bytes);
+    prefetch_l2(gamma + colbase * N - (long long)comp * g.npts, bytes);
+    if (src1) prefetch_l2(src1 + colbase * N, bytes);
+  }
+  cg::cluster_group cl = cg::this_cluster();
+  // K3: inverse x transform of the block's rows
+  for (int r0 = 0; r0 < LR; r0 += RPR) {
+    const int rl = r0 + tid % RPR, p = tid / RPR;
+    float2 v[16];
+#pragma unroll
+    for (int r = 0; r < 16; ++r) v[r] = slab[(long long)(p + P * r) * N + rl];
+    RowLine L{rt + rl + (rl >> 4), G::CS2};
+    line_fft<N, true>(v, L, p, a.twx, SyncBlock{});
+#pragma unroll
+    for (int m = 0; m < 16; ++m) L.at(p + P * m) = v[m];
+  }
+  {
+    constexpr int PER = M * N / kThreads;
+    float2 hold[PER];
+    cl.sync();  // also publishes every block's armed recv_bar
+#pragma unroll
+    for (int i = 0; i < PER; ++i) {
+      const int e = tid + kThreads * i;
+      const int ky = e % N, c = e / N;
+      const float2* rs = cl.map_shared_rank(rt, ky / LR);
+      const int kyl = ky % LR;
+      hold[i] = rs[(x0 + c) * G::CS2 + kyl + (kyl >> 4)];
+    }
+    cl.sync();  // every row tile is dead from here on: pushes may land in it
+#pragma unroll
+    for (int i = 0; i < PER; ++i) {
+      const int e = tid + kThreads * i;
+      const int ky = e % N, c = e / N;
+      ct[c * G::CS + ky + (ky >> 4)] = hold[i];
+    }
+  }
+  __syncthreads();
+  float esum = 0.f;
+  {
+    const int cc = tid / P, p = tid % P;
+    float2 v[16];
+    ColLine L{ct + cc * G::CS};
+#pragma unroll
+    for (int r = 0; r < 16; ++r) v[r] = L.at(p + P * r);
+    if constexpr (P <= 32) {
+      line_fft<N, true>(v, L, p, a.py.tw, SyncWarp{});
+    } else {
+      line_fft<N, true>(v, L, p, a.py.tw, SyncBlock{});
+    }
+    const int x = x0 + cc;
+    const long long col = colbase + cc;
+    const float2 gxz = cmul(a.w.gx[x], a.w.gz[z]);
+    const bool in_xzc = x >= g.r0[1] && x < g.r1[1] && z >= g.r0[2] && z < g.r1[2] && comp >= g.r0[3] && comp < g.r1[3];
+    const long long gcol = col * N;
+    const float2* __restrict__ gmc = gamma + (gcol - (long long)comp * g.npts);
+    float2* __restrict__ dEc = dE + gcol;
+    float2* __restrict__ Ec = E + gcol;
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      float2 gm[8], d0[8], e0[8];
+#pragma unroll
+      for (int i = 0; i < 8; ++i) {
+        const int y = p + P * (8 * h + i);
+        gm[i] = gmc[y];
+        d0[i] = dEc[y];
+        e0[i] = acc_now ? Ec[y] : make_float2(0.f, 0.f);
+      }
+#pragma unroll
+      for (int i = 0; i < 8; ++i) {
+        const int m = 8 * h + i;
+        const int y = p + P * m;
+        const float2 ep = cmul_conj(cmul_conj(v[m], gxz), a.w.gy[y]);
+        const float2 one_m = make_float2(1.f - kAlpha * gm[i].x, -kAlpha * gm[i].y);
+        const float2 t = cmul(cmul(gm[i], gm[i]), ep);
+        const float2 dn = cadd(cmul(one_m, d0[i]), make_float2(kAlpha * t.y, -kAlpha * t.x));
+        dEc[y] = dn;
+        if (acc_now) Ec[y] = cadd(e0[i], a.acc2 ? cadd(d0[i], dn) : dn);
+        if (in_xzc && y >= g.r0[0] && y < g.r1[0]) esum = fmaf(dn.x, dn.x, fmaf(dn.y, dn.y, esum));
+        v[m] = dn;
+      }
+    }
+    // K1 of iteration k + 1 on the same column
+    const float2 gxz1 = cmul(w1.gx[x], w1.gz[z]);
+    const float2* __restrict__ sr = src1 ? src1 + gcol : nullptr;
+#pragma unroll
+    for (int m = 0; m < 16; ++m) {
+      const int y = p + P * m;
+      float2 e = v[m];
+      if (sr) e = cadd(e, cmul(A, sr[y]));
+      v[m] = cmul(cmul(e, gxz1), w1.gy[y]);
+    }
+    if constexpr (P <= 32) {
+      line_fft<N, false>(v, L, p, a.py.tw, SyncWarp{});
+    } else {
+      line_fft<N, false>(v, L, p, a.py.tw, SyncBlock{});
+    }
+    // X[ky] of column x to the block holding row ky, in 16-byte pairs (ky, ky + 1)
+    // as in kf_plane_fwd
+    float2 w[16];
+#pragma unroll
+    for (int m = 0; m < 16; ++m) {
+      w[m].x = __shfl_xor_sync(0xffffffffu, v[m].x, 1);
+      w[m].y = __shfl_xor_sync(0xffffffffu, v[m].y, 1);
+    }
+    const uint32_t lbar = smem_addr(&recv_bar);
+    const bool odd = p & 1;
+#pragma unroll
+    for (int h = 0; h < 8; ++h) {
+      const int m = odd ? 8 + h : h;
+      const int ky = (p & ~1) + P * m;
+      const int dst = ky / LR, kyl = ky - dst * LR;
+      const uint32_t la = smem_addr(rt + x * G::CS2 + kyl + 2 * (kyl >> 4));
+      const float2 lo = odd ? w[8 + h] : v[h], hi = odd ? v[8 + h] : w[h];
+      st_async_f4(map_rank(la, dst), lo, hi, map_rank(lbar, dst));
+    }
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) esum += __shfl_xor_sync(0xffffffffu, esum, o);
+  if ((tid & 31) == 0) red[tid >> 5] = esum;
+  if (!mbar_wait_cluster(&recv_bar)) {
+    if (a.err) atomicExch(a.err, 1);
+  }
+  __syncthreads();
+  if (tid < 32) {
+    float v = tid < kThreads / 32 ? red[tid] : 0.f;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    if (tid == 0) partials[bid] = (double)v;
+  }
+  // K1's x transform of the received rows, written over the slab K3 read
+  for (int r0 = 0; r0 < LR; r0 += RPR) {
+    const int rl = r0 + tid % RPR, p = tid / RPR;
+    RowLine L{rt + rl + 2 * (rl >> 4), G::CS2};
+    float2 v[16];
+#pragma unroll
+    for (int r = 0; r < 16; ++r) v[r] = L.at(p + P * r);
+    line_fft<N, false>(v, L, p, a.twx, SyncBlock{});
+#pragma unroll
+    for (int m = 0; m < 16; ++m) slab[(long long)(p + P * m) * N + rl] = v[m];
+  }
+  // (no block leaves before every push into it has arrived: recv_bar)
+}
+
 }  // namespace fast
 }  // namespace ws

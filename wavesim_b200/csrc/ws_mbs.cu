@@ -81,6 +81,7 @@ struct FastInner {
   size_t smem;      // bytes (3-D, enough for both kernels); 2-D: bytes per held column, one extra column of scratch
   size_t smem_fwd, smem_inv;  // 3-D: what each kernel needs
   const void* fused = nullptr;  // K3 of one iteration + K1 of the next (3-D planes on a cluster), or null
+  size_t smem_fused = 0;
 };
 struct FastPencil {
   int no, ty;
@@ -97,7 +98,15 @@ static FastInner fast_inner() {
   FastInner f{N, C, DX ? 1 : 0, (const void*)fast::kf_plane_fwd<N, C, DX>,
               (const void*)fast::kf_plane_inv<N, C, DX>, DX ? G::smem : (size_t)G::CS * sizeof(float2),
               DX ? (G::PUSH ? G::smem_push : G::smem_a) : 0, DX ? G::smem_max_ab : 0};
-  if constexpr (DX && C > 1) f.fused = (const void*)fast::kf_plane_fused<N, C>;
+  if constexpr (DX && C > 1) {
+    if constexpr (C >= 16) {  // small tiles: the column tile and the row tile fit side by side
+      f.fused = (const void*)fast::kf_plane_fused_push<N, C>;
+      f.smem_fused = fast::FusedPushGeom<N, C>::smem;
+    } else {
+      f.fused = (const void*)fast::kf_plane_fused<N, C>;
+      f.smem_fused = G::smem_max_ab;
+    }
+  }
   return f;
 }
 template <int NO, int TY>
@@ -921,7 +930,7 @@ static cudaError_t launch_k3k1(const Solver* s, int w, int w1, bool src_next) {
   cudaLaunchConfig_t cfg{};
   cfg.gridDim = dim3((unsigned)(s->lay.grid_inner * s->nrhs));
   cfg.blockDim = dim3(fast::kThreads);
-  cfg.dynamicSmemBytes = s->lay.fi->smem_inv;
+  cfg.dynamicSmemBytes = s->lay.fi->smem_fused;
   cfg.stream = s->stream;
   cudaLaunchAttribute attr[1];
   attr[0].id = cudaLaunchAttributeClusterDimension;
