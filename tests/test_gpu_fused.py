@@ -41,6 +41,9 @@ CASES = {
     "256_cluster8": ((224, 224, 16), [16, 16, 8], None),
     # 16-block clusters: K1's half of the exchange pushed (kf_plane_fused_push)
     "256_cluster16": ((224, 224, 16), [16, 16, 8], {"WAVESIM_B200_CLUSTER": "16"}),
+    # 192-point planes on 6 blocks (km_plane_fused), scalar and vector
+    "192_cluster6": ((160, 160, 8), [16, 16, 4], None),
+    "192_cluster6_vector": ((160, 160, 4), [16, 16, 2], "vector"),
 }
 
 
@@ -48,16 +51,19 @@ CASES = {
 @pytest.mark.parametrize("use_graph", [True, False])
 def test_fused_loop_is_bit_identical(gpu, name, use_graph):
     shape, bw, env = CASES[name]
+    vector = env == "vector"
+    env = None if vector else env
     n = medium(shape)
-    opt = {"lambda": 1.0, "pixel_size": 0.25, "boundary_widths": bw, "energy_threshold": 1e-3,
-           "max_iterations": 48, "use_graph": use_graph}
+    opt = {"lambda": 1.0, "pixel_size": 0.125 if vector else 0.25, "boundary_widths": bw,
+           "energy_threshold": 1e-3, "max_iterations": 48, "use_graph": use_graph}
     val = np.ones(shape[:2]) + 0.3j
+    pos = [1, 1, 1, 2] if vector else [1, 1, 1]
 
     def run(ws):
-        sim = ws.WaveSim(n, opt)
+        sim = (ws.WaveSimVector if vector else ws.WaveSim)(n, opt)
         from wavesim_b200 import _lib
         fused = _lib.lib.ws_solver_launches_per_iteration(sim.solver()) == 3
-        E, st = sim.exec(ws.Source(val, [1, 1, 1]))
+        E, st = sim.exec(ws.Source(val, pos))
         sim.close()
         return E, st, fused
 

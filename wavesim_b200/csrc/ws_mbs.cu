@@ -119,8 +119,11 @@ using Plan192 = mixed::Plan<192, 12, 12, 4, 4>;
 template <class PL, int C>
 static FastInner mixed_inner() {
   using G = mixed::MGeom<PL, C>;
-  return FastInner{PL::N, C, 1, (const void*)mixed::km_plane_fwd<PL, C>, (const void*)mixed::km_plane_inv<PL, C>,
-                   G::smem, G::smem, G::smem};
+  FastInner f{PL::N, C, 1, (const void*)mixed::km_plane_fwd<PL, C>, (const void*)mixed::km_plane_inv<PL, C>,
+              G::smem, G::smem, G::smem};
+  f.fused = (const void*)mixed::km_plane_fused<PL, C>;
+  f.smem_fused = G::smem;
+  return f;
 }
 template <class PL, int TY, int NC>
 static FastPencil mixed_pencil() {

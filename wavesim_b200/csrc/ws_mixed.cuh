@@ -377,5 +377,169 @@ __global__ void __launch_bounds__(kThreads, 2)
   }
 }
 
+
+// K3 fused with K1 of the next iteration (as fast::kf_plane_fused): after
+// K3's epilogue a column's new increment is in registers as K1 loads it, so
+// the block adds the next source, applies the next wiggle's ramps, transforms
+// the column along y in place, exchanges rows across the cluster (pull
+// between two cluster barriers) and writes the x transform of its rows over
+// the slab of T it read at the start.  Bit-identical to km_plane_inv followed
+// by km_plane_fwd.
+template <class PL, int C>
+__global__ void __launch_bounds__(kThreads, 2)
+    km_plane_fused(InnerArgs a, Wig w1, const float2* __restrict__ src1, float2 A, float2* __restrict__ T,
+                   float2* __restrict__ dE, float2* __restrict__ E, const float2* __restrict__ gamma,
+                   const DevState* __restrict__ st, double* __restrict__ partials) {
+  using G = MGeom<PL, C>;
+  constexpr int N = PL::N, EL = PL::E, P = PL::P, M = G::M, LR = G::LR, LPR = G::LPR;
+  constexpr int RPR = kThreads / P;
+  const int rhs = blockIdx.x / a.bpr, bid = blockIdx.x - rhs * a.bpr;
+  st += rhs;
+  if (load_done(st)) return;  // the same for every block of a cluster
+  const bool acc_now = !a.acc2 || (__ldcg(&st->it) & 1) == 0;
+  T += rhs * a.fstride;
+  dE += rhs * a.fstride;
+  E += rhs * a.fstride;
+  if (src1) src1 += rhs * a.fstride;
+  partials += (long long)rhs * a.bpr;
+  extern __shared__ float2 sm[];
+  __shared__ float red[kThreads / 32];
+  const int tid = threadIdx.x;
+  const Geom& g = a.g;
+  const int rank = bid % C, plane = bid / C, z = plane % g.nz, comp = plane / g.nz;
+  const int x0 = rank * M;
+  const long long colbase = (long long)plane * N + x0;
+  float2* __restrict__ slab = T + (long long)plane * N * N + rank * LR;  // rows [rank LR, +LR) of the plane
+  cg::cluster_group cluster = cg::this_cluster();
+  // K3: inverse x transforms of the block's rows
+  for (int r0 = 0; r0 < LR; r0 += RPR) {
+    const int rl = r0 + tid % RPR, p = tid / RPR;
+    float2 v[EL];
+#pragma unroll
+    for (int r = 0; r < EL; ++r) v[r] = slab[(long long)(p + P * r) * N + rl];
+    fast::RowLine L{sm + rl, G::RS};
+    line_fft<PL, true>(v, L, p, a.twx, fast::SyncBlock{});
+#pragma unroll
+    for (int m = 0; m < EL; ++m) L.at(p + P * m) = v[m];
+  }
+  {
+    float2 hold[G::PER];
+    cluster.sync();
+#pragma unroll
+    for (int i = 0; i < G::PER; ++i) {
+      const int e = tid + kThreads * i;
+      const int ky = e % N, c = e / N;
+      const float2* rs = cluster.map_shared_rank(sm, ky / LR);
+      hold[i] = rs[(x0 + c) * G::RS + ky % LR];
+    }
+    cluster.sync();
+#pragma unroll
+    for (int i = 0; i < G::PER; ++i) {
+      const int e = tid + kThreads * i;
+      const int ky = e % N, c = e / N;
+      sm[c * G::CS + ky + (ky >> 4)] = hold[i];
+    }
+  }
+  __syncthreads();
+  const float2 gzz = a.w.gz[z];
+  const float2 gzz1 = w1.gz[z];
+  float esum = 0.f;
+  for (int c0 = 0; c0 < M; c0 += LPR) {
+    const int cl = c0 + tid / P, p = tid % P;
+    fast::ColLine L{sm + cl * G::CS};
+    float2 v[EL];
+#pragma unroll
+    for (int r = 0; r < EL; ++r) v[r] = L.at(p + P * r);
+    line_fft<PL, true>(v, L, p, a.py.tw, typename LineSync<P>::type{});
+    const int x = x0 + cl;
+    const long long gcol = (colbase + cl) * N;
+    const float2 gxz = cmul(a.w.gx[x], gzz);
+    const bool in_xzc =
+        x >= g.r0[1] && x < g.r1[1] && z >= g.r0[2] && z < g.r1[2] && comp >= g.r0[3] && comp < g.r1[3];
+    const float2* __restrict__ gmc = gamma + (gcol - (long long)comp * g.npts);
+    float2* __restrict__ dEc = dE + gcol;
+    float2* __restrict__ Ec = E + gcol;
+    // K3's epilogue; v[m] becomes dE'_k(y = p + P m)
+    constexpr int H = EL / 2;
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      float2 gm[H], d0[H], e0[H];
+#pragma unroll
+      for (int i = 0; i < H; ++i) {
+        const int y = p + P * (H * h + i);
+        gm[i] = gmc[y];
+        d0[i] = dEc[y];
+        e0[i] = acc_now ? Ec[y] : make_float2(0.f, 0.f);
+      }
+#pragma unroll
+      for (int i = 0; i < H; ++i) {
+        const int m = H * h + i;
+        const int y = p + P * m;
+        const float2 ep = cmul_conj(cmul_conj(v[m], gxz), a.w.gy[y]);
+        const float2 one_m = make_float2(1.f - kAlpha * gm[i].x, -kAlpha * gm[i].y);
+        const float2 t = cmul(cmul(gm[i], gm[i]), ep);
+        const float2 dn = cadd(cmul(one_m, d0[i]), make_float2(kAlpha * t.y, -kAlpha * t.x));
+        dEc[y] = dn;
+        if (acc_now) Ec[y] = cadd(e0[i], a.acc2 ? cadd(d0[i], dn) : dn);
+        if (in_xzc && y >= g.r0[0] && y < g.r1[0]) esum = fmaf(dn.x, dn.x, fmaf(dn.y, dn.y, esum));
+        v[m] = dn;
+      }
+    }
+    // K1 of iteration k + 1 on the same column: source, next ramps, y transform
+    const float2 gxz1 = cmul(w1.gx[x], gzz1);
+    const float2* __restrict__ sr = src1 ? src1 + gcol : nullptr;
+#pragma unroll
+    for (int m = 0; m < EL; ++m) {
+      const int y = p + P * m;
+      float2 e = v[m];
+      if (sr) e = cadd(e, cmul(A, sr[y]));
+      v[m] = cmul(cmul(e, gxz1), w1.gy[y]);
+    }
+    line_fft<PL, false>(v, L, p, a.py.tw, typename LineSync<P>::type{});
+#pragma unroll
+    for (int m = 0; m < EL; ++m) L.at(p + P * m) = v[m];
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) esum += __shfl_xor_sync(0xffffffffu, esum, o);
+  if ((tid & 31) == 0) red[tid >> 5] = esum;
+  // rows [rank LR, rank LR + LR) of all N transformed columns
+  {
+    float2 hold[G::PER];
+    cluster.sync();
+#pragma unroll
+    for (int i = 0; i < G::PER; ++i) {
+      const int e = tid + kThreads * i;
+      const int kyl = e % LR, x = e / LR;
+      const int ky = rank * LR + kyl;
+      const float2* rs = cluster.map_shared_rank(sm, x / M);
+      hold[i] = rs[(x % M) * G::CS + ky + (ky >> 4)];
+    }
+    cluster.sync();
+#pragma unroll
+    for (int i = 0; i < G::PER; ++i) {
+      const int e = tid + kThreads * i;
+      sm[(e / LR) * G::RS + e % LR] = hold[i];
+    }
+  }
+  __syncthreads();
+  if (tid < 32) {
+    float v = tid < kThreads / 32 ? red[tid] : 0.f;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    if (tid == 0) partials[bid] = (double)v;
+  }
+  // K1's x transforms, written over the slab K3 read
+  for (int r0 = 0; r0 < LR; r0 += RPR) {
+    const int rl = r0 + tid % RPR, p = tid / RPR;
+    fast::RowLine L{sm + rl, G::RS};
+    float2 v[EL];
+#pragma unroll
+    for (int r = 0; r < EL; ++r) v[r] = L.at(p + P * r);
+    line_fft<PL, false>(v, L, p, a.twx, fast::SyncBlock{});
+#pragma unroll
+    for (int m = 0; m < EL; ++m) slab[(long long)(p + P * m) * N + rl] = v[m];
+  }
+}
+
 }  // namespace mixed
 }  // namespace ws
