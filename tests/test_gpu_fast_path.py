@@ -55,6 +55,9 @@ CASES = {
     "3d_pencil_192": ((16, 16, 160), [8, 8, 16], 16, False),
     "3d_pencil_192_vector": ((16, 16, 160), [8, 8, 16], 16, True),
     "3d_128_vector": ((96, 96, 96), [16, 16, 16], 8, True),
+    # 96-point lines (12 x 4 x 2): a whole 96^2 plane on one block
+    "3d_96": ((64, 64, 64), [16, 16, 16], 16, False),
+    "3d_96_vector": ((64, 64, 64), [16, 16, 16], 8, True),
     # layout variants the autotuner may choose
     "3d_256_cluster16": ((224, 224, 16), [16, 16, 8], 16, False, {"WAVESIM_B200_CLUSTER": "16"}),
     "3d_pencil_192_vector_ty8": ((16, 16, 160), [8, 8, 16], 16, True, {"WAVESIM_B200_PENCIL_TY": "8"}),

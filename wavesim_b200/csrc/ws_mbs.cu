@@ -116,6 +116,7 @@ static FastPencil fast_pencil() {
 }
 // mixed-radix / vector kernels (ws_mixed.cuh)
 using Plan192 = mixed::Plan<192, 12, 12, 4, 4>;
+using Plan96 = mixed::Plan<96, 12, 12, 4, 2>;
 template <class PL, int C>
 static FastInner mixed_inner() {
   using G = mixed::MGeom<PL, C>;
@@ -137,7 +138,7 @@ static const std::vector<FastInner>& fast_inner_table() {
       fast_inner<256, 16, true>(),
       fast_inner<64, 1, false>(),    fast_inner<128, 1, false>(),   fast_inner<256, 1, false>(),
       fast_inner<512, 1, false>(),   fast_inner<1024, 1, false>(),  fast_inner<2048, 1, false>(),
-      mixed_inner<Plan192, 6>()};
+      mixed_inner<Plan192, 6>(),     mixed_inner<Plan96, 1>()};
   return t;
 }
 // Persistent TMA-pipelined K2 (ws_tma.cuh) for z pencils of a 3-D grid.
@@ -166,6 +167,8 @@ static const std::vector<FastPencil>& fast_pencil_table() {
       mixed_pencil<Plan192, 8, 3>(),   // (a TY = 8 variant first: the later TY = 16 is the default)
       mixed_pencil<Plan192, 16, 1>(),
       mixed_pencil<Plan192, 16, 3>(),
+      mixed_pencil<Plan96, 16, 1>(),
+      mixed_pencil<Plan96, 16, 3>(),
       mixed_pencil<mixed::Plan<64, 16, 16, 4>, 16, 3>(),
       mixed_pencil<mixed::Plan<128, 16, 16, 8>, 16, 3>(),
       mixed_pencil<mixed::Plan<256, 16, 16, 16>, 16, 3>()};
