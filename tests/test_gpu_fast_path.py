@@ -62,6 +62,11 @@ CASES = {
     "3d_256_cluster16": ((224, 224, 16), [16, 16, 8], 16, False, {"WAVESIM_B200_CLUSTER": "16"}),
     "3d_pencil_192_vector_ty8": ((16, 16, 160), [8, 8, 16], 16, True, {"WAVESIM_B200_PENCIL_TY": "8"}),
     "3d_256_pencil_tma": ((16, 16, 224), [8, 8, 16], 16, False),
+    "3d_256_pencil_tma_ty8": ((16, 16, 224), [8, 8, 16], 16, False, {"WAVESIM_B200_TMA_TY": "8"}),
+    "3d_256_pencil_tma_ty8_s6": ((16, 16, 224), [8, 8, 16], 16, False,
+                                 {"WAVESIM_B200_TMA_TY": "8", "WAVESIM_B200_TMA_STAGES": "6"}),
+    "3d_256_pencil_tma_ty4": ((16, 16, 224), [8, 8, 16], 16, False, {"WAVESIM_B200_TMA_TY": "4"}),
+    "3d_256_pencil_tma_ty16": ((16, 16, 224), [8, 8, 16], 16, False, {"WAVESIM_B200_TMA_TY": "16"}),
     "3d_256_pencil_plain": ((16, 16, 224), [8, 8, 16], 16, False, {"WAVESIM_B200_K2": "plain"}),
 }
 
