@@ -44,6 +44,9 @@ CASES = {
     # 192-point planes on 6 blocks (km_plane_fused), scalar and vector
     "192_cluster6": ((160, 160, 8), [16, 16, 4], None),
     "192_cluster6_vector": ((160, 160, 4), [16, 16, 2], "vector"),
+    # K3's rows by per-thread loads instead of one tensor copy (kf_plane_fused)
+    "128_cluster2_loads": ((96, 96, 96), [16, 16, 16], {"WAVESIM_B200_FUSED_TMA": "0"}),
+    "256_cluster8_loads": ((224, 224, 16), [16, 16, 8], {"WAVESIM_B200_FUSED_TMA": "0"}),
     # 96^2 planes on one block (km_plane_fused with a cluster of 1)
     "96_one_block": ((64, 64, 32), [16, 16, 16], None),
 }

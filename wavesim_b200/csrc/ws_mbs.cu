@@ -82,6 +82,7 @@ struct FastInner {
   size_t smem_fwd, smem_inv;  // 3-D: what each kernel needs
   const void* fused = nullptr;  // K3 of one iteration + K1 of the next (3-D planes on a cluster), or null
   size_t smem_fused = 0;
+  const void* fused_tma = nullptr;  // the same with K3's rows loaded by a tensor copy (first argument: the map)
 };
 struct FastPencil {
   int no, ty;
@@ -104,6 +105,7 @@ static FastInner fast_inner() {
       f.smem_fused = fast::FusedPushGeom<N, C>::smem;
     } else {
       f.fused = (const void*)fast::kf_plane_fused<N, C>;
+      f.fused_tma = (const void*)fast::kf_plane_fused_tma<N, C>;
       f.smem_fused = G::smem_max_ab;
     }
   }
@@ -383,6 +385,11 @@ struct Solver {
   int tmap_nrhs = 0;
   const void* tmap_kernel = nullptr;  // the TMA pencil the map and tma_blocks were made for
   int tma_blocks = 0;            // resident blocks of the TMA pencil (its persistent grid)
+  CUtensorMap tmap_slab{};       // T as 2-D {2 Ny floats, Nx Nz Nc nrhs}, box {2 LR, N}, for kf_plane_fused_tma
+  const void* slab_base = nullptr;
+  int slab_nrhs = 0;
+  const void* slab_kernel = nullptr;
+  int fused_tma = 1;             // the fused step loads K3's rows by a tensor copy (WAVESIM_B200_FUSED_TMA=0: not)
   int pf_inner = 0, pf_outer = 0;  // L2 prefetch distance of the fast kernels, in blocks (0: off)
   bool warm = false;             // the current solve starts from d_init
   int pstd = 0;                  // a PSTD stepper's solver: K2 applies the Laplacian (see ws_pstd_*)
@@ -485,6 +492,10 @@ static int set_kernel_attributes() {
     if (f.fused) {
       WS_CUDA(allow_dynamic_smem(f.fused, optin));
       WS_CUDA(cudaFuncSetAttribute(f.fused, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
+    }
+    if (f.fused_tma) {
+      WS_CUDA(allow_dynamic_smem(f.fused_tma, optin));
+      WS_CUDA(cudaFuncSetAttribute(f.fused_tma, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
     }
   }
   for (const FastPencil& f : fast_pencil_table()) WS_CUDA(allow_dynamic_smem(f.fn, optin));
@@ -600,6 +611,7 @@ static int create_solver(const int64_t N[4], const ws_complex* gamma, int64_t n_
     const int c = s->lay.fi ? std::max(1, s->lay.fi->c) : 1;
     s->pf_inner = (per_sm * kNumSms / c) * c;
     s->pf_outer = per_sm * kNumSms;
+    if (const char* e = std::getenv("WAVESIM_B200_FUSED_TMA")) s->fused_tma = std::atoi(e) ? 1 : 0;
   }
 #define WS_TRY(call)                 \
   do {                               \
@@ -928,7 +940,36 @@ static cudaError_t launch_iteration(const Solver* s, int it0, bool with_source, 
 
 // K3 of the iteration with wiggle w fused with K1 of the next (wiggle w1,
 // with the source when that iteration is one of the first Nw)
+// T as a 2-D float tensor {2 Ny, Nx Nz Nc nrhs} (one row per y column), box
+// {2 LR, N}: the x coordinate of every copy is 2 LR rank floats (a multiple
+// of 128 bytes), the row coordinate rhs Nx Nz Nc + plane Nx >= 0.
+static cudaError_t ensure_slab_map(Solver* s) {
+  const FastInner* f = s->lay.fi;
+  if (s->slab_base == s->d_T && s->slab_nrhs == s->nrhs && s->slab_kernel == f->fused_tma) return cudaSuccess;
+  EncodeTiledFn enc = encode_tiled();
+  if (!enc) return cudaErrorNotSupported;
+  const Geom& g = s->g;
+  const int LR = g.ny / f->c;
+  const cuuint64_t dims[2] = {(cuuint64_t)2 * g.ny, (cuuint64_t)g.nx * g.nz * g.nc * s->nrhs};
+  const cuuint64_t strides[1] = {(cuuint64_t)g.ny * sizeof(float2)};
+  const cuuint32_t box[2] = {(cuuint32_t)(2 * LR), (cuuint32_t)g.nx};
+  const cuuint32_t estr[2] = {1u, 1u};
+  if (enc(&s->tmap_slab, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, s->d_T, dims, strides, box, estr,
+          CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+          CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+    return cudaErrorInvalidValue;
+  s->slab_base = s->d_T;
+  s->slab_nrhs = s->nrhs;
+  s->slab_kernel = f->fused_tma;
+  return cudaSuccess;
+}
+
 static cudaError_t launch_k3k1(const Solver* s, int w, int w1, bool src_next) {
+  const bool tma = s->fused_tma && s->lay.fi->fused_tma;
+  if (tma) {
+    cudaError_t e = ensure_slab_map(const_cast<Solver*>(s));  // the map cache only
+    if (e != cudaSuccess) return e;
+  }
   InnerArgs a = inner_args(s, w);
   a.ncols = s->lay.ncols;
   Wig W1 = s->wig[w1];
@@ -941,6 +982,8 @@ static cudaError_t launch_k3k1(const Solver* s, int w, int w1, bool src_next) {
   const DevState* st = s->d_state;
   double* partials = s->d_partials;
   void* args[] = {&a, &W1, &src1, &A, &T, &dE, &E, &gamma, &st, &partials};
+  void* args_tma[] = {const_cast<CUtensorMap*>(&s->tmap_slab), &a, &W1, &src1, &A, &T, &dE, &E, &gamma, &st,
+                      &partials};
   cudaLaunchConfig_t cfg{};
   cfg.gridDim = dim3((unsigned)(s->lay.grid_inner * s->nrhs));
   cfg.blockDim = dim3(fast::kThreads);
@@ -953,7 +996,8 @@ static cudaError_t launch_k3k1(const Solver* s, int w, int w1, bool src_next) {
   attr[0].val.clusterDim.z = 1;
   cfg.attrs = attr;
   cfg.numAttrs = 1;
-  return cudaLaunchKernelExC(&cfg, s->lay.fi->fused, args);
+  return tma ? cudaLaunchKernelExC(&cfg, s->lay.fi->fused_tma, args_tma)
+             : cudaLaunchKernelExC(&cfg, s->lay.fi->fused, args);
 }
 
 // One iteration of the fused loop: T already holds K1's output for it.
