@@ -49,6 +49,8 @@ CASES = {
     "256_cluster8_loads": ((224, 224, 16), [16, 16, 8], {"WAVESIM_B200_FUSED_TMA": "0"}),
     # 96^2 planes on one block (km_plane_fused with a cluster of 1)
     "96_one_block": ((64, 64, 32), [16, 16, 16], None),
+    "192_cluster6_loads": ((160, 160, 8), [16, 16, 4], {"WAVESIM_B200_FUSED_TMA": "0"}),
+    "96_one_block_loads": ((64, 64, 32), [16, 16, 16], {"WAVESIM_B200_FUSED_TMA": "0"}),
 }
 
 

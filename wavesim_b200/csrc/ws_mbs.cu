@@ -125,7 +125,9 @@ static FastInner mixed_inner() {
   FastInner f{PL::N, C, 1, (const void*)mixed::km_plane_fwd<PL, C>, (const void*)mixed::km_plane_inv<PL, C>,
               G::smem, G::smem, G::smem};
   f.fused = (const void*)mixed::km_plane_fused<PL, C>;
+  f.fused_tma = (const void*)mixed::km_plane_fused_tma<PL, C>;
   f.smem_fused = G::smem;
+  static_assert((size_t)PL::N * G::LR * sizeof(float2) + 128 <= G::smem, "the dense row tile fits");
   return f;
 }
 template <class PL, int TY, int NC>

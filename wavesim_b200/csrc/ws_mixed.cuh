@@ -541,5 +541,206 @@ __global__ void __launch_bounds__(kThreads, 2)
   }
 }
 
+// The fused step with K3's rows loaded by one tensor copy (TMA) into a dense
+// tile instead of per-thread loads.
+template <class PL, int C>
+__global__ void __launch_bounds__(kThreads, 2)
+    km_plane_fused_tma(const __grid_constant__ CUtensorMap tslab, InnerArgs a, Wig w1, const float2* __restrict__ src1, float2 A, float2* __restrict__ T,
+                   float2* __restrict__ dE, float2* __restrict__ E, const float2* __restrict__ gamma,
+                   const DevState* __restrict__ st, double* __restrict__ partials) {
+  using G = MGeom<PL, C>;
+  constexpr int N = PL::N, EL = PL::E, P = PL::P, M = G::M, LR = G::LR, LPR = G::LPR;
+  constexpr int RPR = kThreads / P;
+  const int rhs = blockIdx.x / a.bpr, bid = blockIdx.x - rhs * a.bpr;
+  st += rhs;
+  if (load_done(st)) return;  // the same for every block of a cluster
+  const bool acc_now = !a.acc2 || (__ldcg(&st->it) & 1) == 0;
+  T += rhs * a.fstride;
+  dE += rhs * a.fstride;
+  E += rhs * a.fstride;
+  if (src1) src1 += rhs * a.fstride;
+  partials += (long long)rhs * a.bpr;
+  extern __shared__ float2 sm[];
+  __shared__ float red[kThreads / 32];
+  const int tid = threadIdx.x;
+  const Geom& g = a.g;
+  const int rank = bid % C, plane = bid / C, z = plane % g.nz, comp = plane / g.nz;
+  const int x0 = rank * M;
+  const long long colbase = (long long)plane * N + x0;
+  float2* __restrict__ slab = T + (long long)plane * N * N + rank * LR;  // rows [rank LR, +LR) of the plane
+  cg::cluster_group cluster = cg::this_cluster();
+  // K3's rows by one tensor copy: the box {2 LR floats, N columns} of the
+  // 2-D view {2 Ny floats, Nx Nz Nc nrhs columns} of T, landing dense:
+  // element (row kyl, x) at rt[x * LR + kyl]
+  float2* const rt = reinterpret_cast<float2*>((reinterpret_cast<uintptr_t>(sm) + 127) & ~(uintptr_t)127);
+  __shared__ __align__(8) uint64_t slab_bar;
+  if (tid == 0) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(fast::smem_addr(&slab_bar)));
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  __syncthreads();
+  if (tid == 0) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(fast::smem_addr(&slab_bar)),
+                 "r"((uint32_t)(N * LR * sizeof(float2)))
+                 : "memory");
+    const int c0 = 2 * rank * LR;
+    const int c1 = (int)((long long)rhs * (a.fstride / N) + (long long)plane * N);
+    asm volatile(
+        "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];" ::"r"(
+            fast::smem_addr(rt)),
+        "l"(&tslab), "r"(c0), "r"(c1), "r"(fast::smem_addr(&slab_bar))
+        : "memory");
+  }
+  {
+    const uint32_t ba = fast::smem_addr(&slab_bar);
+    const long long t0 = clock64();
+    bool ok = false;
+    while (true) {
+      uint32_t done;
+      asm volatile(
+          "{\n\t.reg .pred p;\n\t"
+          "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], 0;\n\t"
+          "selp.u32 %0, 1, 0, p;\n\t}"
+          : "=r"(done)
+          : "r"(ba)
+          : "memory");
+      if (done) {
+        ok = true;
+        break;
+      }
+      if (clock64() - t0 > 50000000LL) break;
+    }
+    if (!ok && a.err) atomicExch(a.err, 1);
+  }
+  // K3: inverse x transforms of the block's rows, in place
+  for (int r0 = 0; r0 < LR; r0 += RPR) {
+    const int rl = r0 + tid % RPR, p = tid / RPR;
+    float2 v[EL];
+    fast::RowLine L{rt + rl, LR};
+#pragma unroll
+    for (int r = 0; r < EL; ++r) v[r] = L.at(p + P * r);
+    line_fft<PL, true>(v, L, p, a.twx, fast::SyncBlock{});
+#pragma unroll
+    for (int m = 0; m < EL; ++m) L.at(p + P * m) = v[m];
+  }
+  {
+    float2 hold[G::PER];
+    cluster.sync();
+#pragma unroll
+    for (int i = 0; i < G::PER; ++i) {
+      const int e = tid + kThreads * i;
+      const int ky = e % N, c = e / N;
+      const float2* rs = cluster.map_shared_rank(rt, ky / LR);
+      hold[i] = rs[(x0 + c) * LR + ky % LR];
+    }
+    cluster.sync();
+#pragma unroll
+    for (int i = 0; i < G::PER; ++i) {
+      const int e = tid + kThreads * i;
+      const int ky = e % N, c = e / N;
+      sm[c * G::CS + ky + (ky >> 4)] = hold[i];
+    }
+  }
+  __syncthreads();
+  const float2 gzz = a.w.gz[z];
+  const float2 gzz1 = w1.gz[z];
+  float esum = 0.f;
+  for (int c0 = 0; c0 < M; c0 += LPR) {
+    const int cl = c0 + tid / P, p = tid % P;
+    fast::ColLine L{sm + cl * G::CS};
+    float2 v[EL];
+#pragma unroll
+    for (int r = 0; r < EL; ++r) v[r] = L.at(p + P * r);
+    line_fft<PL, true>(v, L, p, a.py.tw, typename LineSync<P>::type{});
+    const int x = x0 + cl;
+    const long long gcol = (colbase + cl) * N;
+    const float2 gxz = cmul(a.w.gx[x], gzz);
+    const bool in_xzc =
+        x >= g.r0[1] && x < g.r1[1] && z >= g.r0[2] && z < g.r1[2] && comp >= g.r0[3] && comp < g.r1[3];
+    const float2* __restrict__ gmc = gamma + (gcol - (long long)comp * g.npts);
+    float2* __restrict__ dEc = dE + gcol;
+    float2* __restrict__ Ec = E + gcol;
+    // K3's epilogue; v[m] becomes dE'_k(y = p + P m)
+    constexpr int H = EL / 2;
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      float2 gm[H], d0[H], e0[H];
+#pragma unroll
+      for (int i = 0; i < H; ++i) {
+        const int y = p + P * (H * h + i);
+        gm[i] = gmc[y];
+        d0[i] = dEc[y];
+        e0[i] = acc_now ? Ec[y] : make_float2(0.f, 0.f);
+      }
+#pragma unroll
+      for (int i = 0; i < H; ++i) {
+        const int m = H * h + i;
+        const int y = p + P * m;
+        const float2 ep = cmul_conj(cmul_conj(v[m], gxz), a.w.gy[y]);
+        const float2 one_m = make_float2(1.f - kAlpha * gm[i].x, -kAlpha * gm[i].y);
+        const float2 t = cmul(cmul(gm[i], gm[i]), ep);
+        const float2 dn = cadd(cmul(one_m, d0[i]), make_float2(kAlpha * t.y, -kAlpha * t.x));
+        dEc[y] = dn;
+        if (acc_now) Ec[y] = cadd(e0[i], a.acc2 ? cadd(d0[i], dn) : dn);
+        if (in_xzc && y >= g.r0[0] && y < g.r1[0]) esum = fmaf(dn.x, dn.x, fmaf(dn.y, dn.y, esum));
+        v[m] = dn;
+      }
+    }
+    // K1 of iteration k + 1 on the same column: source, next ramps, y transform
+    const float2 gxz1 = cmul(w1.gx[x], gzz1);
+    const float2* __restrict__ sr = src1 ? src1 + gcol : nullptr;
+#pragma unroll
+    for (int m = 0; m < EL; ++m) {
+      const int y = p + P * m;
+      float2 e = v[m];
+      if (sr) e = cadd(e, cmul(A, sr[y]));
+      v[m] = cmul(cmul(e, gxz1), w1.gy[y]);
+    }
+    line_fft<PL, false>(v, L, p, a.py.tw, typename LineSync<P>::type{});
+#pragma unroll
+    for (int m = 0; m < EL; ++m) L.at(p + P * m) = v[m];
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) esum += __shfl_xor_sync(0xffffffffu, esum, o);
+  if ((tid & 31) == 0) red[tid >> 5] = esum;
+  // rows [rank LR, rank LR + LR) of all N transformed columns
+  {
+    float2 hold[G::PER];
+    cluster.sync();
+#pragma unroll
+    for (int i = 0; i < G::PER; ++i) {
+      const int e = tid + kThreads * i;
+      const int kyl = e % LR, x = e / LR;
+      const int ky = rank * LR + kyl;
+      const float2* rs = cluster.map_shared_rank(sm, x / M);
+      hold[i] = rs[(x % M) * G::CS + ky + (ky >> 4)];
+    }
+    cluster.sync();
+#pragma unroll
+    for (int i = 0; i < G::PER; ++i) {
+      const int e = tid + kThreads * i;
+      sm[(e / LR) * G::RS + e % LR] = hold[i];
+    }
+  }
+  __syncthreads();
+  if (tid < 32) {
+    float v = tid < kThreads / 32 ? red[tid] : 0.f;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    if (tid == 0) partials[bid] = (double)v;
+  }
+  // K1's x transforms, written over the slab K3 read
+  for (int r0 = 0; r0 < LR; r0 += RPR) {
+    const int rl = r0 + tid % RPR, p = tid / RPR;
+    fast::RowLine L{sm + rl, G::RS};
+    float2 v[EL];
+#pragma unroll
+    for (int r = 0; r < EL; ++r) v[r] = L.at(p + P * r);
+    line_fft<PL, false>(v, L, p, a.twx, fast::SyncBlock{});
+#pragma unroll
+    for (int m = 0; m < EL; ++m) slab[(long long)(p + P * m) * N + rl] = v[m];
+  }
+}
+
 }  // namespace mixed
 }  // namespace ws
