@@ -54,6 +54,7 @@ CASES = {
     "3d_192_cluster6_vector": ((160, 160, 4), [16, 16, 2], 16, True),
     "3d_pencil_192": ((16, 16, 160), [8, 8, 16], 16, False),
     "3d_pencil_192_vector": ((16, 16, 160), [8, 8, 16], 16, True),
+    "3d_pencil_192_vector_plain": ((16, 16, 160), [8, 8, 16], 16, True, {"WAVESIM_B200_K2": "plain"}),
     "3d_128_vector": ((96, 96, 96), [16, 16, 16], 8, True),
     # 96-point lines (12 x 4 x 2): a whole 96^2 plane on one block
     "3d_96": ((64, 64, 64), [16, 16, 16], 16, False),

@@ -151,12 +151,19 @@ struct TmaPencil {
   const void* fn;
   size_t smem;
   int threads;
+  int nc = 1;  // components (3: the vector form, kt_pencil_vec)
 };
 template <int NO, int TY, int S>
 static TmaPencil tma_pencil() {
   using PT = tma::PencilTile<NO, TY, S>;
   return TmaPencil{NO, TY, S, (const void*)tma::kt_pencil<NO, TY, S>, PT::smem, PT::kThreads};
 }
+template <class PL, int TY, int S>
+static TmaPencil tma_pencil_vec() {
+  using PT = tma::VecPencilTile<PL, TY, S>;
+  return TmaPencil{PL::N, TY, S, (const void*)tma::kt_pencil_vec<PL, TY, S>, PT::smem, PT::kThreads, 3};
+}
+using Plan192t = mixed::Plan<192, 12, 12, 4, 4>;
 static const std::vector<TmaPencil>& tma_pencil_table() {
   // the first match of (no, ty) is the default; the autotuner tries the rest
   // (at 256: 8 y x 4 stages measured 0.072 ms against 0.074 for 16 x 3, 0.081
@@ -164,7 +171,8 @@ static const std::vector<TmaPencil>& tma_pencil_table() {
   static const std::vector<TmaPencil> t = {tma_pencil<64, 16, 3>(), tma_pencil<128, 16, 3>(),
                                            tma_pencil<256, 8, 4>(),  tma_pencil<256, 16, 3>(),
                                            tma_pencil<256, 16, 2>(), tma_pencil<256, 8, 6>(),
-                                           tma_pencil<256, 4, 4>()};
+                                           tma_pencil<256, 4, 4>(),
+                                           tma_pencil_vec<Plan192t, 8, 3>()};
   return t;
 }
 
@@ -324,14 +332,14 @@ static int make_layout(const Geom& g, Layout& L, std::string& why, const LayoutC
   // the TMA pencil where a shape matches: by default (WAVESIM_B200_K2=plain keeps kf_pencil), or the
   // autotuner's choice of stages
   const char* k2 = std::getenv("WAVESIM_B200_K2");
-  const bool tma_ok = L.mode3d && g.nc == 1 && (ch.outer == 0 || ch.outer >= 3) &&
+  const bool tma_ok = L.mode3d && (ch.outer == 0 || ch.outer >= 3) &&
                       !(ch.outer == 0 && k2 && std::strcmp(k2, "plain") == 0);
   int want_tty = 0, want_ts = 0;  // WAVESIM_B200_TMA_TY / _TMA_STAGES: the y tile and stages of the TMA pencil
   if (const char* e = std::getenv("WAVESIM_B200_TMA_TY")) want_tty = std::atoi(e);
   if (const char* e = std::getenv("WAVESIM_B200_TMA_STAGES")) want_ts = std::atoi(e);
   if (tma_ok)
     for (const TmaPencil& f : tma_pencil_table())
-      if (f.no == no && g.ny % f.ty == 0 && (ch.outer < 3 || f.stages == ch.outer - 3) &&
+      if (f.no == no && f.nc == g.nc && g.ny % f.ty == 0 && (ch.outer < 3 || f.stages == ch.outer - 3) &&
           (!want_tty || f.ty == want_tty) && (!want_ts || f.stages == want_ts)) {
         L.tp = &f;
         break;
@@ -849,9 +857,9 @@ static EncodeTiledFn encode_tiled() {
   return fn;
 }
 
-// T of the current batch as a 3-D float tensor {2 Ny, Nx, Nz nrhs}, box
+// T of the current batch as a 3-D float tensor {2 Ny, Nx, Nz Nc nrhs}, box
 // {2 TY, 1, Nz}: every x coordinate the kernel issues is 2 TY yt floats, a
-// multiple of 32 floats, so each copy starts on a 128-byte boundary.
+// multiple of 16 floats (TY >= 8), so each copy starts on a 64-byte boundary.
 static cudaError_t ensure_tmap(Solver* s) {
   const TmaPencil* f = s->lay.tp;
   if (s->tmap_base == s->d_T && s->tmap_nrhs == s->nrhs && s->tmap_kernel == f->fn) return cudaSuccess;
@@ -860,7 +868,7 @@ static cudaError_t ensure_tmap(Solver* s) {
   EncodeTiledFn enc = encode_tiled();
   if (!enc) return cudaErrorNotSupported;
   const Geom& g = s->g;
-  const cuuint64_t dims[3] = {(cuuint64_t)2 * g.ny, (cuuint64_t)g.nx, (cuuint64_t)g.nz * s->nrhs};
+  const cuuint64_t dims[3] = {(cuuint64_t)2 * g.ny, (cuuint64_t)g.nx, (cuuint64_t)g.nz * g.nc * s->nrhs};
   const cuuint64_t strides[2] = {(cuuint64_t)g.ny * sizeof(float2), (cuuint64_t)g.ny * g.nx * sizeof(float2)};
   const cuuint32_t box[3] = {(cuuint32_t)(2 * f->ty), 1u, (cuuint32_t)f->no};
   const cuuint32_t estr[3] = {1u, 1u, 1u};

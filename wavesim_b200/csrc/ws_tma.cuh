@@ -18,7 +18,7 @@
 #pragma once
 #include <cuda.h>
 
-#include "ws_fast.cuh"
+#include "ws_mixed.cuh"
 
 namespace ws {
 namespace tma {
@@ -184,6 +184,136 @@ __global__ void __launch_bounds__(PencilTile<NO, TY, S>::kThreads, 2)
     if (tid == 0) atomicExch(err, 1);
     // drain the loads still in flight: tiles i .. min(i + S - 2, mine - 1); a
     // load that never arrives is abandoned after the same bound
+    for (int j = i; j < mine && j < i + S - 1; ++j) (void)wait_parity(&full[j % S], (uint32_t)((j / S) & 1));
+  }
+  if (tid == 0) bulk_wait_all();
+}
+
+
+// The vector form (WaveSimVector, 3 components): a tile is the three
+// component boxes of the same (x, y tile), at z offsets c Nz of the map
+// {2 Ny floats, Nx, Nz Nc nrhs}; each line is transformed with the
+// register-resident mixed-radix schedule (ws_mixed.cuh), the dyadic Green's
+// function (f_g0_vector.m) applied at every k point in registers, and the
+// three boxes stored back.  The rest is kt_pencil.
+template <class PL, int TY, int S>
+struct VecPencilTile {
+  static constexpr int NO = PL::N, P = PL::P, E = PL::E;
+  static_assert(NO <= 256, "a TMA box dimension holds at most 256 elements");
+  static_assert(2 * TY * 4 % 16 == 0 && 2 * TY <= 256, "inner box extent");
+  static constexpr int kThreads = TY * P;
+  static constexpr unsigned kBoxBytes = NO * TY * sizeof(float2);
+  static constexpr unsigned kTileBytes = 3 * kBoxBytes;
+  static constexpr size_t smem = S * (size_t)kTileBytes + 128;
+};
+
+template <class PL, int TY, int S>
+__global__ void __launch_bounds__(VecPencilTile<PL, TY, S>::kThreads, 1)
+    kt_pencil_vec(const __grid_constant__ CUtensorMap tmap, OuterArgs a, const DevState* __restrict__ st, int ntiles,
+                  int* __restrict__ err) {
+  using PT = VecPencilTile<PL, TY, S>;
+  constexpr int NO = PT::NO, P = PT::P, E = PT::E;
+  extern __shared__ uint8_t smem_raw[];
+  float2* const buf0 = reinterpret_cast<float2*>((reinterpret_cast<uintptr_t>(smem_raw) + 127) & ~(uintptr_t)127);
+  __shared__ __align__(8) uint64_t full[S];
+  const Geom& g = a.g;
+  const int tid = threadIdx.x;
+  const int yl = tid % TY, p = tid / TY;
+  const int nyt = g.ny / TY;
+  const int per_rhs = nyt * g.nx;
+  if (tid == 0) {
+#pragma unroll
+    for (int b = 0; b < S; ++b) asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(fast::smem_addr(&full[b])));
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  __syncthreads();
+  auto coords = [&](int t, int& rhs, int& mid, int& yt) {
+    rhs = t / per_rhs;
+    const int r = t - rhs * per_rhs;
+    mid = r / nyt;
+    yt = r - mid * nyt;
+  };
+  auto box = [&](int b, int c) { return buf0 + (b * 3 + c) * NO * TY; };
+  auto issue = [&](int t, int b) {
+    int rhs, mid, yt;
+    coords(t, rhs, mid, yt);
+    expect_bytes(&full[b], PT::kTileBytes);
+#pragma unroll
+    for (int c = 0; c < 3; ++c)
+      load_3d(fast::smem_addr(box(b, c)), &tmap, 2 * TY * yt, mid, (rhs * 3 + c) * g.nz, fast::smem_addr(&full[b]));
+  };
+  const int G = gridDim.x;
+  const int mine = blockIdx.x < ntiles ? (ntiles - 1 - blockIdx.x) / G + 1 : 0;
+  if (tid == 0)
+    for (int i = 0; i < S - 1 && i < mine; ++i) issue(blockIdx.x + i * G, i);
+  const float kk = fmaf(a.k02e.x, a.k02e.x, a.k02e.y * a.k02e.y);
+  const float di = -a.k02e.y;
+  int i = 0;
+  bool ok = true;
+  for (; i < mine; ++i) {
+    const int b = i % S;
+    const int t = blockIdx.x + i * G;
+    ok = wait_parity(&full[b], (uint32_t)((i / S) & 1));
+    if (__syncthreads_or(!ok)) {
+      ok = false;
+      break;
+    }
+    auto refill = [&]() {
+      const int nxt = i + S - 1;
+      if (tid == 0 && nxt < mine) {
+        bulk_wait_read_0();
+        issue(blockIdx.x + nxt * G, nxt % S);
+      }
+    };
+    int rhs, mid, yt;
+    coords(t, rhs, mid, yt);
+    const bool live = !load_done(st + rhs);
+    if (!live) refill();
+    if (live) {
+      float2 v[3][E];
+#pragma unroll
+      for (int c = 0; c < 3; ++c)
+#pragma unroll
+        for (int r = 0; r < E; ++r) v[c][r] = box(b, c)[(p + P * r) * TY + yl];
+#pragma unroll
+      for (int c = 0; c < 3; ++c)
+        mixed::line_fft<PL, false>(v[c], fast::RowLine{box(b, c) + yl, TY}, p, a.po.tw, fast::SyncBlock{});
+      // f_g0_vector with the 1/N of ifftn: div = (p . E) / k02e; E_i <- (E_i - p_i div) / (|p|^2 - k02e)
+      const float px = a.w.pxe[mid], py = a.w.pye[yt * TY + yl];
+#pragma unroll
+      for (int m = 0; m < E; ++m) {
+        const float pz = a.w.pze[p + P * m];
+        const float dr = fmaf(px, px, fmaf(py, py, pz * pz)) - a.k02e.x;
+        const float inv = __fdividef(a.norm, fmaf(dr, dr, di * di));
+        const float2 g0 = make_float2(dr * inv, -di * inv);
+        const float2 ex = v[0][m], ey = v[1][m], ez = v[2][m];
+        const float2 pe =
+            make_float2(fmaf(px, ex.x, fmaf(py, ey.x, pz * ez.x)), fmaf(px, ex.y, fmaf(py, ey.y, pz * ez.y)));
+        const float2 dv =
+            make_float2((pe.x * a.k02e.x + pe.y * a.k02e.y) / kk, (pe.y * a.k02e.x - pe.x * a.k02e.y) / kk);
+        v[0][m] = cmul(g0, make_float2(ex.x - px * dv.x, ex.y - px * dv.y));
+        v[1][m] = cmul(g0, make_float2(ey.x - py * dv.x, ey.y - py * dv.y));
+        v[2][m] = cmul(g0, make_float2(ez.x - pz * dv.x, ez.y - pz * dv.y));
+      }
+      refill();
+#pragma unroll
+      for (int c = 0; c < 3; ++c)
+        mixed::line_fft<PL, true>(v[c], fast::RowLine{box(b, c) + yl, TY}, p, a.po.tw, fast::SyncBlock{});
+#pragma unroll
+      for (int c = 0; c < 3; ++c)
+#pragma unroll
+        for (int m = 0; m < E; ++m) box(b, c)[(p + P * m) * TY + yl] = v[c][m];
+      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    }
+    __syncthreads();
+    if (tid == 0 && live) {
+#pragma unroll
+      for (int c = 0; c < 3; ++c) store_3d(&tmap, 2 * TY * yt, mid, (rhs * 3 + c) * g.nz, fast::smem_addr(box(b, c)));
+      bulk_commit();
+    }
+  }
+  if (!ok) {
+    if (tid == 0) atomicExch(err, 1);
     for (int j = i; j < mine && j < i + S - 1; ++j) (void)wait_parity(&full[j % S], (uint32_t)((j / S) & 1));
   }
   if (tid == 0) bulk_wait_all();
