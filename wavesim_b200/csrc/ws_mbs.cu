@@ -172,6 +172,8 @@ static const std::vector<TmaPencil>& tma_pencil_table() {
                                            tma_pencil<256, 8, 4>(),  tma_pencil<256, 16, 3>(),
                                            tma_pencil<256, 16, 2>(), tma_pencil<256, 8, 6>(),
                                            tma_pencil<256, 4, 4>(),
+                                           // 192 x 3 components: 8 y x 3 stages measured 0.131 ms against
+                                           // 0.132 (8 x 2), 0.137 (16 x 2), 0.163 (4 x 4)
                                            tma_pencil_vec<Plan192t, 8, 3>()};
   return t;
 }
