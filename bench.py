@@ -148,63 +148,110 @@ def profile_traffic(kernel):
     return None
 
 
+def load_workloads():
+    """wavesim_b200/workloads.py loaded on its own (NumPy only): importing it
+    through the package would load the CUDA library, which the reference arm
+    must never touch."""
+    import importlib.util
+    spec = importlib.util.spec_from_file_location("ws_bench_workloads",
+                                                  os.path.join(ROOT, "wavesim_b200", "workloads.py"))
+    mod = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mod)
+    return mod
+
+
 def build_problem(config):
-    from wavesim_b200 import workloads
     import wavesim_b200 as ws
-    n, opt, val, pos, vector = workloads.CONFIGS[config]()
+    n, opt, val, pos, vector = load_workloads().CONFIGS[config]()
     t = time.time()
     sim = (ws.WaveSimVector if vector else ws.WaveSim)(n, dict(opt, device_setup=True))
     return sim, ws.Source(val, pos), time.time() - t, (n, opt, val, pos, vector)
 
 
-def reference_iterations():
+def reference_iterations(config="c3"):
+    """Iterations the oracle's restatement of the reference loop needs to reach
+    the tolerance on this workload (tests/golden/make_config_runs.py)."""
     try:
-        return json.load(open(os.path.join(ROOT, "tests", "golden", "c3_reference_run.json")))["iterations"]
+        return json.load(open(os.path.join(ROOT, "tests", "golden", f"{config}_reference_run.json")))["iterations"]
     except Exception:
         return None
 
 
-def cpu_sample(spec, iters):
+def config_dict(config, grid, ws):
+    """The `config` object of both arms' JSON lines (same keys, same values)."""
+    return {"workload": WORKLOAD if config == "c3" else config, "grid": [int(v) for v in grid],
+            "stop_rule": "reference (Simulation.next)",
+            "l2": "inputs larger than L2 (each 256^3 c64 array is 134 MB > 126 MB L2)",
+            "parallelism": f"replicas x{ws}"}
+
+
+def cpu_sample(spec, iters, sim=None):
     """The FP32 restatement of the reference loop (oracle/) timed for `iters`
-    iterations on all host cores; returns ms per iteration."""
+    iterations on all host cores; returns ms per iteration and the
+    iterations run (the loop ends on a multiple of Nw)."""
     from oracle import mbs_oracle as ref
     n, opt, val, pos, vector = spec
-    sim = (ref.WaveSimVector if vector else ref.WaveSim)(n, dict(opt, single_precision=True))
+    if sim is None:
+        sim = (ref.WaveSimVector if vector else ref.WaveSim)(n, dict(opt, single_precision=True))
     src = ref.Source(val, pos)
     t = time.perf_counter()
     sim.exec(src, max_iterations=iters)
     dt = time.perf_counter() - t
     nw = len(sim.wiggles)
-    done = ((iters + nw - 1) // nw) * nw  # the loop ends on a multiple of Nw
+    done = ((iters + nw - 1) // nw) * nw
     return 1e3 * dt / done, done
 
 
 def run_reference(args):
-    torch, dist, ws, rank, local = dist_setup("gloo")
-    if rank != 0:
-        if ws > 1:
+    """The reference arm: the reference loop's CPU implementation (the FP32
+    restatement in oracle/, scipy.fft on every host core) on the same
+    workload, built from the seeded generator and the oracle only - no part
+    of the CUDA product is imported or run.  A full solve takes minutes on
+    the host, so each step times one wiggle cycle (Nw iterations) of the
+    solve and the line reports that per-iteration time times the iterations
+    the reference loop needs to reach the tolerance (152 for the 256^3
+    workload, tests/golden/c3_reference_run.json)."""
+    import scipy.fft  # noqa: F401
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    if ws > 1:
+        import torch.distributed as dist
+        from datetime import timedelta
+        dist.init_process_group("gloo", timeout=timedelta(seconds=600))
+        if rank != 0:
             dist.barrier()
             dist.destroy_process_group()
-        return
-    _, _, _, spec = build_problem(args.config)
-    iters_tol = reference_iterations() if args.config == "c3" else None
-    samples = []
+            return
+    from oracle import mbs_oracle as ref
+    spec = load_workloads().CONFIGS[args.config]()
+    n, opt, val, pos, vector = spec
+    sim = (ref.WaveSimVector if vector else ref.WaveSim)(n, dict(opt, single_precision=True))
+    iters_tol = reference_iterations(args.config)
+    samples, timed = [], 0
+    t_all = time.perf_counter()
     for i in range(args.warmup + args.steps):
-        ms_it, done = cpu_sample(spec, 1)
+        ms_it, done = cpu_sample(spec, 1, sim)
         if i >= args.warmup:
             samples.append(ms_it)
+            timed += done
+    wall_s = time.perf_counter() - t_all
     ms_it = float(np.mean(samples))
     value = ms_it * iters_tol if iters_tol else None
+    threads = os.cpu_count()
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": value, "higher_is_better": False,
         "scaling": "weak", "vs_baseline": None, "dtype": "c64 (fp32 complex)", "data": "synthetic (seeded)",
-        "config": {"workload": WORKLOAD if args.config == "c3" else args.config},
-        "ms_per_iteration": ms_it, "iterations_to_tol": iters_tol,
-        "cpu_baseline": {"value": value, "unit": UNIT, "cores": os.cpu_count(), "kind": "port",
-                         "sample": f"{args.steps} steps of one MBS iteration each (rounded up to a multiple of "
-                                   f"Nw by the reference stop rule) of the 256^3 workload, FP32 scipy.fft "
-                                   f"restatement on {os.cpu_count()} threads, projected to the reference's "
+        "config": config_dict(args.config, sim.N, ws),
+        "value_kind": f"projection: measured ms per iteration x {iters_tol} iterations to tolerance "
+                      f"(a full solve is ~{(value or 0) / 1e3:.0f} s on the host)",
+        "ms_per_iteration": ms_it, "iterations_timed": timed, "iterations_to_tol": iters_tol,
+        "timed_wall_s": wall_s,
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
+                         "sample": f"{args.steps} steps of one wiggle cycle ({timed // max(1, args.steps)} "
+                                   f"iterations) each of the {args.config} workload, FP32 scipy.fft "
+                                   f"restatement of the reference loop on {threads} threads, "
+                                   f"{ms_it:.1f} ms per iteration, projected to the reference's "
                                    f"{iters_tol} iterations to tolerance"},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
@@ -338,15 +385,12 @@ def run_ours(args):
                          f"{ms_it:.1f} ms/iteration, projected to the {n_iter} iterations to tolerance"}
 
     if rank == 0:
-        ref_it = reference_iterations() if args.config == "c3" else None
+        ref_it = reference_iterations(args.config)
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": value, "higher_is_better": False, "scaling": "weak",
             "vs_baseline": None, "dtype": "c64 (fp32 complex)", "data": "synthetic (seeded)",
-            "config": {"workload": WORKLOAD if args.config == "c3" else args.config,
-                       "grid": [int(v) for v in sim.N], "stop_rule": "reference (Simulation.next), on device",
-                       "l2": "inputs larger than L2 (each 256^3 c64 array is 134 MB > 126 MB L2)",
-                       "parallelism": f"replicas x{ws}"},
+            "config": config_dict(args.config, sim.N, ws),
             "iterations_to_tol": n_iter, "reference_iterations_to_tol": ref_it, "converged": bool(conv.value),
             "ms_per_solve_per_gpu": ms_per_solve_gpu, "ms_per_iteration": ms_per_solve_gpu / n_iter,
             "iterations_per_s": n_iter / (ms_per_solve_gpu * 1e-3) * ws,
@@ -434,6 +478,7 @@ def run_warm(args, sim, h, s, blocks, opts, torch, dev, E_plain, plain_ms):
     n_it, conv = C.c_int64(), C.c_int()
 
     cold, warm, disc = C.c_double(), C.c_double(), C.c_int()
+    rc, rw = C.c_double(), C.c_double()
 
     def step():
         psi = model.predict_grid(sim, n_roi)
@@ -441,6 +486,7 @@ def run_warm(args, sim, h, s, blocks, opts, torch, dev, E_plain, plain_ms):
         _lib.check(_lib.lib.ws_solver_solve(h, len(s.values), blocks, _lib.WS_DEVICE, C.byref(o), E_w.data_ptr(),
                                             _lib.WS_DEVICE, None, C.byref(n_it), C.byref(conv)))
         _lib.check(_lib.lib.ws_solver_warm_report(h, 0, C.byref(cold), C.byref(warm), C.byref(disc)))
+        _lib.check(_lib.lib.ws_solver_warm_residual(h, 0, C.byref(rc), C.byref(rw)))
         if disc.value:  # given up after one cycle: the cold solve decides
             _lib.check(_lib.lib.ws_solver_solve(h, len(s.values), blocks, _lib.WS_DEVICE, C.byref(opts),
                                                 E_w.data_ptr(), _lib.WS_DEVICE, None, C.byref(n_it), C.byref(conv)))
@@ -465,6 +511,7 @@ def run_warm(args, sim, h, s, blocks, opts, torch, dev, E_plain, plain_ms):
             "iterations": int(n_it.value) + (0 if disc.value else 1),
             "note_iterations": "loop iterations plus the cold probe iteration of a warm start",
             "discarded": bool(disc.value), "first_cycle_energy_ratio": warm.value / cold.value,
+            "initial_residual_ratio": (rw.value / rc.value) if rc.value > 0 else None,
             "rel_l2_vs_plain": diff, "speedup_vs_plain": plain_ms / ms, "checkpoint": os.path.relpath(DEFAULT_OUT, ROOT)}
 
 

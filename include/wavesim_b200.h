@@ -129,10 +129,14 @@ typedef struct ws_solve_options {
   const ws_complex* initial_field;
   int initial_memory;            /* WS_HOST or WS_DEVICE */
   int initial_is_eprime;
-  /* A warm start whose true ROI increment energy at the end of its first
-   * wiggle cycle exceeds warm_discard_ratio x diff_energy(1) stops there,
-   * unconverged and marked discarded (ws_solver_warm_report), to be rerun
-   * cold.  0 keeps every start. */
+  /* A warm start whose initial residual is worse than the cold start's is
+   * given up before its first wiggle cycle: unconverged and marked discarded
+   * (ws_solver_warm_report), to be rerun cold.  The residual of a start u
+   * (E' variables) is r(u) = T(u, S) - u, T one reference iteration with the
+   * first wiggle and the whole source, so r(0) is the cold start's; the test
+   * is ROI energy |r(u)|^2 > warm_discard_ratio x |r(0)|^2 (1e-3 relative
+   * slack for rounding).  It costs one iteration.  1.0 is the plain rule,
+   * 0 keeps every start. */
   double warm_discard_ratio;
 } ws_solve_options;
 
@@ -234,6 +238,15 @@ int ws_solver_buffers(ws_solver s, void** E_prime, void** stream);
  * iterations only, and every stop of the loop falls after an even one). */
 int ws_solver_time_kernels(ws_solver s, int n_iterations, float ms_out[3], double bytes_out[3]);
 
+/* Bound of the waits of the TMA-pipelined outer pass (K2 of 3-D grids): a
+ * block whose tile load has not arrived after `clocks` SM clocks gives up,
+ * waits for its copies still in flight (with the default bound), and the
+ * solve returns WS_ERR_CUDA ("timed out") instead of hanging.  0 restores the
+ * default (5e7 clocks, ~25 ms).  A very small bound makes the waits run out
+ * on purpose: the failure path can be tested without a GPU fault.  No
+ * counterpart in the reference. */
+int ws_solver_set_wait_limit(ws_solver s, int64_t clocks);
+
 /* Number of kernel launches one iteration makes. */
 int ws_solver_launches_per_iteration(ws_solver s);
 
@@ -246,10 +259,18 @@ int ws_solver_time_fused(ws_solver s, int n_iterations, float* ms_out, double* b
 /* After a warm-started solve of right-hand side `rhs`: the ROI energy of the
  * cold first increment (diff_energy(1), from the probe iteration), the ROI
  * energy of the true increment at the end of the warm first wiggle cycle,
- * and whether the start was discarded there.  Any pointer may be NULL; the
+ * and whether the start was discarded (by its initial residual, see
+ * warm_discard_ratio).  Any pointer may be NULL; the
  * values are -1 / 0 after a cold solve.  No counterpart in the reference. */
 int ws_solver_warm_report(ws_solver s, int64_t rhs, double* cold_first_energy, double* warm_cycle_energy,
                           int* discarded);
+
+/* After a warm-started solve of right-hand side `rhs` with a discard test
+ * (warm_discard_ratio > 0): the ROI energies of the cold start's initial
+ * residual (Nw^2 diff_energy(1)) and of the warm start's (see
+ * warm_discard_ratio).  -1 when no test ran.  No counterpart in the
+ * reference. */
+int ws_solver_warm_residual(ws_solver s, int64_t rhs, double* cold_residual_energy, double* warm_residual_energy);
 
 /* Autotuner (no counterpart in the reference): times the kernel layouts the
  * solver's grid supports - the power-of-two fast kernels or the generic

@@ -81,15 +81,38 @@ def test_perturbed_start_is_faster_and_as_accurate(gpu):
     assert rel(Ew, Einf) <= 1.5 * rel(E, Einf) + 1e-4, (rel(Ew, Einf), rel(E, Einf))
 
 
-def test_bad_start_is_discarded_after_one_cycle(gpu):
+def test_bad_start_is_discarded_before_its_first_cycle(gpu):
+    """A start whose initial residual is far worse than the cold start's is
+    given up after the residual probe, before any warm iteration, and the
+    solve reruns cold: the cold loop's result and iteration count."""
     sim, src = _problem(1e-4)
     E, st = sim.exec(src)
     rng = np.random.default_rng(0)
     noise = 50 * np.abs(E).max() * (rng.standard_normal(E.shape) + 1j * rng.standard_normal(E.shape))
     Eb, sb = sim.exec(src, warm_start=noise)
-    assert sb.warm_discarded and sb.warm_cycle_energy > sim.warm_discard_ratio * sb.cold_first_energy
-    assert sb.warm_iterations == len(sim.wiggles)
+    assert sb.warm_discarded and sb.warm_residual_energy > sim.warm_discard_ratio * sb.cold_residual_energy
+    assert sb.warm_iterations == 0
     assert sb.it == st.it and rel(Eb, E) < 1e-6
+
+
+def test_discard_rule_is_the_cold_start_residual(gpu):
+    """The rule compares initial residuals: r(u) = T(u, S) - u against
+    r(0) = Nw times the probe increment.  For u = c E'_inf (E'_inf the
+    loop's limit, whose residual is ~0) the residual is ~(1 - c) r(0), of
+    energy (1 - c)^2 times the cold one.  c = -0.22 gives ~1.5x: discarded,
+    although it is below the 2x a first-cycle rule with a factor-2 margin
+    would allow; c = 0.5 gives ~0.25x: kept.  The measured residual energies
+    follow (1 - c)^2 to within the single-wiggle residual of the limit, and
+    the zero start has exactly the cold residual (kept)."""
+    sim, src = _problem(1e-4)
+    Ep, _ = _problem(1e-9)[0].exec(src, output="eprime")
+    psi = _psi_full(sim, Ep)
+    for c, discard in ((-0.22, True), (0.5, False), (0.0, False)):
+        E, st = sim.exec(src, warm_start=c * psi)
+        ratio = st.warm_residual_energy / st.cold_residual_energy
+        assert ratio == pytest.approx((1 - c) ** 2, rel=0.2), (c, ratio)
+        assert st.warm_discarded == discard, (c, ratio)
+        assert st.converged
 
 
 def test_discard_can_be_switched_off(gpu):

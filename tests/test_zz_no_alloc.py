@@ -90,10 +90,28 @@ def run_noalloc(sim, source, maxit, torch):
 
 
 CASES = {
-    "2d_disordered": (lambda rng: 1.0 + 0.3 * rng.random((96, 80)) + 0.01j, [16, 16], (48, 40)),
-    "2d_mixed_radix": (lambda rng: 1.0 + 0.2 * rng.random((45, 60)), [5, 7], (23, 31)),
-    "3d_spheres": (lambda rng: np.where(rng.random((32, 32, 32)) < 0.1, 1.5, 1.33), [16, 16, 16], (1, 1, 1)),
+    # name: (medium, boundary widths, source position, vector, energy threshold, max iterations)
+    "2d_disordered": (lambda rng: 1.0 + 0.3 * rng.random((96, 80)) + 0.01j, [16, 16], (48, 40), False, 1e-3, 2000),
+    "2d_mixed_radix": (lambda rng: 1.0 + 0.2 * rng.random((45, 60)), [5, 7], (23, 31), False, 1e-3, 2000),
+    "3d_spheres": (lambda rng: np.where(rng.random((32, 32, 32)) < 0.1, 1.5, 1.33), [16, 16, 16], (1, 1, 1),
+                   False, 1e-3, 2000),
+    # 128^3: the fast 128^2 planes on a cluster of 2 blocks (about 32 MiB of scratch)
+    "3d_128_cluster": (lambda rng: np.where(rng.random((96, 96, 96)) < 0.1, 1.5, 1.33), [16, 16, 16], (1, 1, 1),
+                       False, 1e-99, 24),
+    # 48^3 x 3: vector fields on the generic mixed-radix kernels
+    "3d_vector_48": (lambda rng: np.where(rng.random((32, 32, 32)) < 0.1, 1.5, 1.33), [8, 8, 8], (1, 1, 1, 1),
+                     True, 1e-3, 2000),
 }
+
+
+def make_sim(ws, name):
+    make_n, bw, pos, vector, thr, maxit = CASES[name]
+    rng = np.random.default_rng(11)
+    n = make_n(rng)
+    opt = {"lambda": 1.0, "pixel_size": 0.25, "boundary_widths": bw, "energy_threshold": thr}
+    sim = (ws.WaveSimVector if vector else ws.WaveSim)(n, opt)
+    val = np.ones(n.shape[:2]) if n.ndim == 3 else 1.0
+    return n, opt, sim, (val, list(pos)), vector, maxit
 
 
 @pytest.mark.parametrize("name", list(CASES))
@@ -101,20 +119,54 @@ def test_noalloc_matches_allocating_entry_twice(gpu, name):
     import torch
 
     import wavesim_b200 as ws
-    make_n, bw, pos = CASES[name]
-    rng = np.random.default_rng(11)
-    n = make_n(rng)
-    opt = {"lambda": 1.0, "pixel_size": 0.25, "boundary_widths": bw, "energy_threshold": 1e-3}
-    sim = ws.WaveSim(n, opt)
-    val = np.ones(n.shape[:2]) if n.ndim == 3 else 1.0
-    source = ws.Source(val, list(pos))
-    maxit = 2000
+    n, opt, sim, (val, pos), vector, maxit = make_sim(ws, name)
+    source = ws.Source(val, pos)
     E_ref, n_ref, h_ref = run_allocating(sim, source, maxit)
     for _ in range(2):
         E, n_it, hist = run_noalloc(sim, source, maxit, torch)
         assert n_it == n_ref
         assert rel(E, E_ref) < TOL
         np.testing.assert_allclose(hist, h_ref, rtol=1e-5)
+
+
+def test_noalloc_near_the_scratch_limit_matches_oracle(gpu):
+    """A 320 x 7680 2-D grid (2.46 million elements, 39.3 of the 40 MiB)
+    through the generic mixed-radix columns: Ny = 320 does not divide the
+    8192 elements a block can hold, so the column count per block is capped
+    by the kernel's element limit, not by shared memory.  Two calls in a row
+    against the allocating entry point, and the field against the FP32
+    oracle after the same 16 iterations."""
+    import torch
+
+    import wavesim_b200 as ws
+    from oracle import mbs_oracle as ref
+    rng = np.random.default_rng(5)
+    n = 1.0 + 0.2 * rng.random((288, 7648)) + 0.01j
+    opt = {"lambda": 1.0, "pixel_size": 0.25, "boundary_widths": [16, 16], "energy_threshold": 1e-99}
+    sim = ws.WaveSim(n, opt)
+    assert tuple(int(v) for v in sim.N[:2]) == (320, 7680)
+    assert 16 * int(np.prod(sim.N)) < _lib_scratch_bytes()
+    pos = [144, 3000]
+    source = ws.Source(1.0, pos)
+    maxit = 16
+    E_ref, n_ref, h_ref = run_allocating(sim, source, maxit)
+    for _ in range(2):
+        E, n_it, hist = run_noalloc(sim, source, maxit, torch)
+        assert n_it == n_ref == maxit
+        assert rel(E, E_ref) < TOL
+        np.testing.assert_allclose(hist, h_ref, rtol=1e-5)
+    Eo, so = ref.WaveSim(n, opt).exec(ref.Source(1.0, pos), max_iterations=maxit)
+    assert so.it - 1 == maxit
+    # E' -> E = E' / gamma on the roi, as WaveSimBase.m:150-153 does
+    Ef = E.reshape(tuple(int(v) for v in sim.N), order="F")[..., 0, 0] / sim.gamma[..., 0]
+    r0 = sim.roi[0]
+    Ef = Ef[r0[0] - 1:r0[0] - 1 + 288, r0[1] - 1:r0[1] - 1 + 7648]
+    assert rel(Ef, np.squeeze(Eo)) < TOL
+
+
+def _lib_scratch_bytes():
+    from wavesim_b200 import _lib
+    return int(_lib.lib.ws_noalloc_scratch_bytes())
 
 
 def test_noalloc_rejects_oversize_grid(gpu):

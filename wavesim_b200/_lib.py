@@ -70,7 +70,7 @@ EXPORTS = [
     "ws_run_algorithm_release",
     "ws_solver_create", "ws_solver_solve", "ws_solver_solve_batch", "ws_solver_solve_plane_waves", "ws_solver_buffers",
     "ws_solver_time_kernels",
-    "ws_solver_launches_per_iteration", "ws_solver_time_fused", "ws_solver_warm_report", "ws_solver_autotune", "ws_solver_destroy",
+    "ws_solver_launches_per_iteration", "ws_solver_set_wait_limit", "ws_solver_time_fused", "ws_solver_warm_report", "ws_solver_warm_residual", "ws_solver_autotune", "ws_solver_destroy",
     "ws_run_algorithm_noalloc", "ws_medium_reduce", "ws_build_gamma", "ws_setup_last_error",
     "ws_noalloc_scratch_bytes", "ws_noalloc_last_error",
     "ws_pstd_default_options", "ws_pstd_create", "ws_pstd_run", "ws_pstd_destroy",
@@ -127,6 +127,8 @@ def _load():
     lib.ws_solver_buffers.restype = C.c_int
     lib.ws_solver_time_kernels.argtypes = [P, C.c_int, C.POINTER(C.c_float), C.POINTER(C.c_double)]
     lib.ws_solver_time_kernels.restype = C.c_int
+    lib.ws_solver_set_wait_limit.argtypes = [P, C.c_int64]
+    lib.ws_solver_set_wait_limit.restype = C.c_int
     lib.ws_solver_launches_per_iteration.argtypes = [P]
     lib.ws_solver_launches_per_iteration.restype = C.c_int
     lib.ws_solver_time_fused.argtypes = [P, C.c_int, C.POINTER(C.c_float), C.POINTER(C.c_double)]
@@ -134,6 +136,8 @@ def _load():
     lib.ws_solver_warm_report.argtypes = [P, C.c_int64, C.POINTER(C.c_double), C.POINTER(C.c_double),
                                           C.POINTER(C.c_int)]
     lib.ws_solver_warm_report.restype = C.c_int
+    lib.ws_solver_warm_residual.argtypes = [P, C.c_int64, C.POINTER(C.c_double), C.POINTER(C.c_double)]
+    lib.ws_solver_warm_residual.restype = C.c_int
     lib.ws_solver_autotune.argtypes = [P, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_float), C.POINTER(C.c_float)]
     lib.ws_solver_autotune.restype = C.c_int
     i64a = C.POINTER(C.c_int64)

@@ -66,6 +66,7 @@ struct DevState {
   int diff1_locked;         // diff1 comes from the cold probe iteration; iteration 1 keeps it
   int discarded;            // given up at the end of the first wiggle cycle
   double warm_e;            // ROI energy of the true increment dE'_Nw of a warm start
+  double warm_r;            // ROI energy of the warm start's initial residual (k_warm_resid_energy)
 };
 
 struct StopRule {
@@ -113,6 +114,8 @@ struct OuterArgs {
   int pf;       // fast kernels: block b pulls the inputs of block b + pf into L2 (0: off)
   int pstd;     // 1: PSTD Laplacian -(px^2 + py^2 + pz^2) / N instead of the Green's function
                 // (k02e = 0), and the output conjugated (scalar fields only)
+  long long wait_clocks;  // TMA pencils: clocks a tile load may take before the block gives up
+                          // (<= 0: the default bound)
 };
 
 __device__ __forceinline__ int load_done(const DevState* st) { return __ldcg(&st->done); }
@@ -466,6 +469,7 @@ static __global__ void k_reset_state(DevState* st, int n) {
     s->diff1_locked = 0;
     s->discarded = 0;
     s->warm_e = 0.0;
+    s->warm_r = 0.0;
   }
 }
 
@@ -545,15 +549,62 @@ static __global__ void __launch_bounds__(256) k_warm_shift(float2* __restrict__ 
   }
 }
 
-// A warm start whose true increment energy after its first cycle exceeds
-// ratio x diff_energy(1) (NaN included) is worse than starting from zero: it
-// stops here, unconverged and marked discarded, so that the caller reruns
-// it cold having paid for one cycle only.  ratio <= 0 keeps every start.
-static __global__ void k_warm_check(DevState* st, int n, double ratio) {
+// The initial residual of a warm start (no counterpart in the reference).
+// With the whole source S (its Nw per-iteration parts A S summed) the loop is
+// the Richardson iteration E'_k = T_w(E'_(k-1), Nw A S), T_w(x, s) =
+// f_mix(x, G'_w(x + s)); a start u = Nw v has the residual
+// r(u) = T_1(u, Nw A S) - u, and the cold start r(0) = Nw T_1(0, A S), Nw
+// times the probe iteration's increment, of ROI energy Nw^2 diff_energy(1).
+// k_warm_resid_begin sets dE' = u, one iteration with the source scaled by Nw
+// follows (K1, K2, K3, no stop rule), and k_warm_resid_energy sums
+// |dE' - u|^2 over the ROI into warm_r of right-hand side blockIdx.y.
+static __global__ void k_warm_resid_begin(float2* __restrict__ dE, const float2* __restrict__ v, long long n,
+                                          float nw) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+    dE[i] = make_float2(v[i].x * nw, v[i].y * nw);
+}
+
+static __global__ void __launch_bounds__(256) k_warm_resid_energy(const float2* __restrict__ dE,
+                                                                  const float2* __restrict__ v, Geom g,
+                                                                  long long fstride, float nw, DevState* st) {
+  const int r = blockIdx.y;
+  dE += (long long)r * fstride;
+  v += (long long)r * fstride;
+  float acc = 0.f;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < fstride; i += (long long)gridDim.x * blockDim.x) {
+    long long k = i;
+    const int y = (int)(k % g.ny); k /= g.ny;
+    const int x = (int)(k % g.nx); k /= g.nx;
+    const int z = (int)(k % g.nz);
+    const int c = (int)(k / g.nz);
+    if (y >= g.r0[0] && y < g.r1[0] && x >= g.r0[1] && x < g.r1[1] && z >= g.r0[2] && z < g.r1[2] && c >= g.r0[3] &&
+        c < g.r1[3]) {
+      const float2 d = make_float2(dE[i].x - nw * v[i].x, dE[i].y - nw * v[i].y);
+      acc = fmaf(d.x, d.x, fmaf(d.y, d.y, acc));
+    }
+  }
+  __shared__ float red[8];
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = acc;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    float t = 0.f;
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t += red[w];
+    atomicAdd(&st[r].warm_r, (double)t);
+  }
+}
+
+// A warm start whose initial residual is worse than the cold start's (ROI
+// energy above ratio x Nw^2 diff_energy(1), with 1e-3 of slack for rounding:
+// a zero start has exactly the cold residual) is given up before its first
+// cycle: the right-hand side stops unconverged, marked discarded, and the
+// caller reruns it cold.  ratio <= 0 keeps every start.
+static __global__ void k_warm_check(DevState* st, int n, double ratio, double nw2) {
   for (int r = threadIdx.x; r < n; r += blockDim.x) {
     DevState* d = st + r;
     if (ratio <= 0.0 || d->done) continue;
-    if (!(d->warm_e <= ratio * d->diff1)) {
+    if (!(d->warm_r <= ratio * nw2 * d->diff1 * (1.0 + 1e-3))) {
       d->done = 1;
       d->converged = 0;
       d->discarded = 1;

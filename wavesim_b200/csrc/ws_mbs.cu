@@ -408,6 +408,7 @@ struct Solver {
   int fuse = 0;                  // the loop runs K3 of each iteration fused with K1 of the next
   LayoutChoice tuned{};          // the autotuner's choice (all zero: the heuristics)
   double warm_ratio = 0.0;       // discard threshold of the current solve
+  long long wait_clocks = 0;     // bound of the TMA pencils' tile waits (0: the default)
   float2* d_tw = nullptr;
   FftPlan py{}, pxl{}, po{};
   const float2* twx = nullptr;
@@ -758,12 +759,14 @@ static OuterArgs outer_args(const Solver* s, int w) {
   a.fstride = (long long)field_elems(s);
   a.pf = 0;  // K2 measured slower with it
   a.pstd = s->pstd;
+  a.wait_clocks = s->wait_clocks;
   return a;
 }
 
 template <int RS>
-static cudaError_t launch_k1_t(const Solver* s, int w, const float2* in, const float2* src, float2* out) {
-  const float2 A = make_float2(0.f, (float)(1.0f / s->eps / (float)s->nw));  // 1i/epsilon/Nwiggles
+static cudaError_t launch_k1_t(const Solver* s, int w, const float2* in, const float2* src, float2* out,
+                              float a_mult) {
+  const float2 A = make_float2(0.f, a_mult * (float)(1.0f / s->eps / (float)s->nw));  // 1i/epsilon/Nwiggles
   cudaLaunchConfig_t cfg{};
   cfg.gridDim = dim3((unsigned)(s->lay.grid_inner * s->nrhs));
   cfg.blockDim = dim3(s->lay.th_inner);
@@ -826,18 +829,23 @@ static cudaError_t launch_fast_inner(const Solver* s, const void* fn, void** arg
   return cudaLaunchKernelExC(&cfg, fn, args);
 }
 
-// K1 on explicit buffers: out = inner FFT of (in + A src) times the ramps of wiggle w
-static cudaError_t launch_k1_io(const Solver* s, int w, const float2* in, const float2* src, float2* out) {
+// K1 on explicit buffers: out = inner FFT of (in + a_mult A src) times the
+// ramps of wiggle w (A = i/epsilon/Nw, the reference's per-iteration share of
+// the source; a_mult = Nw gives the whole source, for the warm start's
+// residual probe)
+static cudaError_t launch_k1_io(const Solver* s, int w, const float2* in, const float2* src, float2* out,
+                                float a_mult = 1.f) {
   if (s->lay.fi) {
     InnerArgs a = inner_args(s, w);
     a.ncols = s->lay.ncols;
     a.pf = s->pf_inner;  // K1 only: its loads come first, so the next wave's columns are worth pulling early
-    float2 A = make_float2(0.f, (float)(1.0f / s->eps / (float)s->nw));
+    float2 A = make_float2(0.f, a_mult * (float)(1.0f / s->eps / (float)s->nw));
     const DevState* st = s->d_state;
     void* args[] = {&a, &in, &src, &A, &out, &st};
     return launch_fast_inner(s, s->lay.fi->fwd, args);
   }
-  return s->lay.rset == kPow2 ? launch_k1_t<kPow2>(s, w, in, src, out) : launch_k1_t<kMixed>(s, w, in, src, out);
+  return s->lay.rset == kPow2 ? launch_k1_t<kPow2>(s, w, in, src, out, a_mult)
+                              : launch_k1_t<kMixed>(s, w, in, src, out, a_mult);
 }
 static cudaError_t launch_k1(const Solver* s, int w, bool with_source) {
   return launch_k1_io(s, w, s->d_dE, with_source ? s->d_src : nullptr, s->d_T);
@@ -1052,8 +1060,9 @@ static int ensure_hist(Solver* s, long long cap) {
 // The prologue and first wiggle cycle of a solve (with the source).  Cold:
 // the reference's iterations 1..Nw from E' = dE' = 0.  Warm (d_init holds
 // v = u/Nw, see k_warm_scale): a cold probe iteration for diff_energy(1),
-// the restart from dE' = v, E' = 0, iterations 1..Nw with the source, the
-// shift dE' -= v and the discard check.
+// the residual probe of the start and the discard check (k_warm_resid_*,
+// k_warm_check), the restart from dE' = v, E' = 0, iterations 1..Nw with the
+// source and the shift dE' -= v.
 static cudaError_t launch_prologue(const Solver* s, const StopRule& rule, const Hist& h) {
   const size_t nbytes = field_elems(s) * s->nrhs * sizeof(float2);
   cudaError_t e;
@@ -1065,8 +1074,23 @@ static cudaError_t launch_prologue(const Solver* s, const StopRule& rule, const 
     if ((e = launch_iteration(s, 0, true, rule, h)) != cudaSuccess) return e;  // the probe
     const long long n = (long long)field_elems(s) * s->nrhs;
     const unsigned blocks = (unsigned)std::min<long long>((n + 255) / 256, 8 * kNumSms);
+    const float nw = (float)s->nw;
+    if (s->warm_ratio > 0.0) {
+      // residual of the start: one iteration from dE' = u with the whole source
+      k_warm_resid_begin<<<blocks, 256, 0, s->stream>>>(s->d_dE, s->d_init, n, nw);
+      if ((e = cudaGetLastError()) != cudaSuccess) return e;
+      if ((e = launch_k1_io(s, 0, s->d_dE, s->d_src, s->d_T, nw)) != cudaSuccess) return e;
+      if ((e = launch_k2(s, 0)) != cudaSuccess) return e;
+      if ((e = launch_k3_only(s, 0)) != cudaSuccess) return e;
+      const long long fe = (long long)field_elems(s);
+      const unsigned bpr = (unsigned)std::max<long long>(1, std::min<long long>((fe + 255) / 256, 4 * kNumSms));
+      k_warm_resid_energy<<<dim3(bpr, s->nrhs), 256, 0, s->stream>>>(s->d_dE, s->d_init, s->g, fe, nw,
+                                                                     s->d_state);
+    }
     k_warm_begin<<<blocks, 256, 0, s->stream>>>(s->d_dE, s->d_E, s->d_init, n);
     k_warm_restart<<<1, 256, 0, s->stream>>>(s->d_state, s->nrhs);
+    if (s->warm_ratio > 0.0)
+      k_warm_check<<<1, 256, 0, s->stream>>>(s->d_state, s->nrhs, s->warm_ratio, (double)s->nw * s->nw);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
   }
   if (s->fuse) {
@@ -1083,7 +1107,6 @@ static cudaError_t launch_prologue(const Solver* s, const StopRule& rule, const 
     const long long fe = (long long)field_elems(s);
     const unsigned bpr = (unsigned)std::max<long long>(1, std::min<long long>((fe + 255) / 256, 4 * kNumSms));
     k_warm_shift<<<dim3(bpr, s->nrhs), 256, 0, s->stream>>>(s->d_dE, s->d_init, s->g, fe, s->d_state);
-    k_warm_check<<<1, 256, 0, s->stream>>>(s->d_state, s->nrhs, s->warm_ratio);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
     // the shift changed dE': the fused loop's T is recomputed from it
     if (s->fuse && (e = launch_k1(s, 0, false)) != cudaSuccess) return e;
@@ -1368,7 +1391,7 @@ static int solve_batch(Solver* s, int nrhs, const int64_t* counts, const ws_sour
   WS_CUDA(cudaStreamSynchronize(s->stream));
   if (kerr) {
     cudaMemset(s->d_err, 0, sizeof(int));
-    return fail(WS_ERR_CUDA, "a cluster exchange of the FFT kernels timed out");
+    return fail(WS_ERR_CUDA, "a bounded wait of the FFT kernels (cluster exchange or TMA tile load) timed out");
   }
   bool diverged = false;
   for (int r = 0; r < nrhs; ++r) {
@@ -1512,6 +1535,15 @@ int ws_solver_buffers(ws_solver h, void** E_prime, void** stream) {
   return WS_OK;
 }
 
+int ws_solver_set_wait_limit(ws_solver h, int64_t clocks) {
+  if (!h) return fail(WS_ERR_INVALID_ARGUMENT, "null solver");
+  if (clocks < 0) return fail(WS_ERR_INVALID_ARGUMENT, "clocks must be >= 0");
+  Solver* s = reinterpret_cast<Solver*>(h);
+  if (s->wait_clocks != (long long)clocks) free_graph(s);  // the graph holds the kernels' arguments
+  s->wait_clocks = (long long)clocks;
+  return WS_OK;
+}
+
 int ws_solver_launches_per_iteration(ws_solver h) {
   if (!h) return 0;
   return reinterpret_cast<Solver*>(h)->fuse ? 3 : 4;  // (K1,) K2, K3 or K3 + next K1, stop rule
@@ -1608,6 +1640,19 @@ int ws_solver_warm_report(ws_solver h, int64_t rhs, double* cold_first_energy, d
   if (cold_first_energy) *cold_first_energy = st.diff1;
   if (warm_cycle_energy) *warm_cycle_energy = s->warm ? st.warm_e : -1.0;
   if (discarded) *discarded = s->warm ? st.discarded : 0;
+  return WS_OK;
+}
+
+int ws_solver_warm_residual(ws_solver h, int64_t rhs, double* cold_residual_energy, double* warm_residual_energy) {
+  if (!h) return fail(WS_ERR_INVALID_ARGUMENT, "null solver");
+  Solver* s = reinterpret_cast<Solver*>(h);
+  if (rhs < 0 || rhs >= s->nrhs) return fail(WS_ERR_INVALID_ARGUMENT, "right-hand side out of range");
+  WS_CUDA(cudaSetDevice(s->device));
+  DevState st{};
+  WS_CUDA(cudaMemcpy(&st, s->d_state + rhs, sizeof(DevState), cudaMemcpyDeviceToHost));
+  const bool have = s->warm && s->warm_ratio > 0.0;
+  if (cold_residual_energy) *cold_residual_energy = have ? (double)s->nw * s->nw * st.diff1 : -1.0;
+  if (warm_residual_energy) *warm_residual_energy = have ? st.warm_r : -1.0;
   return WS_OK;
 }
 

@@ -28,6 +28,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <mutex>
 #include <string>
 
 #include "wavesim_b200.h"
@@ -44,6 +45,7 @@ static __device__ __align__(256) unsigned char g_ws_scratch[kScratchBytes];
 
 static void* g_scratch_addr[kMaxDevices] = {};  // device address of g_ws_scratch per device
 static bool g_attrs_set[kMaxDevices] = {};
+static std::mutex g_setup_mutex;  // guards the two tables above
 
 thread_local std::string t_error;
 static int fail(int code, const std::string& m) {
@@ -163,6 +165,8 @@ static int shape_for(const Geom& g, Shape& s) {
       if (g.nx % c) continue;
       const long long cols = g.nx / c;
       if (cols * g.ny > (long long)lim_threads * emax || cols * colb > budget) continue;
+      FftPlan tmp{};
+      if (c > 1 && !plan((int)cols, tmp)) continue;  // the x-local length must have a radix schedule
       best = c;
       break;
     }
@@ -175,7 +179,11 @@ static int shape_for(const Geom& g, Shape& s) {
   } else {
     if ((long long)g.ny > (long long)lim_threads * emax || colb > budget) return WS_ERR_UNSUPPORTED;
     const long long total = (long long)g.nx * g.nc;
-    long long want = std::max(1LL, std::min((long long)(budget / colb), (8192LL + g.ny - 1) / g.ny));
+    // a block holds at most lim_threads x emax elements: the FFT stages of the
+    // generic kernels cover no more butterflies than that
+    const long long max_cols_fit =
+        std::max(1LL, std::min((long long)(budget / colb), (long long)lim_threads * emax / (long long)g.ny));
+    long long want = std::max(1LL, std::min(max_cols_fit, (8192LL + g.ny - 1) / g.ny));
     while (want > 1 && (total + want - 1) / want < 296) want /= 2;
     s.ncols = (int)want;
     s.th = threads_for(want * g.ny);
@@ -355,7 +363,7 @@ extern "C" int ws_run_algorithm_noalloc(const int64_t N[4], const ws_complex* ga
   const size_t field = (size_t)g.npts * g.nc;
   const size_t ntw = (size_t)g.ny + g.nx + nxl + no;
   const size_t need = 2 * field * sizeof(float2) + ntw * sizeof(float2) + 256 + sizeof(DevState) + 256 +
-                      (size_t)sh.grid_inner * sizeof(double);
+                      (size_t)sh.grid_inner * sizeof(double) + 256 + sizeof(int);
   if (need > kScratchBytes)
     return fail(WS_ERR_INVALID_ARGUMENT, "grid too large for the static scratch array (" +
                                              std::to_string(need) + " > " + std::to_string(kScratchBytes) +
@@ -364,12 +372,18 @@ extern "C" int ws_run_algorithm_noalloc(const int64_t N[4], const ws_complex* ga
   int dev = 0;
   NA_CUDA(cudaGetDevice(&dev));
   if (dev < 0 || dev >= kMaxDevices) return fail(WS_ERR_INVALID_ARGUMENT, "device ordinal above 63");
-  if (!g_scratch_addr[dev]) {
-    void* p = nullptr;
-    NA_CUDA(cudaGetSymbolAddress(&p, g_ws_scratch));  // device address of the array on this device
-    g_scratch_addr[dev] = p;
+  int rc = WS_OK;
+  {
+    // the per-device lookup runs once; the lock keeps two host threads that
+    // make their first call on a device at the same time from racing on it
+    std::lock_guard<std::mutex> lock(g_setup_mutex);
+    if (!g_scratch_addr[dev]) {
+      void* p = nullptr;
+      NA_CUDA(cudaGetSymbolAddress(&p, g_ws_scratch));  // device address of the array on this device
+      g_scratch_addr[dev] = p;
+    }
+    rc = set_attributes(dev);
   }
-  int rc = set_attributes(dev);
   if (rc) return rc;
   cudaStream_t s = (cudaStream_t)stream;
   char* base = (char*)g_scratch_addr[dev];
@@ -381,6 +395,8 @@ extern "C" int ws_run_algorithm_noalloc(const int64_t N[4], const ws_complex* ga
   float2* tw = r.T + field;
   r.st = (DevState*)(((uintptr_t)(tw + ntw) + 255) & ~(uintptr_t)255);
   r.partials = (double*)(((uintptr_t)(r.st + 1) + 255) & ~(uintptr_t)255);
+  // set by a fast kernel whose bounded cluster or barrier wait gave up
+  int* d_err = (int*)(((uintptr_t)(r.partials + sh.grid_inner) + 255) & ~(uintptr_t)255);
   r.E = (float2*)E_out;
   r.src = (float2*)source_field;
   r.gamma = (const float2*)gamma;
@@ -402,6 +418,7 @@ extern "C" int ws_run_algorithm_noalloc(const int64_t N[4], const ws_complex* ga
   // clear what must start at zero: dE, E (the caller's output), the loop state
   NA_CUDA(cudaMemsetAsync(r.dE, 0, field * sizeof(float2), s));
   NA_CUDA(cudaMemsetAsync(r.E, 0, field * sizeof(float2), s));
+  NA_CUDA(cudaMemsetAsync(d_err, 0, sizeof(int), s));
   k_reset_state<<<1, 32, 0, s>>>(r.st, 1);
   NA_CUDA(cudaGetLastError());
   Wig wig[64];
@@ -419,6 +436,7 @@ extern "C" int ws_run_algorithm_noalloc(const int64_t N[4], const ws_complex* ga
   r.ia.ncols = sh.ncols;
   r.ia.bpr = (int)sh.grid_inner;  // a single right-hand side
   r.ia.fstride = 0;
+  r.ia.err = d_err;
   r.oa.g = g;
   r.oa.po = po;
   r.oa.k02e = make_float2(k02e.re, k02e.im);
@@ -438,12 +456,15 @@ extern "C" int ws_run_algorithm_noalloc(const int64_t N[4], const ws_complex* ga
   const float2 A = make_float2(0.f, (float)(1.0f / epsilon / (float)n_wiggles));
   const long long max_cycles = (max_iterations + n_wiggles - 1) / n_wiggles + 1;
   DevState hs{};
+  int kerr = 0;
   long long it = 0;
   for (long long cycle = 0;; ++cycle) {
     if (cycle >= max_cycles) return fail(WS_ERR_CUDA, "loop did not stop within max_iterations (internal error)");
     for (int i = 0; i < n_wiggles; ++i, ++it) NA_CUDA(iteration(r, i, wig, it < n_wiggles, A, rule, h));
     NA_CUDA(cudaMemcpyAsync(&hs, r.st, sizeof(DevState), cudaMemcpyDeviceToHost, s));
+    NA_CUDA(cudaMemcpyAsync(&kerr, d_err, sizeof(int), cudaMemcpyDeviceToHost, s));
     NA_CUDA(cudaStreamSynchronize(s));
+    if (kerr) return fail(WS_ERR_CUDA, "a cluster exchange of the FFT kernels timed out");
     if (hs.done) break;
   }
   if (n_iterations) *n_iterations = hs.it - 1;

@@ -13,8 +13,9 @@
 //          is reloaded only after the store that reads it has read it
 //          (cp.async.bulk.wait_group.read)
 // The tensor map spans this GPU's own T only (no multicast).  Every wait is
-// bounded: a block whose load does not arrive in ~5e7 clocks sets *err,
-// drains its copies (bounded again) and returns.
+// bounded: a block whose load does not arrive in a.wait_clocks clocks (5e7 by
+// default) sets *err, drains its copies (with the default bound, so that no
+// copy outlives its block) and returns.
 #pragma once
 #include <cuda.h>
 
@@ -43,8 +44,10 @@ __device__ __forceinline__ void expect_bytes(uint64_t* bar, uint32_t bytes) {
   asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(fast::smem_addr(bar)), "r"(bytes)
                : "memory");
 }
-// phase with parity `parity` of the barrier complete; false after ~5e7 clocks
-__device__ __forceinline__ bool wait_parity(uint64_t* bar, uint32_t parity) {
+constexpr long long kWaitClocks = 50000000LL;  // ~25 ms at 2 GHz: the default bound of every wait
+
+// phase with parity `parity` of the barrier complete; false after `limit` clocks
+__device__ __forceinline__ bool wait_parity(uint64_t* bar, uint32_t parity, long long limit = kWaitClocks) {
   const uint32_t a = fast::smem_addr(bar);
   const long long t0 = clock64();
   while (true) {
@@ -57,7 +60,7 @@ __device__ __forceinline__ bool wait_parity(uint64_t* bar, uint32_t parity) {
         : "r"(a), "r"(parity)
         : "memory");
     if (done) return true;
-    if (clock64() - t0 > 50000000LL) return false;
+    if (clock64() - t0 > limit) return false;
   }
 }
 
@@ -123,7 +126,7 @@ __global__ void __launch_bounds__(PencilTile<NO, TY, S>::kThreads, 2)
     const int b = i % S;
     const int t = blockIdx.x + i * G;
     float2* const buf = buf0 + b * NO * TY;
-    ok = wait_parity(&full[b], (uint32_t)((i / S) & 1));
+    ok = wait_parity(&full[b], (uint32_t)((i / S) & 1), a.wait_clocks > 0 ? a.wait_clocks : kWaitClocks);
     if (__syncthreads_or(!ok)) {
       ok = false;
       break;
@@ -253,7 +256,7 @@ __global__ void __launch_bounds__(VecPencilTile<PL, TY, S>::kThreads, 1)
   for (; i < mine; ++i) {
     const int b = i % S;
     const int t = blockIdx.x + i * G;
-    ok = wait_parity(&full[b], (uint32_t)((i / S) & 1));
+    ok = wait_parity(&full[b], (uint32_t)((i / S) & 1), a.wait_clocks > 0 ? a.wait_clocks : kWaitClocks);
     if (__syncthreads_or(!ok)) {
       ok = false;
       break;

@@ -77,7 +77,9 @@ class WaveSim:
         self.stop_rule = o.get("stop_rule", "reference")
         self.device = int(o.get("device", 0))
         self.use_graph = bool(o.get("use_graph", True))
-        self.warm_discard_ratio = o.get("warm_discard_ratio", None)  # None: 2 Nw (set with the wiggles)
+        # a warm start whose initial residual is worse than the cold start's is
+        # discarded (ratio 1); 0 keeps every start
+        self.warm_discard_ratio = float(o.get("warm_discard_ratio", 1.0))
 
         # device_setup: e_r, V, the ARL window and gamma are built on the GPU
         # (wavesim_b200/csrc/ws_setup.cu) instead of in NumPy; same values
@@ -112,12 +114,6 @@ class WaveSim:
         self.epsilon = np.float32(eps)
         self.k0, self.k0c = k0, k0c
         self.wiggles, self.ACC = self._wiggles(o.get("ACC", True))
-        # a zero start (the cold loop) carries about Nw times the first
-        # increment's energy at the end of its first cycle: starts above twice
-        # that are worse than no start
-        if self.warm_discard_ratio is None:
-            self.warm_discard_ratio = 2.0 * len(self.wiggles)
-        self.warm_discard_ratio = float(self.warm_discard_ratio)
         if self.vector:
             if o.get("roi") is None:
                 self.roi[1, 3] = 3  # WaveSimVector.m:14-16
@@ -365,10 +361,11 @@ class WaveSim:
         on the device.  The loop starts from it, injected over the first
         wiggle cycle as the reference injects its source, and runs to the
         same energy tolerance against the cold first-iteration energy.  A
-        start whose true increment after the first cycle carries more than
-        warm_discard_ratio (option, default 2 Nw) times the energy of the
-        cold first increment is given up there and the solve reruns cold
-        (state.warm_discarded; state.time covers both)."""
+        start whose initial residual is worse than the cold start's (ROI
+        energy above warm_discard_ratio, option, default 1, times the cold
+        start's) is given up before its first cycle and the solve reruns
+        cold (state.warm_discarded; state.time covers both;
+        state.cold_residual_energy, state.warm_residual_energy)."""
         if output not in ("field", "eprime"):
             raise ValueError("output must be 'field' or 'eprime'")
         t0 = time.perf_counter()
@@ -415,10 +412,14 @@ class WaveSim:
             _lib.check(_lib.lib.ws_solver_warm_report(h, 0, C.byref(cold), C.byref(warm), C.byref(disc)))
             state.cold_first_energy, state.warm_cycle_energy = cold.value, warm.value
             state.warm_discarded = bool(disc.value)
+            rc_, rw_ = C.c_double(), C.c_double()
+            _lib.check(_lib.lib.ws_solver_warm_residual(h, 0, C.byref(rc_), C.byref(rw_)))
+            state.cold_residual_energy, state.warm_residual_energy = rc_.value, rw_.value
             del init
             if state.warm_discarded:
                 E, st2 = self.exec(source, output=output)
-                st2.cold_first_energy, st2.warm_cycle_energy = state.cold_first_energy, state.warm_cycle_energy
+                for k in ("cold_first_energy", "warm_cycle_energy", "cold_residual_energy", "warm_residual_energy"):
+                    setattr(st2, k, getattr(state, k))
                 st2.warm_discarded, st2.warm_iterations = True, state.it - 1
                 st2.time = time.perf_counter() - t0
                 return E, st2
@@ -492,6 +493,9 @@ class WaveSim:
                 _lib.check(_lib.lib.ws_solver_warm_report(h, i, C.byref(cold), C.byref(warm), C.byref(disc)))
                 states[i].cold_first_energy, states[i].warm_cycle_energy = cold.value, warm.value
                 states[i].warm_discarded = bool(disc.value)
+                rc_, rw_ = C.c_double(), C.c_double()
+                _lib.check(_lib.lib.ws_solver_warm_residual(h, i, C.byref(rc_), C.byref(rw_)))
+                states[i].cold_residual_energy, states[i].warm_residual_energy = rc_.value, rw_.value
             for i in range(R):
                 if states[i].warm_discarded:
                     outs[i], st = self.exec(sources[i])
