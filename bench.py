@@ -373,6 +373,9 @@ def run_ours(args):
             legs["batched"] = run_batched(args, sim, h, stream, torch, dev, value)
         if not args.no_warm:
             legs["warm_start"] = run_warm(args, sim, h, s, blocks, opts, torch, dev, E_dev, value)
+            if args.batch > 0:
+                legs["warm_start_batched"] = run_warm_batched(args, sim, torch, dev, value)
+            legs["start_quality"] = run_start_quality(sim, h, s, blocks, opts, torch, dev, n_iter)
         if args.media > 0:
             legs["mixed_media"] = run_media(args)
 
@@ -513,6 +516,105 @@ def run_warm(args, sim, h, s, blocks, opts, torch, dev, E_plain, plain_ms):
             "discarded": bool(disc.value), "first_cycle_energy_ratio": warm.value / cold.value,
             "initial_residual_ratio": (rw.value / rc.value) if rc.value > 0 else None,
             "rel_l2_vs_plain": diff, "speedup_vs_plain": plain_ms / ms, "checkpoint": os.path.relpath(DEFAULT_OUT, ROOT)}
+
+
+def _tilt(sim, angle_deg, n_bg=1.33):
+    """exp(i k n_bg sin(theta) x) over the ROI (y, x, z), and along x: the
+    phase of a plane wave tilted in the x-z plane, at the source plane."""
+    r = sim.roi
+    ny, nx, nz = (int(r[1, d] - r[0, d] + 1) for d in range(3))
+    k = 2 * np.pi / sim.lambda_ * n_bg * float(sim.options["pixel_size"])
+    ph = np.exp(1j * k * np.sin(np.radians(angle_deg)) * np.arange(nx))
+    return np.broadcast_to(ph[None, :, None], (ny, nx, nz)), ph
+
+
+def run_warm_batched(args, sim, torch, dev, plain_ms):
+    """The two sides together: args.batch plane waves at angles over +-30
+    degrees on the c3 medium in one batched solve (exec_batch), each
+    warm-started from the network's prediction for normal incidence times the
+    tilt's phase across the ROI; the time covers inference and the batched
+    solve (and any cold rerun of a discarded start).  Per-solve time against
+    the plain single solve."""
+    import wavesim_b200 as ws
+    from wavesim_b200 import warmstart
+    from wavesim_b200.train_warmstart import DEFAULT_OUT
+    if not os.path.exists(DEFAULT_OUT):
+        return {"unavailable": "no trained checkpoint (python -m wavesim_b200.train_warmstart)"}
+    model = warmstart.WarmStart.load(DEFAULT_OUT, device=dev.index or 0)
+    B = args.batch
+    angles = np.linspace(-30, 30, B) if B > 1 else np.zeros(1)
+    r = sim.roi
+    ny, nx = int(r[1, 0] - r[0, 0] + 1), int(r[1, 1] - r[0, 1] + 1)
+    n_roi = sim.roi_medium()
+    srcs = [ws.Source(np.broadcast_to(_tilt(sim, a)[1][None, :], (ny, nx)).copy(), [1, 1, 1]) for a in angles]
+
+    def step():
+        base = model.predict(n_roi)
+        starts = [base * _tilt(sim, a)[0] for a in angles]
+        return sim.exec_batch(srcs, warm_starts=starts)
+    step()
+    torch.cuda.synchronize()
+    steps = max(1, args.steps // 4)
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        Es, sts = step()
+    torch.cuda.synchronize()
+    ms = (time.perf_counter() - t0) * 1e3 / steps
+    return {"sources": B, "angles_deg": [float(a) for a in angles], "ms_per_batch": ms, "ms_per_solve": ms / B,
+            "iterations": [int(st.it - 1) for st in sts],
+            "discarded": [bool(getattr(st, "warm_discarded", False)) for st in sts],
+            "initial_residual_ratio": [float(st.warm_residual_energy / st.cold_residual_energy) for st in sts],
+            "speedup_vs_plain": plain_ms / (ms / B),
+            "timing": "host wall clock: inference (host round trip of the prediction) + the batched warm solve"}
+
+
+def run_start_quality(sim, h, s, blocks, opts, torch, dev, plain_it):
+    """How good a start must be: the c3 solve warm-started from the converged
+    field (energy threshold 1e-7) plus smooth complex noise of relative
+    amplitude a, for several a: total iterations (loop + the two probe
+    iterations) and the speed-up over the plain solve that a start of that
+    quality would give at zero inference cost."""
+    from wavesim_b200 import _lib
+    r = sim.roi
+    shape = tuple(int(r[1, d] - r[0, d] + 1) for d in range(3))
+    n_out = int(np.prod(shape))
+    E_out = torch.empty(2 * n_out, dtype=torch.float32, device=dev)
+    o = _lib.ws_solve_options()
+    C.pointer(o)[0] = opts
+    o.energy_threshold = 1e-7
+    n_it, conv = C.c_int64(), C.c_int()
+    _lib.check(_lib.lib.ws_solver_solve(h, len(s.values), blocks, _lib.WS_DEVICE, C.byref(o), E_out.data_ptr(),
+                                        _lib.WS_DEVICE, None, C.byref(n_it), C.byref(conv)))
+    Einf = E_out.cpu().numpy().view(np.complex64).reshape(shape, order="F")
+    tight_it = int(n_it.value)
+    rng = np.random.default_rng(5)
+    k = [np.fft.fftfreq(n).astype(np.float32) for n in shape]
+    lp = np.exp(-(k[0][:, None, None] ** 2 + k[1][None, :, None] ** 2 + k[2][None, None, :] ** 2)
+                * (2 * np.pi * 2) ** 2 / 2)
+    z = np.fft.ifftn(np.fft.fftn(rng.standard_normal(shape) + 1j * rng.standard_normal(shape)) * lp)
+    z *= np.linalg.norm(Einf) / np.linalg.norm(z)
+    o2 = _lib.ws_solve_options()
+    C.pointer(o2)[0] = opts
+    o2.warm_discard_ratio = sim.warm_discard_ratio
+    o2.initial_memory = _lib.WS_HOST
+    out = []
+    for a in (0.02, 0.05, 0.1, 0.2, 0.4):
+        u = sim.initial_field((Einf + a * z).astype(np.complex64))
+        o2.initial_field = u.ctypes.data
+        _lib.check(_lib.lib.ws_solver_solve(h, len(s.values), blocks, _lib.WS_DEVICE, C.byref(o2), E_out.data_ptr(),
+                                            _lib.WS_DEVICE, None, C.byref(n_it), C.byref(conv)))
+        disc = C.c_int()
+        rc_, rw_ = C.c_double(), C.c_double()
+        _lib.check(_lib.lib.ws_solver_warm_report(h, 0, None, None, C.byref(disc)))
+        _lib.check(_lib.lib.ws_solver_warm_residual(h, 0, C.byref(rc_), C.byref(rw_)))
+        it = int(n_it.value) + 2
+        out.append({"start_error": a, "iterations": it, "discarded": bool(disc.value),
+                    "initial_residual_ratio": rw_.value / rc_.value if rc_.value > 0 else None,
+                    "speedup_at_zero_inference": plain_it / it})
+    o2.initial_field = None
+    return {"converged_field_iterations": tight_it, "plain_iterations": plain_it, "curve": out,
+            "note": "start = converged field (threshold 1e-7) + smooth noise of relative L2 amplitude start_error; "
+                    "speed-up = plain iterations / (warm loop iterations + 2 probe iterations)"}
 
 
 def run_media(args):

@@ -6,8 +6,8 @@
   (The reference would run on to max_iterations; this is an addition.)
 * An Inf in the source does the same through WaveSim.exec.
 * The bounded waits of the TMA-pipelined outer pass: with a wait limit of one
-  clock (ws_solver_set_wait_limit) the tile loads cannot arrive in time, the
-  blocks give up, wait for their copies in flight with the default bound, set
+  clock (ws_solver_set_wait_limit; such a short bound polls the barrier
+  without suspending) the tile loads cannot arrive in time, the blocks give up, wait for their copies in flight with the default bound, set
   the error flag and return; the solve returns WS_ERR_CUDA ("timed out").
   The CUDA context stays usable: with the default limit restored, the same
   solver solves again and reproduces the result of a normal solve.
@@ -73,12 +73,12 @@ def test_tma_wait_limit_runs_out_and_reports(gpu):
     import wavesim_b200 as ws
     from wavesim_b200 import WaveSimError, _lib
     rng = np.random.default_rng(3)
-    # 64^3 grid: K2 is the TMA-pipelined pencil kernel (z = 64)
-    n = np.where(rng.random((32, 32, 32)) < 0.1, 1.5, 1.33)
+    # 128^3 grid: K2 is the TMA-pipelined pencil kernel (z = 128)
+    n = np.where(rng.random((96, 96, 96)) < 0.1, 1.5, 1.33)
     opt = {"lambda": 1.0, "pixel_size": 0.25, "boundary_widths": [16, 16, 16], "energy_threshold": 1e-99,
            "max_iterations": 16}
     sim = ws.WaveSim(n, opt)
-    src = ws.Source(np.ones((32, 32)), [1, 1, 1])
+    src = ws.Source(np.ones((96, 96)), [1, 1, 1])
     E0, st0 = sim.exec(src)
     h = sim.solver()
     for use_graph in (True, False):

@@ -46,19 +46,32 @@ __device__ __forceinline__ void expect_bytes(uint64_t* bar, uint32_t bytes) {
 }
 constexpr long long kWaitClocks = 50000000LL;  // ~25 ms at 2 GHz: the default bound of every wait
 
-// phase with parity `parity` of the barrier complete; false after `limit` clocks
+// phase with parity `parity` of the barrier complete; false after `limit`
+// clocks.  With the default bound the thread may be suspended inside
+// mbarrier.try_wait until the phase completes; a shorter bound polls with
+// the non-blocking mbarrier.test_wait, so that the bound itself decides.
 __device__ __forceinline__ bool wait_parity(uint64_t* bar, uint32_t parity, long long limit = kWaitClocks) {
   const uint32_t a = fast::smem_addr(bar);
   const long long t0 = clock64();
+  const bool poll = limit < kWaitClocks;
   while (true) {
     uint32_t done;
-    asm volatile(
-        "{\n\t.reg .pred p;\n\t"
-        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
-        "selp.u32 %0, 1, 0, p;\n\t}"
-        : "=r"(done)
-        : "r"(a), "r"(parity)
-        : "memory");
+    if (poll)
+      asm volatile(
+          "{\n\t.reg .pred p;\n\t"
+          "mbarrier.test_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+          "selp.u32 %0, 1, 0, p;\n\t}"
+          : "=r"(done)
+          : "r"(a), "r"(parity)
+          : "memory");
+    else
+      asm volatile(
+          "{\n\t.reg .pred p;\n\t"
+          "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+          "selp.u32 %0, 1, 0, p;\n\t}"
+          : "=r"(done)
+          : "r"(a), "r"(parity)
+          : "memory");
     if (done) return true;
     if (clock64() - t0 > limit) return false;
   }

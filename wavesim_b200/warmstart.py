@@ -471,17 +471,21 @@ def field_scale(pixel_size, lam, n_bg):
 def make_training_set(count, roi=48, bw=8, seed=0, n_bg=1.33, tol=1e-4, pixel_size=0.25, lam=1.0):
     """MBS solutions (this package's solver) of `count` seeded media of the
     c3 sphere distribution with a plane-wave source on the z = 1 face.
-    Returns a list of (n_roi, E_roi)."""
+    `roi` is one cube side or a sequence of sides (each sample draws one:
+    crops of several sizes).  Returns a list of (n_roi, E_roi)."""
     from .problem import Source
     from .simulation import WaveSim
     from .workloads import sphere_medium
     rng = np.random.default_rng(seed)
+    sides = [int(roi)] if np.ndim(roi) == 0 else [int(v) for v in roi]
     out = []
-    opt = {"lambda": lam, "pixel_size": pixel_size, "boundary_widths": [bw, bw, bw], "energy_threshold": tol}
+    opt = {"lambda": lam, "pixel_size": pixel_size, "boundary_widths": [bw, bw, bw], "energy_threshold": tol,
+           "device_setup": True}
     for _ in range(count):
-        n = sphere_medium(roi, rng, n_bg=n_bg)
+        side = sides[int(rng.integers(len(sides)))]
+        n = sphere_medium(side, rng, n_bg=n_bg)
         sim = WaveSim(n, opt)
-        E, st = sim.exec(Source(np.ones((roi, roi)), [1, 1, 1]))
+        E, st = sim.exec(Source(np.ones((side, side)), [1, 1, 1]))
         sim.close()
         out.append((n, E))
     return out
@@ -568,20 +572,33 @@ class WarmStart:
         self.net._check_err()
         return psi
 
-    def save(self, path, bf16=False):
+    def save(self, path, bf16=False, provenance=None):
         """Weights and normalisation to an .npz; bf16=True stores the weights
-        as bfloat16 bit patterns (uint16), the precision the kernels use."""
+        as bfloat16 bit patterns (uint16), the precision the kernels use.
+        provenance: a dict (e.g. the training command and its results),
+        stored as JSON text."""
         st = self.net.state()
         if bf16:
             st = {k: _to_bf16_bits(v) for k, v in st.items()}
         st["meta"] = np.array([self.n_bg, self.pixel_size, self.lam] + list(self.net.widths) +
                               [self.net.IN_CH, self.net.OUT_CH], np.float64)
+        if provenance is not None:
+            import json
+            st["provenance"] = np.array(json.dumps(provenance))
         np.savez_compressed(path, **st)
+
+    @staticmethod
+    def provenance(path):
+        """The provenance dict stored with a checkpoint (None if absent)."""
+        import json
+        st = np.load(path)
+        return json.loads(str(st["provenance"])) if "provenance" in st.files else None
 
     @classmethod
     def load(cls, path, device=0):
         st = dict(np.load(path))
         meta = st.pop("meta")
+        st.pop("provenance", None)
         st = {k: (_from_bf16_bits(v) if v.dtype == np.uint16 else v) for k, v in st.items()}
         in_ch, out_ch = (int(meta[7]), int(meta[8])) if meta.size > 7 else (8, 2)
         net = WarmStartNet(widths=tuple(int(v) for v in meta[3:7]), device=device, in_ch=in_ch, out_ch=out_ch)
