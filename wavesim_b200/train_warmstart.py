@@ -25,7 +25,6 @@ from __future__ import annotations
 import argparse
 import json
 import os
-import sys
 import time
 
 import numpy as np
@@ -87,10 +86,10 @@ def main(argv=None):
                          log=lambda s, l: print(json.dumps({"step": s, "loss": l}), flush=True))
     t_train = time.time() - t0
     del data
-    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
-    stored = dict(vars(args), out=os.path.relpath(os.path.abspath(args.out), root))
-    report = {"command": "python -m wavesim_b200.train_warmstart " + " ".join(argv if argv is not None else sys.argv[1:]),
-              "args": stored, "params": model.net.nparams, "data_s": t_data, "train_s": t_train,
+    # the command that reproduces these weights (every option but the output path)
+    stored = {k: v for k, v in vars(args).items() if k != "out"}
+    command = "python -m wavesim_b200.train_warmstart " + " ".join(f"--{k} {v}" for k, v in stored.items())
+    report = {"command": command, "args": stored, "params": model.net.nparams, "data_s": t_data, "train_s": t_train,
               "final_loss": float(np.mean(losses[-50:]))}
     report["eval"] = evaluate(model, sides, args.eval, boundary=args.boundary)
     for e in report["eval"]:
