@@ -322,8 +322,9 @@ def run_ours(args):
     # and the stop-rule kernel per iteration, the cycle guard per wiggle
     # cycle, state reset, source scatter, finalize
     per_it = _lib.lib.ws_solver_launches_per_iteration(h)
+    fused = per_it != 4
     launches_per_solve = (per_it * n_iter + (n_iter // len(sim.wiggles)) + 1 + len(s.values) + 1
-                          + (1 if per_it == 3 else 0))
+                          + (1 if fused else 0))
 
     # per-kernel device time (CUDA events on the solver's stream) -> roofline
     ms3 = (C.c_float * 3)()
@@ -342,7 +343,7 @@ def run_ours(args):
                      "frac": gbs / peak})
     iter_ms = sum(ms3)
     bytes_iter = sum(by3)
-    if per_it == 3:
+    if fused:
         # the loop runs K2 and K3K1 (K3 of an iteration fused with K1 of the
         # next, kf_plane_fused): the separate K1/K3 above are its parts, timed
         # alone for reference; the roofline is taken on the kernels that run
@@ -356,6 +357,16 @@ def run_ours(args):
                      "frac": gbs / peak, "in_loop": True})
         iter_ms = ms3[1] + msf.value
         bytes_iter = by3[1] + byf.value
+        # the split step: its three kernels (inverse x pencils, the column
+        # pass, forward x pencils) are the loop's kernels
+        ms_s, by_s = (C.c_float * 3)(), (C.c_double * 3)()
+        if _lib.lib.ws_solver_time_split(h, 24, ms_s, by_s) == 0:
+            kern[-1]["in_loop"] = False
+            kern[-1]["kernel"] = "K3K1 (split step, sum)"
+            for nm, i in (("Xinv", 0), ("Ycol", 1), ("Xfwd", 2)):
+                g_ = by_s[i] / (ms_s[i] * 1e-3) / 1e9
+                kern.append({"kernel": nm, "ms": ms_s[i], "algorithmic_bytes": by_s[i], "achieved_gbs": g_,
+                             "frac": g_ / peak, "in_loop": True})
     dom = max([k for k in kern if k.get("in_loop", True)], key=lambda k: k["ms"])
 
     # e2e: the reference-facing one-shot call (ws_run_algorithm, the MEX

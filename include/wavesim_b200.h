@@ -256,6 +256,15 @@ int ws_solver_launches_per_iteration(ws_solver s);
  * WS_ERR_UNSUPPORTED. */
 int ws_solver_time_fused(ws_solver s, int n_iterations, float* ms_out, double* bytes_out);
 
+/* Where the loop runs K3 of an iteration and K1 of the next as the split
+ * step (3-D power-of-two planes: inverse x transforms, the column pass with
+ * the y transforms and the pointwise epilogue, forward x transforms, each a
+ * separate kernel that needs no cluster), the mean CUDA-event time of each of
+ * the three kernels (ms_out[0..2], in that order) and their algorithmic bytes
+ * per launch (the column pass: the mean of an odd and an even iteration);
+ * otherwise WS_ERR_UNSUPPORTED.  No counterpart in the reference. */
+int ws_solver_time_split(ws_solver s, int n_iterations, float ms_out[3], double bytes_out[3]);
+
 /* After a warm-started solve of right-hand side `rhs`: the ROI energy of the
  * cold first increment (diff_energy(1), from the probe iteration), the ROI
  * energy of the true increment at the end of the warm first wiggle cycle,

@@ -1,8 +1,9 @@
-"""The fused loop (K3 of each iteration and K1 of the next in one kernel, on
-3-D planes split over a cluster) against the three separate kernels
-(WAVESIM_B200_FUSE=0).  The fused kernel does the same arithmetic in the same
-order, so the fields must agree bit for bit: cold, warm, batched, with the
-host loop and with the CUDA graph."""
+"""The fused loop (K3 of each iteration and K1 of the next: on power-of-two
+planes the split step - x pencils, the column pass, x pencils - and with
+WAVESIM_B200_STEP=cluster, or on 192- and 96-point planes, one kernel on a
+cluster) against the three separate kernels (WAVESIM_B200_FUSE=0).  Both do
+the same arithmetic in the same order, so the fields must agree bit for bit:
+cold, warm, batched, with the host loop and with the CUDA graph."""
 import os
 
 import numpy as np
@@ -36,17 +37,25 @@ def medium(shape, seed=3):
     return 1.3 + 0.15 * rng.random(shape) + 0.002j
 
 
+CLUSTER = {"WAVESIM_B200_STEP": "cluster"}
 CASES = {
-    "128_cluster2": ((96, 96, 96), [16, 16, 16], None),
-    "256_cluster8": ((224, 224, 16), [16, 16, 8], None),
+    # power-of-two planes: the split step (x pencils, column pass, x pencils)
+    "64_split": ((32, 32, 32), [16, 16, 16], None),
+    "128_split": ((96, 96, 96), [16, 16, 16], None),
+    "256_split": ((224, 224, 16), [16, 16, 8], None),
+    "256_split_x16": ((224, 224, 16), [16, 16, 8], {"WAVESIM_B200_XTY": "16"}),
+    "256_split_vector": ((224, 224, 8), [16, 16, 4], "vector"),
+    # the one-kernel step with the cluster exchange
+    "128_cluster2": ((96, 96, 96), [16, 16, 16], CLUSTER),
+    "256_cluster8": ((224, 224, 16), [16, 16, 8], CLUSTER),
     # 16-block clusters: K1's half of the exchange pushed (kf_plane_fused_push)
-    "256_cluster16": ((224, 224, 16), [16, 16, 8], {"WAVESIM_B200_CLUSTER": "16"}),
+    "256_cluster16": ((224, 224, 16), [16, 16, 8], dict(CLUSTER, WAVESIM_B200_CLUSTER="16")),
     # 192-point planes on 6 blocks (km_plane_fused), scalar and vector
     "192_cluster6": ((160, 160, 8), [16, 16, 4], None),
     "192_cluster6_vector": ((160, 160, 4), [16, 16, 2], "vector"),
     # K3's rows by per-thread loads instead of one tensor copy (kf_plane_fused)
-    "128_cluster2_loads": ((96, 96, 96), [16, 16, 16], {"WAVESIM_B200_FUSED_TMA": "0"}),
-    "256_cluster8_loads": ((224, 224, 16), [16, 16, 8], {"WAVESIM_B200_FUSED_TMA": "0"}),
+    "128_cluster2_loads": ((96, 96, 96), [16, 16, 16], dict(CLUSTER, WAVESIM_B200_FUSED_TMA="0")),
+    "256_cluster8_loads": ((224, 224, 16), [16, 16, 8], dict(CLUSTER, WAVESIM_B200_FUSED_TMA="0")),
     # 96^2 planes on one block (km_plane_fused with a cluster of 1)
     "96_one_block": ((64, 64, 32), [16, 16, 16], None),
     "192_cluster6_loads": ((160, 160, 8), [16, 16, 4], {"WAVESIM_B200_FUSED_TMA": "0"}),
@@ -69,7 +78,7 @@ def test_fused_loop_is_bit_identical(gpu, name, use_graph):
     def run(ws):
         sim = (ws.WaveSimVector if vector else ws.WaveSim)(n, opt)
         from wavesim_b200 import _lib
-        fused = _lib.lib.ws_solver_launches_per_iteration(sim.solver()) == 3
+        fused = _lib.lib.ws_solver_launches_per_iteration(sim.solver()) != 4
         E, st = sim.exec(ws.Source(val, pos))
         sim.close()
         return E, st, fused

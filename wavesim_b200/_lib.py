@@ -69,7 +69,7 @@ EXPORTS = [
     "ws_default_options", "ws_version", "ws_last_error", "ws_size_supported", "ws_run_algorithm",
     "ws_run_algorithm_release",
     "ws_solver_create", "ws_solver_solve", "ws_solver_solve_batch", "ws_solver_solve_plane_waves", "ws_solver_buffers",
-    "ws_solver_time_kernels",
+    "ws_solver_time_kernels", "ws_solver_time_split",
     "ws_solver_launches_per_iteration", "ws_solver_set_wait_limit", "ws_solver_time_fused", "ws_solver_warm_report", "ws_solver_warm_residual", "ws_solver_autotune", "ws_solver_destroy",
     "ws_run_algorithm_noalloc", "ws_medium_reduce", "ws_build_gamma", "ws_setup_last_error",
     "ws_noalloc_scratch_bytes", "ws_noalloc_last_error",
@@ -132,6 +132,8 @@ def _load():
     lib.ws_solver_launches_per_iteration.argtypes = [P]
     lib.ws_solver_launches_per_iteration.restype = C.c_int
     lib.ws_solver_time_fused.argtypes = [P, C.c_int, C.POINTER(C.c_float), C.POINTER(C.c_double)]
+    lib.ws_solver_time_split.argtypes = [P, C.c_int, C.POINTER(C.c_float), C.POINTER(C.c_double)]
+    lib.ws_solver_time_split.restype = C.c_int
     lib.ws_solver_time_fused.restype = C.c_int
     lib.ws_solver_warm_report.argtypes = [P, C.c_int64, C.POINTER(C.c_double), C.POINTER(C.c_double),
                                           C.POINTER(C.c_int)]

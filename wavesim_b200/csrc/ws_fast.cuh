@@ -1020,6 +1020,138 @@ __global__ void __launch_bounds__(kThreads, 2)
 }
 
 
+// The fused step split into passes that need no cluster (the default loop of
+// 3-D power-of-two planes).  K3 of iteration k followed by K1 of iteration
+// k + 1 is an inverse 2-D (y, x) transform, the pointwise epilogue and a
+// forward 2-D transform of every z plane; run as
+//   kt_xpencil<.., INV>  inverse x transforms (TMA-pipelined pencils along x)
+//   kc_col_step<N, C>    per (x, z) column: inverse y transform, unwiggle,
+//                        f_mix, E' += dE', ROI energy, the next iteration's
+//                        source and ramps, forward y transform
+//   kt_xpencil<.., FWD>  forward x transforms
+// each pass reads and writes whole contiguous lines, so no block waits for
+// another.  It moves 80 instead of 48 bytes per point, but each pass streams
+// at close to the HBM bandwidth where the cluster exchange of the one-kernel
+// step left it latency bound.
+//
+// kc_col_step covers the columns of the plane kernels' block (plane, rank):
+// x0 = rank M .. x0 + M - 1 at z, with the same thread of each line, the same
+// arithmetic in the same order (line_fft, the epilogue of kf_plane_fused) and
+// the same per-block energy partial, so its fields equal the one-kernel
+// step's bit for bit.
+template <int N, int C>
+__global__ void __launch_bounds__(kThreads, 2)
+    kc_col_step(InnerArgs a, Wig w1, const float2* __restrict__ src1, float2 A, float2* __restrict__ T,
+                float2* __restrict__ dE, float2* __restrict__ E, const float2* __restrict__ gamma,
+                const DevState* __restrict__ st, double* __restrict__ partials) {
+  using G = PlaneGeom<N, C, true>;
+  constexpr int P = G::P, LPR = G::LPR, M = G::M;
+  static_assert(M % LPR == 0, "whole rounds of lines");
+  const int rhs = blockIdx.x / a.bpr, bid = blockIdx.x - rhs * a.bpr;
+  st += rhs;
+  if (load_done(st)) return;
+  const bool acc_now = !a.acc2 || (__ldcg(&st->it) & 1) == 0;
+  T += rhs * a.fstride;
+  dE += rhs * a.fstride;
+  E += rhs * a.fstride;
+  if (src1) src1 += rhs * a.fstride;
+  partials += (long long)rhs * a.bpr;
+  __shared__ float2 sm[LPR * G::CS];  // one round of lines: the transforms' exchanges
+  __shared__ float red[kThreads / 32];
+  const int tid = threadIdx.x;
+  const Geom& g = a.g;
+  const int nx = g.nx;
+  const int rank = (int)(bid % C), plane = bid / C;
+  const int x0 = rank * M, z = plane % g.nz, comp = plane / g.nz;
+  const long long colbase = (long long)plane * nx + x0;
+  // the y ramps of this and the next wiggle, read from shared memory: as
+  // per-element global loads inside the epilogue they left the pass latency
+  // bound (0.19 against 0.12 ms at 256^3)
+  __shared__ float2 sgy[2 * N];
+  for (int i = tid; i < N; i += kThreads) {
+    sgy[i] = a.w.gy[i];
+    sgy[N + i] = w1.gy[i];
+  }
+  __syncthreads();
+  const float2 gzz = a.w.gz[z];
+  const float2 gzz1 = w1.gz[z];
+  float esum = 0.f;
+  for (int c0 = 0; c0 < M; c0 += LPR) {
+    const int cl = tid / P, cc = c0 + cl, p = tid % P;
+    const int x = x0 + cc;
+    const long long col = colbase + cc;
+    const long long gcol = col * N;
+    float2* __restrict__ Tc = T + gcol;
+    float2 v[16];
+#pragma unroll
+    for (int r = 0; r < 16; ++r) v[r] = Tc[p + P * r];
+    ColLine L{sm + cl * G::CS};
+    if constexpr (P <= 32) {
+      line_fft<N, true>(v, L, p, a.py.tw, SyncWarp{});
+    } else {
+      line_fft<N, true>(v, L, p, a.py.tw, SyncBlock{});
+    }
+    const float2 gxz = cmul(a.w.gx[x], gzz);
+    const bool in_xzc = x >= g.r0[1] && x < g.r1[1] && z >= g.r0[2] && z < g.r1[2] && comp >= g.r0[3] && comp < g.r1[3];
+    const float2* __restrict__ gmc = gamma + (gcol - (long long)comp * g.npts);
+    float2* __restrict__ dEc = dE + gcol;
+    float2* __restrict__ Ec = E + gcol;
+    // K3's epilogue (unwiggle, f_mix, E' += dE', ROI energy); v[m] becomes dE'_k(y)
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      float2 gm[8], d0[8], e0[8];
+#pragma unroll
+      for (int i = 0; i < 8; ++i) {
+        const int y = p + P * (8 * h + i);
+        gm[i] = gmc[y];
+        d0[i] = dEc[y];
+        e0[i] = acc_now ? Ec[y] : make_float2(0.f, 0.f);
+      }
+#pragma unroll
+      for (int i = 0; i < 8; ++i) {
+        const int m = 8 * h + i;
+        const int y = p + P * m;
+        const float2 ep = cmul_conj(cmul_conj(v[m], gxz), sgy[y]);
+        const float2 one_m = make_float2(1.f - kAlpha * gm[i].x, -kAlpha * gm[i].y);
+        const float2 t = cmul(cmul(gm[i], gm[i]), ep);
+        const float2 dn = cadd(cmul(one_m, d0[i]), make_float2(kAlpha * t.y, -kAlpha * t.x));
+        dEc[y] = dn;
+        if (acc_now) Ec[y] = cadd(e0[i], a.acc2 ? cadd(d0[i], dn) : dn);
+        if (in_xzc && y >= g.r0[0] && y < g.r1[0]) esum = fmaf(dn.x, dn.x, fmaf(dn.y, dn.y, esum));
+        v[m] = dn;
+      }
+    }
+    // K1 of iteration k + 1 on the same column: source, next ramps, y transform
+    const float2 gxz1 = cmul(w1.gx[x], gzz1);
+    const float2* __restrict__ sr = src1 ? src1 + gcol : nullptr;
+#pragma unroll
+    for (int m = 0; m < 16; ++m) {
+      const int y = p + P * m;
+      float2 e = v[m];
+      if (sr) e = cadd(e, cmul(A, sr[y]));
+      v[m] = cmul(cmul(e, gxz1), sgy[N + y]);
+    }
+    if constexpr (P <= 32) {
+      line_fft<N, false>(v, L, p, a.py.tw, SyncWarp{});
+    } else {
+      line_fft<N, false>(v, L, p, a.py.tw, SyncBlock{});
+    }
+#pragma unroll
+    for (int m = 0; m < 16; ++m) Tc[p + P * m] = v[m];
+  }
+  // the ROI energy of dE'_k, reduced as in the one-kernel step
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) esum += __shfl_xor_sync(0xffffffffu, esum, o);
+  if ((tid & 31) == 0) red[tid >> 5] = esum;
+  __syncthreads();
+  if (tid < 32) {
+    float v = tid < kThreads / 32 ? red[tid] : 0.f;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    if (tid == 0) partials[bid] = (double)v;
+  }
+}
+
 // The same fused step with K1's half of the plane exchange pushed: each block
 // sends its transformed columns to the row owners with st.async, completion
 // counted in bytes on the receiver's mbarrier (as in kf_plane_fwd), instead of

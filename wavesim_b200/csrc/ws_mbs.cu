@@ -83,6 +83,7 @@ struct FastInner {
   const void* fused = nullptr;  // K3 of one iteration + K1 of the next (3-D planes on a cluster), or null
   size_t smem_fused = 0;
   const void* fused_tma = nullptr;  // the same with K3's rows loaded by a tensor copy (first argument: the map)
+  const void* col_step = nullptr;   // the column pass of the split fused step (kc_col_step), or null
 };
 struct FastPencil {
   int no, ty;
@@ -99,6 +100,7 @@ static FastInner fast_inner() {
   FastInner f{N, C, DX ? 1 : 0, (const void*)fast::kf_plane_fwd<N, C, DX>,
               (const void*)fast::kf_plane_inv<N, C, DX>, DX ? G::smem : (size_t)G::CS * sizeof(float2),
               DX ? (G::PUSH ? G::smem_push : G::smem_a) : 0, DX ? G::smem_max_ab : 0};
+  if constexpr (DX) f.col_step = (const void*)fast::kc_col_step<N, C>;
   if constexpr (DX && C > 1) {
     if constexpr (C >= 16) {  // small tiles: the column tile and the row tile fit side by side
       f.fused = (const void*)fast::kf_plane_fused_push<N, C>;
@@ -163,6 +165,26 @@ static TmaPencil tma_pencil_vec() {
   using PT = tma::VecPencilTile<PL, TY, S>;
   return TmaPencil{PL::N, TY, S, (const void*)tma::kt_pencil_vec<PL, TY, S>, PT::smem, PT::kThreads, 3};
 }
+// The x passes of the split fused step (kt_xpencil, ws_tma.cuh).
+struct XPencil {
+  int no, ty, stages;
+  const void* fwd;
+  const void* inv;
+  size_t smem;
+  int threads;
+};
+template <int NO, int TY, int S>
+static XPencil x_pencil() {
+  using PT = tma::PencilTile<NO, TY, S>;
+  return XPencil{NO, TY, S, (const void*)tma::kt_xpencil<NO, TY, S, false>,
+                 (const void*)tma::kt_xpencil<NO, TY, S, true>, PT::smem, PT::kThreads};
+}
+static const std::vector<XPencil>& x_pencil_table() {
+  // the first match of (no, ty) is the default
+  static const std::vector<XPencil> t = {x_pencil<64, 16, 3>(), x_pencil<128, 16, 3>(), x_pencil<256, 8, 4>(),
+                                         x_pencil<256, 16, 3>()};
+  return t;
+}
 using Plan192t = mixed::Plan<192, 12, 12, 4, 4>;
 static const std::vector<TmaPencil>& tma_pencil_table() {
   // the first match of (no, ty) is the default; the autotuner tries the rest
@@ -197,6 +219,7 @@ struct Layout {
   const FastInner* fi = nullptr;   // fast K1/K3, or null (generic)
   const FastPencil* fp = nullptr;  // fast K2, or null (generic)
   const TmaPencil* tp = nullptr;   // persistent TMA K2 (takes precedence over fp), or null
+  const XPencil* xp = nullptr;     // x passes of the split fused step, or null (one-kernel fused step)
   int rset = kPow2;  // radix set of every plan of the solver
   int mode3d = 0;
   int csize = 1;     // 3-D: blocks (cluster) per plane
@@ -346,6 +369,18 @@ static int make_layout(const Geom& g, Layout& L, std::string& why, const LayoutC
         L.tp = &f;
         break;
       }
+  // the split fused step (x pencils + column pass) on power-of-two planes;
+  // WAVESIM_B200_STEP=cluster keeps the one-kernel step with the cluster
+  // exchange, WAVESIM_B200_XTY picks the x pencils' y tile
+  const char* step = std::getenv("WAVESIM_B200_STEP");
+  int want_xty = 0;
+  if (const char* e = std::getenv("WAVESIM_B200_XTY")) want_xty = std::atoi(e);
+  if (L.mode3d && L.fi && L.fi->col_step && !(step && std::strcmp(step, "cluster") == 0))
+    for (const XPencil& f : x_pencil_table())
+      if (f.no == g.nx && g.ny % f.ty == 0 && (!want_xty || f.ty == want_xty)) {
+        L.xp = &f;
+        break;
+      }
   return WS_OK;
 }
 
@@ -397,6 +432,11 @@ struct Solver {
   int tmap_nrhs = 0;
   const void* tmap_kernel = nullptr;  // the TMA pencil the map and tma_blocks were made for
   int tma_blocks = 0;            // resident blocks of the TMA pencil (its persistent grid)
+  CUtensorMap tmap_X{};          // T as {2 Ny floats, Nx, Nz Nc nrhs}, box {2 TY, Nx, 1}, for the x pencils
+  const void* xmap_base = nullptr;
+  int xmap_nrhs = 0;
+  const void* xmap_kernel = nullptr;
+  int x_blocks = 0;              // resident blocks of the x pencil (its persistent grid)
   CUtensorMap tmap_slab{};       // T as 2-D {2 Ny floats, Nx Nz Nc nrhs}, box {2 LR, N}, for kf_plane_fused_tma
   const void* slab_base = nullptr;
   int slab_nrhs = 0;
@@ -429,7 +469,8 @@ static void free_graph(Solver* s) {
 // a cluster); WAVESIM_B200_FUSE=0 keeps the three kernels separate.
 static void update_fuse(Solver* s) {
   const char* e = std::getenv("WAVESIM_B200_FUSE");
-  const int f = (s->lay.fi && s->lay.fi->fused && s->lay.mode3d && !s->pstd && !(e && std::strcmp(e, "0") == 0))
+  const int f = (s->lay.fi && (s->lay.fi->fused || s->lay.xp) && s->lay.mode3d && !s->pstd &&
+                 !(e && std::strcmp(e, "0") == 0))
                     ? 1 : 0;
   if (f != s->fuse) free_graph(s);
   s->fuse = f;
@@ -513,6 +554,10 @@ static int set_kernel_attributes() {
   }
   for (const FastPencil& f : fast_pencil_table()) WS_CUDA(allow_dynamic_smem(f.fn, optin));
   for (const TmaPencil& f : tma_pencil_table()) WS_CUDA(allow_dynamic_smem(f.fn, optin));
+  for (const XPencil& f : x_pencil_table()) {
+    WS_CUDA(allow_dynamic_smem(f.fwd, optin));
+    WS_CUDA(allow_dynamic_smem(f.inv, optin));
+  }
   if (dev < 31) done_mask |= 1 << dev;
   return WS_OK;
 }
@@ -1020,13 +1065,91 @@ static cudaError_t launch_k3k1(const Solver* s, int w, int w1, bool src_next) {
              : cudaLaunchKernelExC(&cfg, s->lay.fi->fused, args);
 }
 
+// T of the current batch as a 3-D float tensor {2 Ny, Nx, Nz Nc nrhs}, box
+// {2 TY, Nx, 1}, for the x pencils: every x coordinate the kernel issues is
+// 2 TY yt floats (a multiple of 16 floats, TY >= 8), the others 0 and the
+// plane index, both >= 0.
+static cudaError_t ensure_xmap(Solver* s) {
+  const XPencil* f = s->lay.xp;
+  if (s->xmap_base == s->d_T && s->xmap_nrhs == s->nrhs && s->xmap_kernel == f->fwd) return cudaSuccess;
+  s->xmap_kernel = nullptr;
+  s->x_blocks = 0;
+  EncodeTiledFn enc = encode_tiled();
+  if (!enc) return cudaErrorNotSupported;
+  const Geom& g = s->g;
+  const cuuint64_t dims[3] = {(cuuint64_t)2 * g.ny, (cuuint64_t)g.nx, (cuuint64_t)g.nz * g.nc * s->nrhs};
+  const cuuint64_t strides[2] = {(cuuint64_t)g.ny * sizeof(float2), (cuuint64_t)g.ny * g.nx * sizeof(float2)};
+  const cuuint32_t box[3] = {(cuuint32_t)(2 * f->ty), (cuuint32_t)f->no, 1u};
+  const cuuint32_t estr[3] = {1u, 1u, 1u};
+  if (enc(&s->tmap_X, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, s->d_T, dims, strides, box, estr,
+          CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+          CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+    return cudaErrorInvalidValue;
+  s->xmap_base = s->d_T;
+  s->xmap_nrhs = s->nrhs;
+  s->xmap_kernel = f->fwd;
+  return cudaSuccess;
+}
+
+// The x transforms of every (y, z) line of T in place: forward or inverse.
+static cudaError_t launch_xpencil(const Solver* cs, bool inv) {
+  Solver* s = const_cast<Solver*>(cs);  // the tensor-map cache only
+  const XPencil* f = s->lay.xp;
+  cudaError_t e = ensure_xmap(s);
+  if (e != cudaSuccess) return e;
+  if (s->x_blocks <= 0) {
+    int per_sm = 0;
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, f->fwd, f->threads, f->smem);
+    if (e != cudaSuccess) return e;
+    s->x_blocks = std::max(1, per_sm) * kNumSms;
+  }
+  int ntiles = s->nrhs * s->g.nz * s->g.nc * (s->g.ny / f->ty);
+  const unsigned grid = (unsigned)std::min(ntiles, s->x_blocks);
+  Geom g = s->g;
+  const float2* tw = s->twx;
+  const DevState* st = s->d_state;
+  long long wc = s->wait_clocks;
+  int* err = s->d_err;
+  void* args[] = {&s->tmap_X, &g, &tw, &st, &ntiles, &wc, &err};
+  return cudaLaunchKernel(inv ? f->inv : f->fwd, dim3(grid), dim3(f->threads), args, f->smem, s->stream);
+}
+
+// The column pass of the split fused step (kc_col_step): the columns of every
+// plane kernel block, no cluster.
+static cudaError_t launch_colstep(const Solver* s, int w, int w1, bool src_next) {
+  InnerArgs a = inner_args(s, w);
+  a.ncols = s->lay.ncols;
+  Wig W1 = s->wig[w1];
+  const float2* src1 = src_next ? s->d_src : nullptr;
+  float2 A = make_float2(0.f, (float)(1.0f / s->eps / (float)s->nw));
+  float2* T = s->d_T;
+  float2* dE = s->d_dE;
+  float2* E = s->d_E;
+  const float2* gamma = s->d_gamma;
+  const DevState* st = s->d_state;
+  double* partials = s->d_partials;
+  void* args[] = {&a, &W1, &src1, &A, &T, &dE, &E, &gamma, &st, &partials};
+  return cudaLaunchKernel(s->lay.fi->col_step, dim3((unsigned)(s->lay.grid_inner * s->nrhs)), dim3(fast::kThreads),
+                          args, 0, s->stream);
+}
+
+// K3 of an iteration and K1 of the next: one kernel on a cluster, or the
+// split step (inverse x pencils, column pass, forward x pencils).
+static cudaError_t launch_step(const Solver* s, int w, int w1, bool src_next) {
+  if (!s->lay.xp) return launch_k3k1(s, w, w1, src_next);
+  cudaError_t e = launch_xpencil(s, true);
+  if (e != cudaSuccess) return e;
+  if ((e = launch_colstep(s, w, w1, src_next)) != cudaSuccess) return e;
+  return launch_xpencil(s, false);
+}
+
 // One iteration of the fused loop: T already holds K1's output for it.
 static cudaError_t launch_iteration_fused(const Solver* s, int i, bool src_next, const StopRule& rule,
                                           const Hist& h) {
   const int w = i % s->nw, w1 = (i + 1) % s->nw;
   cudaError_t e = launch_k2(s, w);
   if (e != cudaSuccess) return e;
-  if ((e = launch_k3k1(s, w, w1, src_next)) != cudaSuccess) return e;
+  if ((e = launch_step(s, w, w1, src_next)) != cudaSuccess) return e;
   return launch_finish(s, rule, h);
 }
 
@@ -1546,7 +1669,9 @@ int ws_solver_set_wait_limit(ws_solver h, int64_t clocks) {
 
 int ws_solver_launches_per_iteration(ws_solver h) {
   if (!h) return 0;
-  return reinterpret_cast<Solver*>(h)->fuse ? 3 : 4;  // (K1,) K2, K3 or K3 + next K1, stop rule
+  const Solver* s = reinterpret_cast<Solver*>(h);
+  // K2, K3 + next K1 (one kernel, or the split step's three), stop rule; or K1, K2, K3, stop rule
+  return s->fuse ? (s->lay.xp ? 5 : 3) : 4;
 }
 
 int ws_solver_time_fused(ws_solver h, int n_iterations, float* ms_out, double* bytes_out) {
@@ -1569,7 +1694,7 @@ int ws_solver_time_fused(ws_solver h, int n_iterations, float* ms_out, double* b
     const int w = i % s->nw;
     WS_CUDA(launch_k2(s, w));
     WS_CUDA(cudaEventRecord(s->ev[0], s->stream));
-    WS_CUDA(launch_k3k1(s, w, (i + 1) % s->nw, false));
+    WS_CUDA(launch_step(s, w, (i + 1) % s->nw, false));
     WS_CUDA(cudaEventRecord(s->ev[1], s->stream));
     WS_CUDA(launch_finish(s, rule, hh));
     WS_CUDA(cudaEventSynchronize(s->ev[1]));
@@ -1580,8 +1705,54 @@ int ws_solver_time_fused(ws_solver h, int n_iterations, float* ms_out, double* b
   *ms_out = acc / n_iterations;
   if (bytes_out) {
     const double n = (double)s->g.npts * s->g.nc;
-    // K3's bytes (as ws_solver_time_kernels) plus the write of T for the next iteration
-    *bytes_out = (s->nw % 2 == 0 ? 40.0 : 48.0) * n + 8.0 * (double)s->g.npts;
+    // K3's bytes (as ws_solver_time_kernels) plus the write of T for the next
+    // iteration; the split step also reads and writes T in each x pass
+    *bytes_out = (s->nw % 2 == 0 ? 40.0 : 48.0) * n + 8.0 * (double)s->g.npts + (s->lay.xp ? 32.0 * n : 0.0);
+  }
+  return WS_OK;
+}
+
+int ws_solver_time_split(ws_solver h, int n_iterations, float ms_out[3], double bytes_out[3]) {
+  if (!h || !ms_out || n_iterations < 1) return fail(WS_ERR_INVALID_ARGUMENT, "bad argument");
+  Solver* s = reinterpret_cast<Solver*>(h);
+  if (!s->fuse || !s->lay.xp) return fail(WS_ERR_UNSUPPORTED, "this solver's loop does not run the split step");
+  WS_CUDA(cudaSetDevice(s->device));
+  const long long cap = n_iterations + 1;
+  if (s->hist_cap < cap) {
+    const int rc = ensure_hist(s, cap);
+    if (rc) return rc;
+  }
+  StopRule rule{s->nw, 1, 0, 1, (long long)1 << 62, -1.0};
+  Hist hh{s->d_hist, s->d_hist + s->hist_cap, 0, 0};  // cap 0: history untouched
+  s->nrhs = 1;
+  k_resume_state<<<1, 32, 0, s->stream>>>(s->d_state);
+  WS_CUDA(launch_k1(s, 0, false));
+  float acc[3] = {0, 0, 0};
+  for (int i = 0; i < n_iterations; ++i) {
+    const int w = i % s->nw;
+    WS_CUDA(launch_k2(s, w));
+    WS_CUDA(cudaEventRecord(s->ev[0], s->stream));
+    WS_CUDA(launch_xpencil(s, true));
+    WS_CUDA(cudaEventRecord(s->ev[1], s->stream));
+    WS_CUDA(launch_colstep(s, w, (i + 1) % s->nw, false));
+    WS_CUDA(cudaEventRecord(s->ev[2], s->stream));
+    WS_CUDA(launch_xpencil(s, false));
+    WS_CUDA(cudaEventRecord(s->ev[3], s->stream));
+    WS_CUDA(launch_finish(s, rule, hh));
+    WS_CUDA(cudaEventSynchronize(s->ev[3]));
+    float t;
+    for (int k = 0; k < 3; ++k) {
+      WS_CUDA(cudaEventElapsedTime(&t, s->ev[k], s->ev[k + 1]));
+      acc[k] += t;
+    }
+  }
+  for (int k = 0; k < 3; ++k) ms_out[k] = acc[k] / n_iterations;
+  if (bytes_out) {
+    const double n = (double)s->g.npts * s->g.nc;
+    bytes_out[0] = 16.0 * n;  // read T, write T
+    // read T, dE, gamma, write dE, T; E' read and written after even iterations only (the mean)
+    bytes_out[1] = (s->nw % 2 == 0 ? 40.0 : 48.0) * n + 8.0 * (double)s->g.npts;
+    bytes_out[2] = 16.0 * n;
   }
   return WS_OK;
 }

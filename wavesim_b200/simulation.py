@@ -500,8 +500,9 @@ class WaveSim:
                 if states[i].warm_discarded:
                     outs[i], st = self.exec(sources[i])
                     st.warm_discarded, st.warm_iterations = True, states[i].it - 1
-                    st.cold_first_energy = states[i].cold_first_energy
-                    st.warm_cycle_energy = states[i].warm_cycle_energy
+                    for k in ("cold_first_energy", "warm_cycle_energy", "cold_residual_energy",
+                              "warm_residual_energy"):
+                        setattr(st, k, getattr(states[i], k))
                     st.time += dt
                     states[i] = st
         return outs, states
