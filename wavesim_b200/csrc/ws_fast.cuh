@@ -168,6 +168,25 @@ __device__ __forceinline__ void line_stage(float2 (&v)[16], const Line& L, int p
   }
 }
 
+// Lines of up to 256 points have two stages, and the second stage's twiddles
+// of a thread depend on its p only: a persistent kernel that transforms many
+// lines with the same p loads them once (load_tw2) and passes them to
+// line_fft_tw2, which is line_fft with those registers in place of the
+// table loads (the same values, so the same results).
+template <int N>
+__device__ __forceinline__ void load_tw2(float2 (&wt)[16], int p, const float2* __restrict__ tw) {
+  using PL = LinePlan<N>;
+  static_assert(PL::NST == 2, "two-stage lines");
+  constexpr int R = PL::radix(1), Ns = PL::span(1), B = 16 / R, P = PL::P, TS = N / (Ns * R);
+#pragma unroll
+  for (int q = 0; q < B; ++q) {
+    const int jm = (p + P * q) & (Ns - 1);
+    wt[q * R] = make_float2(1.f, 0.f);
+#pragma unroll
+    for (int r = 1; r < R; ++r) wt[q * R + r] = __ldg(&tw[jm * r * TS]);
+  }
+}
+
 // In: v[r] = x[p + P r].  Out: v[m] = X[p + P m] (unnormalised; INV: sign +1).
 template <int N, bool INV, class Line, class Sync>
 __device__ __forceinline__ void line_fft(float2 (&v)[16], const Line& L, int p, const float2* __restrict__ tw,
@@ -175,6 +194,52 @@ __device__ __forceinline__ void line_fft(float2 (&v)[16], const Line& L, int p, 
   line_stage<N, INV, 0>(v, L, p, tw, sync);
   if constexpr (LinePlan<N>::NST > 1) line_stage<N, INV, 1>(v, L, p, tw, sync);
   if constexpr (LinePlan<N>::NST > 2) line_stage<N, INV, 2>(v, L, p, tw, sync);
+}
+
+template <int N, bool INV, class Line, class Sync>
+__device__ __forceinline__ void line_fft_tw2(float2 (&v)[16], const Line& L, int p, const float2 (&wt)[16],
+                                             Sync sync) {
+  using PL = LinePlan<N>;
+  static_assert(PL::NST == 2, "two-stage lines");
+  constexpr int R0 = PL::radix(0), B0 = 16 / R0, Ns0 = PL::span(0);
+  constexpr int R = PL::radix(1), Ns = PL::span(1), B = 16 / R, P = PL::P, NR = N / R;
+  // stage 0 (as line_stage<N, INV, 0>)
+#pragma unroll
+  for (int q = 0; q < B0; ++q) dft_slice<R0, INV>(v, q * R0);
+  sync();
+#pragma unroll
+  for (int q = 0; q < B0; ++q) {
+    const int j = p + P * q;
+    const int jm = j & (Ns0 - 1);
+    const int base = (j - jm) * R0 + jm;
+#pragma unroll
+    for (int r = 0; r < R0; ++r) L.at(base + r * Ns0) = v[q * R0 + r];
+  }
+  sync();
+  // stage 1 (as line_stage<N, INV, 1>, twiddles from wt)
+#pragma unroll
+  for (int q = 0; q < B; ++q) {
+    const int j = p + P * q;
+#pragma unroll
+    for (int r = 0; r < R; ++r) v[q * R + r] = L.at(j + r * NR);
+#pragma unroll
+    for (int r = 1; r < R; ++r) {
+      float2 w = wt[q * R + r];
+      if (INV) w.y = -w.y;
+      v[q * R + r] = cmul(v[q * R + r], w);
+    }
+  }
+#pragma unroll
+  for (int q = 0; q < B; ++q) dft_slice<R, INV>(v, q * R);
+  if constexpr (B > 1) {
+    float2 t[16];
+#pragma unroll
+    for (int q = 0; q < B; ++q)
+#pragma unroll
+      for (int r = 0; r < R; ++r) t[q + B * r] = v[q * R + r];
+#pragma unroll
+    for (int m = 0; m < 16; ++m) v[m] = t[m];
+  }
 }
 
 // shared-memory tile geometry of the plane kernels

@@ -125,6 +125,8 @@ __global__ void __launch_bounds__(PencilTile<NO, TY, S>::kThreads, 2)
   const int mine = blockIdx.x < ntiles ? (ntiles - 1 - blockIdx.x) / G + 1 : 0;  // tiles of this block
   if (tid == 0)
     for (int i = 0; i < S - 1 && i < mine; ++i) issue(blockIdx.x + i * G, i);
+  float2 wt[16];  // the second stage's twiddles of this thread, the same for every tile
+  fast::load_tw2<NO>(wt, p, a.po.tw);
   // this thread's part of the Green's function: pz^2 - Re(k0^2 + i eps) for its 16 z
   float pz2[16];
 #pragma unroll
@@ -165,7 +167,7 @@ __global__ void __launch_bounds__(PencilTile<NO, TY, S>::kThreads, 2)
       // the exchanges go through the tile's own buffer (each starts with a
       // block barrier, so every input has been read before it is overwritten)
       fast::RowLine L{buf + yl, TY};
-      fast::line_fft<NO, false>(v, L, p, a.po.tw, fast::SyncBlock{});
+      fast::line_fft_tw2<NO, false>(v, L, p, wt, fast::SyncBlock{});
       // f_g0_scalar with the 1/N of ifftn: E ./ (px^2 + py^2 + (pz^2 - k02e))
       const float py = a.w.pye[yt * TY + yl];
       const float pxm = a.w.pxe[mid];
@@ -181,7 +183,7 @@ __global__ void __launch_bounds__(PencilTile<NO, TY, S>::kThreads, 2)
         }
       }
       refill();
-      fast::line_fft<NO, true>(v, L, p, a.po.tw, fast::SyncBlock{});
+      fast::line_fft_tw2<NO, true>(v, L, p, wt, fast::SyncBlock{});
       if (a.pstd)
 #pragma unroll
         for (int m = 0; m < 16; ++m) v[m].y = -v[m].y;
@@ -250,6 +252,9 @@ __global__ void __launch_bounds__(PencilTile<NO, TY, S>::kThreads, 2)
   const int mine = blockIdx.x < ntiles ? (ntiles - 1 - blockIdx.x) / G + 1 : 0;
   if (tid == 0)
     for (int i = 0; i < S - 1 && i < mine; ++i) issue(blockIdx.x + i * G, i);
+  // the second stage's twiddles of this thread, the same for every tile
+  float2 wt[16];
+  fast::load_tw2<NO>(wt, p, twx);
   const long long limit = wait_clocks > 0 ? wait_clocks : kWaitClocks;
   int i = 0;
   bool ok = true;
@@ -280,7 +285,7 @@ __global__ void __launch_bounds__(PencilTile<NO, TY, S>::kThreads, 2)
     // tile i + S - 1 goes into the buffer of tile i - 1 once its store has read it
     refill();
     if (live) {
-      fast::line_fft<NO, INV>(v, fast::RowLine{buf + yl, TY}, p, twx, fast::SyncBlock{});
+      fast::line_fft_tw2<NO, INV>(v, fast::RowLine{buf + yl, TY}, p, wt, fast::SyncBlock{});
 #pragma unroll
       for (int m = 0; m < 16; ++m) buf[(p + P * m) * TY + yl] = v[m];
       asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
