@@ -50,16 +50,21 @@ CASES = {
     "256_cluster8": ((224, 224, 16), [16, 16, 8], CLUSTER),
     # 16-block clusters: K1's half of the exchange pushed (kf_plane_fused_push)
     "256_cluster16": ((224, 224, 16), [16, 16, 8], dict(CLUSTER, WAVESIM_B200_CLUSTER="16")),
-    # 192-point planes on 6 blocks (km_plane_fused), scalar and vector
-    "192_cluster6": ((160, 160, 8), [16, 16, 4], None),
-    "192_cluster6_vector": ((160, 160, 4), [16, 16, 2], "vector"),
+    # mixed-radix planes, split step (kt_xpencil_m, kmc_col_step): 192, scalar and vector, and 96
+    "192_split": ((160, 160, 8), [16, 16, 4], None),
+    "192_split_vector": ((160, 160, 4), [16, 16, 2], "vector"),
+    "192_split_x16": ((160, 160, 8), [16, 16, 4], {"WAVESIM_B200_XTY": "16"}),
+    "96_split": ((64, 64, 32), [16, 16, 16], None),
+    # 192-point planes on 6 blocks (km_plane_fused), scalar
+    "192_cluster6": ((160, 160, 8), [16, 16, 4], CLUSTER),
+    "192_cluster6_vector": ((160, 160, 4), [16, 16, 2], ("vector", CLUSTER)),
     # K3's rows by per-thread loads instead of one tensor copy (kf_plane_fused)
     "128_cluster2_loads": ((96, 96, 96), [16, 16, 16], dict(CLUSTER, WAVESIM_B200_FUSED_TMA="0")),
     "256_cluster8_loads": ((224, 224, 16), [16, 16, 8], dict(CLUSTER, WAVESIM_B200_FUSED_TMA="0")),
     # 96^2 planes on one block (km_plane_fused with a cluster of 1)
-    "96_one_block": ((64, 64, 32), [16, 16, 16], None),
-    "192_cluster6_loads": ((160, 160, 8), [16, 16, 4], {"WAVESIM_B200_FUSED_TMA": "0"}),
-    "96_one_block_loads": ((64, 64, 32), [16, 16, 16], {"WAVESIM_B200_FUSED_TMA": "0"}),
+    "96_one_block": ((64, 64, 32), [16, 16, 16], CLUSTER),
+    "192_cluster6_loads": ((160, 160, 8), [16, 16, 4], dict(CLUSTER, WAVESIM_B200_FUSED_TMA="0")),
+    "96_one_block_loads": ((64, 64, 32), [16, 16, 16], dict(CLUSTER, WAVESIM_B200_FUSED_TMA="0")),
 }
 
 
@@ -67,8 +72,8 @@ CASES = {
 @pytest.mark.parametrize("use_graph", [True, False])
 def test_fused_loop_is_bit_identical(gpu, name, use_graph):
     shape, bw, env = CASES[name]
-    vector = env == "vector"
-    env = None if vector else env
+    vector = env == "vector" or (isinstance(env, tuple) and env[0] == "vector")
+    env = env[1] if isinstance(env, tuple) else (None if vector else env)
     n = medium(shape)
     opt = {"lambda": 1.0, "pixel_size": 0.125 if vector else 0.25, "boundary_widths": bw,
            "energy_threshold": 1e-3, "max_iterations": 48, "use_graph": use_graph}

@@ -128,6 +128,7 @@ static FastInner mixed_inner() {
               G::smem, G::smem, G::smem};
   f.fused = (const void*)mixed::km_plane_fused<PL, C>;
   f.fused_tma = (const void*)mixed::km_plane_fused_tma<PL, C>;
+  f.col_step = (const void*)mixed::kmc_col_step<PL, C>;
   f.smem_fused = G::smem;
   static_assert((size_t)PL::N * G::LR * sizeof(float2) + 128 <= G::smem, "the dense row tile fits");
   return f;
@@ -179,10 +180,17 @@ static XPencil x_pencil() {
   return XPencil{NO, TY, S, (const void*)tma::kt_xpencil<NO, TY, S, false>,
                  (const void*)tma::kt_xpencil<NO, TY, S, true>, PT::smem, PT::kThreads};
 }
+template <class PL, int TY, int S>
+static XPencil x_pencil_m() {
+  using PT = tma::MixedXTile<PL, TY, S>;
+  return XPencil{PL::N, TY, S, (const void*)tma::kt_xpencil_m<PL, TY, S, false>,
+                 (const void*)tma::kt_xpencil_m<PL, TY, S, true>, PT::smem, PT::kThreads};
+}
 static const std::vector<XPencil>& x_pencil_table() {
   // the first match of (no, ty) is the default
   static const std::vector<XPencil> t = {x_pencil<64, 16, 3>(), x_pencil<128, 16, 3>(), x_pencil<256, 8, 4>(),
-                                         x_pencil<256, 16, 3>()};
+                                         x_pencil<256, 16, 3>(), x_pencil_m<Plan192, 8, 4>(),
+                                         x_pencil_m<Plan192, 16, 3>(), x_pencil_m<Plan96, 16, 3>()};
   return t;
 }
 using Plan192t = mixed::Plan<192, 12, 12, 4, 4>;

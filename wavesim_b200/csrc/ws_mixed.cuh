@@ -742,5 +742,108 @@ __global__ void __launch_bounds__(kThreads, 2)
   }
 }
 
+// The column pass of the split fused step (see fast::kc_col_step) for the
+// mixed-radix planes: the columns of block (plane, rank) of km_plane_fused,
+// the same arithmetic in the same order and the same energy partial, with
+// the y ramps of both wiggles read from shared memory.
+template <class PL, int C>
+__global__ void __launch_bounds__(kThreads, 2)
+    kmc_col_step(InnerArgs a, Wig w1, const float2* __restrict__ src1, float2 A, float2* __restrict__ T,
+                 float2* __restrict__ dE, float2* __restrict__ E, const float2* __restrict__ gamma,
+                 const DevState* __restrict__ st, double* __restrict__ partials) {
+  using G = MGeom<PL, C>;
+  constexpr int N = PL::N, EL = PL::E, P = PL::P, M = G::M, LPR = G::LPR;
+  const int rhs = blockIdx.x / a.bpr, bid = blockIdx.x - rhs * a.bpr;
+  st += rhs;
+  if (load_done(st)) return;
+  const bool acc_now = !a.acc2 || (__ldcg(&st->it) & 1) == 0;
+  T += rhs * a.fstride;
+  dE += rhs * a.fstride;
+  E += rhs * a.fstride;
+  if (src1) src1 += rhs * a.fstride;
+  partials += (long long)rhs * a.bpr;
+  __shared__ float2 sm[LPR * G::CS];
+  __shared__ float2 sgy[2 * N];
+  __shared__ float red[kThreads / 32];
+  const int tid = threadIdx.x;
+  for (int i = tid; i < N; i += kThreads) {
+    sgy[i] = a.w.gy[i];
+    sgy[N + i] = w1.gy[i];
+  }
+  __syncthreads();
+  const Geom& g = a.g;
+  const int nx = g.nx;
+  const int rank = (int)(bid % C), plane = bid / C;
+  const int x0 = rank * M, z = plane % g.nz, comp = plane / g.nz;
+  const long long colbase = (long long)plane * nx + x0;
+  const float2 gzz = a.w.gz[z];
+  const float2 gzz1 = w1.gz[z];
+  float esum = 0.f;
+  for (int c0 = 0; c0 < M; c0 += LPR) {
+    const int cl = tid / P, cc = c0 + cl, p = tid % P;
+    const int x = x0 + cc;
+    const long long gcol = (colbase + cc) * N;
+    float2* __restrict__ Tc = T + gcol;
+    fast::ColLine L{sm + cl * G::CS};
+    float2 v[EL];
+#pragma unroll
+    for (int r = 0; r < EL; ++r) v[r] = Tc[p + P * r];
+    line_fft<PL, true>(v, L, p, a.py.tw, typename LineSync<P>::type{});
+    const float2 gxz = cmul(a.w.gx[x], gzz);
+    const bool in_xzc =
+        x >= g.r0[1] && x < g.r1[1] && z >= g.r0[2] && z < g.r1[2] && comp >= g.r0[3] && comp < g.r1[3];
+    const float2* __restrict__ gmc = gamma + (gcol - (long long)comp * g.npts);
+    float2* __restrict__ dEc = dE + gcol;
+    float2* __restrict__ Ec = E + gcol;
+    constexpr int H = EL / 2;
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      float2 gm[H], d0[H], e0[H];
+#pragma unroll
+      for (int i = 0; i < H; ++i) {
+        const int y = p + P * (H * h + i);
+        gm[i] = gmc[y];
+        d0[i] = dEc[y];
+        e0[i] = acc_now ? Ec[y] : make_float2(0.f, 0.f);
+      }
+#pragma unroll
+      for (int i = 0; i < H; ++i) {
+        const int m = H * h + i;
+        const int y = p + P * m;
+        const float2 ep = cmul_conj(cmul_conj(v[m], gxz), sgy[y]);
+        const float2 one_m = make_float2(1.f - kAlpha * gm[i].x, -kAlpha * gm[i].y);
+        const float2 t = cmul(cmul(gm[i], gm[i]), ep);
+        const float2 dn = cadd(cmul(one_m, d0[i]), make_float2(kAlpha * t.y, -kAlpha * t.x));
+        dEc[y] = dn;
+        if (acc_now) Ec[y] = cadd(e0[i], a.acc2 ? cadd(d0[i], dn) : dn);
+        if (in_xzc && y >= g.r0[0] && y < g.r1[0]) esum = fmaf(dn.x, dn.x, fmaf(dn.y, dn.y, esum));
+        v[m] = dn;
+      }
+    }
+    const float2 gxz1 = cmul(w1.gx[x], gzz1);
+    const float2* __restrict__ sr = src1 ? src1 + gcol : nullptr;
+#pragma unroll
+    for (int m = 0; m < EL; ++m) {
+      const int y = p + P * m;
+      float2 e = v[m];
+      if (sr) e = cadd(e, cmul(A, sr[y]));
+      v[m] = cmul(cmul(e, gxz1), sgy[N + y]);
+    }
+    line_fft<PL, false>(v, L, p, a.py.tw, typename LineSync<P>::type{});
+#pragma unroll
+    for (int m = 0; m < EL; ++m) Tc[p + P * m] = v[m];
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) esum += __shfl_xor_sync(0xffffffffu, esum, o);
+  if ((tid & 31) == 0) red[tid >> 5] = esum;
+  __syncthreads();
+  if (tid < 32) {
+    float v = tid < kThreads / 32 ? red[tid] : 0.f;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    if (tid == 0) partials[bid] = (double)v;
+  }
+}
+
 }  // namespace mixed
 }  // namespace ws

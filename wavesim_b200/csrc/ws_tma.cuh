@@ -303,6 +303,101 @@ __global__ void __launch_bounds__(PencilTile<NO, TY, S>::kThreads, 2)
   if (tid == 0) bulk_wait_all();
 }
 
+// kt_xpencil for the mixed-radix lines (ws_mixed.cuh): TY y of one x line
+// of N = PL::N points per tile, PL::E elements per thread.
+template <class PL, int TY, int S>
+struct MixedXTile {
+  static constexpr int NO = PL::N, P = PL::P, E = PL::E;
+  static_assert(NO <= 256, "a TMA box dimension holds at most 256 elements");
+  static_assert(2 * TY * 4 % 16 == 0 && 2 * TY <= 256, "inner box extent");
+  static constexpr int kThreads = TY * P;
+  static constexpr unsigned kTileBytes = NO * TY * sizeof(float2);
+  static constexpr size_t smem = S * (size_t)kTileBytes + 128;
+};
+
+template <class PL, int TY, int S, bool INV>
+__global__ void __launch_bounds__(MixedXTile<PL, TY, S>::kThreads, 2)
+    kt_xpencil_m(const __grid_constant__ CUtensorMap tmap, Geom g, const float2* __restrict__ twx,
+                 const DevState* __restrict__ st, int ntiles, long long wait_clocks, int* __restrict__ err) {
+  using PT = MixedXTile<PL, TY, S>;
+  constexpr int NO = PT::NO, P = PT::P, E = PT::E;
+  extern __shared__ uint8_t smem_raw[];
+  float2* const buf0 = reinterpret_cast<float2*>((reinterpret_cast<uintptr_t>(smem_raw) + 127) & ~(uintptr_t)127);
+  __shared__ __align__(8) uint64_t full[S];
+  const int tid = threadIdx.x;
+  const int yl = tid % TY, p = tid / TY;
+  const int nyt = g.ny / TY;
+  const int nzc = g.nz * g.nc;
+  const int per_rhs = nyt * nzc;
+  if (tid == 0) {
+#pragma unroll
+    for (int b = 0; b < S; ++b) asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(fast::smem_addr(&full[b])));
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  __syncthreads();
+  auto coords = [&](int t, int& rhs, int& zc, int& yt) {
+    rhs = t / per_rhs;
+    const int r = t - rhs * per_rhs;
+    zc = r / nyt;
+    yt = r - zc * nyt;
+  };
+  auto issue = [&](int t, int b) {
+    int rhs, zc, yt;
+    coords(t, rhs, zc, yt);
+    expect_bytes(&full[b], PT::kTileBytes);
+    load_3d(fast::smem_addr(buf0 + b * NO * TY), &tmap, 2 * TY * yt, 0, rhs * nzc + zc, fast::smem_addr(&full[b]));
+  };
+  const int G = gridDim.x;
+  const int mine = blockIdx.x < ntiles ? (ntiles - 1 - blockIdx.x) / G + 1 : 0;
+  if (tid == 0)
+    for (int i = 0; i < S - 1 && i < mine; ++i) issue(blockIdx.x + i * G, i);
+  const long long limit = wait_clocks > 0 ? wait_clocks : kWaitClocks;
+  int i = 0;
+  bool ok = true;
+  for (; i < mine; ++i) {
+    const int b = i % S;
+    const int t = blockIdx.x + i * G;
+    float2* const buf = buf0 + b * NO * TY;
+    ok = wait_parity(&full[b], (uint32_t)((i / S) & 1), limit);
+    if (__syncthreads_or(!ok)) {
+      ok = false;
+      break;
+    }
+    auto refill = [&]() {
+      const int nxt = i + S - 1;
+      if (tid == 0 && nxt < mine) {
+        bulk_wait_read_0();
+        issue(blockIdx.x + nxt * G, nxt % S);
+      }
+    };
+    int rhs, zc, yt;
+    coords(t, rhs, zc, yt);
+    const bool live = !load_done(st + rhs);
+    float2 v[E];
+    if (live) {
+#pragma unroll
+      for (int q = 0; q < E; ++q) v[q] = buf[(p + P * q) * TY + yl];
+    }
+    refill();
+    if (live) {
+      mixed::line_fft<PL, INV>(v, fast::RowLine{buf + yl, TY}, p, twx, fast::SyncBlock{});
+#pragma unroll
+      for (int m = 0; m < E; ++m) buf[(p + P * m) * TY + yl] = v[m];
+      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    }
+    __syncthreads();
+    if (tid == 0 && live) {
+      store_3d(&tmap, 2 * TY * yt, 0, rhs * nzc + zc, fast::smem_addr(buf));
+      bulk_commit();
+    }
+  }
+  if (!ok) {
+    if (tid == 0) atomicExch(err, 1);
+    for (int j = i; j < mine && j < i + S - 1; ++j) (void)wait_parity(&full[j % S], (uint32_t)((j / S) & 1));
+  }
+  if (tid == 0) bulk_wait_all();
+}
+
 // The vector form (WaveSimVector, 3 components): a tile is the three
 // component boxes of the same (x, y tile), at z offsets c Nz of the map
 // {2 Ny floats, Nx, Nz Nc nrhs}; each line is transformed with the
