@@ -188,18 +188,20 @@ static XPencil x_pencil_m() {
 }
 static const std::vector<XPencil>& x_pencil_table() {
   // the first match of (no, ty) is the default
-  static const std::vector<XPencil> t = {x_pencil<64, 16, 3>(), x_pencil<128, 16, 3>(), x_pencil<256, 8, 4>(),
-                                         x_pencil<256, 16, 3>(), x_pencil_m<Plan192, 8, 4>(),
+  static const std::vector<XPencil> t = {x_pencil<64, 16, 3>(), x_pencil<128, 16, 3>(), x_pencil<256, 8, 3>(),
+                                         x_pencil<256, 8, 4>(), x_pencil<256, 16, 3>(), x_pencil_m<Plan192, 8, 4>(),
                                          x_pencil_m<Plan192, 16, 3>(), x_pencil_m<Plan96, 16, 3>()};
   return t;
 }
 using Plan192t = mixed::Plan<192, 12, 12, 4, 4>;
 static const std::vector<TmaPencil>& tma_pencil_table() {
   // the first match of (no, ty) is the default; the autotuner tries the rest
-  // (at 256: 8 y x 4 stages measured 0.072 ms against 0.074 for 16 x 3, 0.081
-  // for 4 x 4 and 0.096 for 8 x 6)
+  // (at 256: 8 y x 3 stages, 4 blocks of 128 threads per SM at 128 registers,
+  // measured 0.0667 ms against 0.0732 for 8 x 4 stages at 3 blocks per SM,
+  // 0.070 for 16 x 3, 0.081 for 4 x 4 and 0.096 for 8 x 6)
   static const std::vector<TmaPencil> t = {tma_pencil<64, 16, 3>(), tma_pencil<128, 16, 3>(),
-                                           tma_pencil<256, 8, 4>(),  tma_pencil<256, 16, 3>(),
+                                           tma_pencil<256, 8, 3>(),  tma_pencil<256, 8, 4>(),
+                                           tma_pencil<256, 16, 3>(),
                                            tma_pencil<256, 16, 2>(), tma_pencil<256, 8, 6>(),
                                            tma_pencil<256, 4, 4>(),
                                            // 192 x 3 components: 8 y x 3 stages measured 0.131 ms against
@@ -381,11 +383,12 @@ static int make_layout(const Geom& g, Layout& L, std::string& why, const LayoutC
   // WAVESIM_B200_STEP=cluster keeps the one-kernel step with the cluster
   // exchange, WAVESIM_B200_XTY picks the x pencils' y tile
   const char* step = std::getenv("WAVESIM_B200_STEP");
-  int want_xty = 0;
+  int want_xty = 0, want_xs = 0;  // WAVESIM_B200_XTY / _XSTAGES: the y tile and stages of the x pencils
   if (const char* e = std::getenv("WAVESIM_B200_XTY")) want_xty = std::atoi(e);
+  if (const char* e = std::getenv("WAVESIM_B200_XSTAGES")) want_xs = std::atoi(e);
   if (L.mode3d && L.fi && L.fi->col_step && !(step && std::strcmp(step, "cluster") == 0))
     for (const XPencil& f : x_pencil_table())
-      if (f.no == g.nx && g.ny % f.ty == 0 && (!want_xty || f.ty == want_xty)) {
+      if (f.no == g.nx && g.ny % f.ty == 0 && (!want_xty || f.ty == want_xty) && (!want_xs || f.stages == want_xs)) {
         L.xp = &f;
         break;
       }

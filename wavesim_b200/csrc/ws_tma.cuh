@@ -86,10 +86,14 @@ struct PencilTile {
   static constexpr unsigned kTileBytes = NO * TY * sizeof(float2);
   // S tile buffers, [z][y] as the TMA box lands (128-byte aligned)
   static constexpr size_t smem = S * (size_t)kTileBytes + 128;
+  // blocks per SM the tiles leave room for (228 KB of shared memory, 1 KB
+  // reserved per block, at most 4): the register bound of the kernels
+  static constexpr int kMinBlocks = (int)(228 * 1024 / (smem + 3 * 1024)) >= 4 ? 4
+                                    : ((int)(228 * 1024 / (smem + 3 * 1024)) >= 3 ? 3 : 2);
 };
 
 template <int NO, int TY, int S>
-__global__ void __launch_bounds__(PencilTile<NO, TY, S>::kThreads, 2)
+__global__ void __launch_bounds__(PencilTile<NO, TY, S>::kThreads, PencilTile<NO, TY, S>::kMinBlocks)
     kt_pencil(const __grid_constant__ CUtensorMap tmap, OuterArgs a, const DevState* __restrict__ st, int ntiles,
               int* __restrict__ err) {
   using PT = PencilTile<NO, TY, S>;
@@ -217,7 +221,7 @@ __global__ void __launch_bounds__(PencilTile<NO, TY, S>::kThreads, 2)
 // plane kernels' line_fft and x twiddles, so the result is theirs bit for
 // bit.  The map covers this GPU's T only; no multicast.
 template <int NO, int TY, int S, bool INV>
-__global__ void __launch_bounds__(PencilTile<NO, TY, S>::kThreads, 2)
+__global__ void __launch_bounds__(PencilTile<NO, TY, S>::kThreads, PencilTile<NO, TY, S>::kMinBlocks)
     kt_xpencil(const __grid_constant__ CUtensorMap tmap, Geom g, const float2* __restrict__ twx,
                const DevState* __restrict__ st, int ntiles, long long wait_clocks, int* __restrict__ err) {
   using PT = PencilTile<NO, TY, S>;
