@@ -618,14 +618,16 @@ def run_start_quality(sim, h, s, blocks, opts, torch, dev, plain_it):
         rc_, rw_ = C.c_double(), C.c_double()
         _lib.check(_lib.lib.ws_solver_warm_report(h, 0, None, None, C.byref(disc)))
         _lib.check(_lib.lib.ws_solver_warm_residual(h, 0, C.byref(rc_), C.byref(rw_)))
-        it = int(n_it.value) + 2
+        # a discarded start stops after the two probe iterations and is rerun cold
+        it = int(n_it.value) + 2 + (plain_it if disc.value else 0)
         out.append({"start_error": a, "iterations": it, "discarded": bool(disc.value),
                     "initial_residual_ratio": rw_.value / rc_.value if rc_.value > 0 else None,
                     "speedup_at_zero_inference": plain_it / it})
     o2.initial_field = None
     return {"converged_field_iterations": tight_it, "plain_iterations": plain_it, "curve": out,
             "note": "start = converged field (threshold 1e-7) + smooth noise of relative L2 amplitude start_error; "
-                    "speed-up = plain iterations / (warm loop iterations + 2 probe iterations)"}
+                    "speed-up = plain iterations / (warm loop iterations + 2 probe iterations, + the cold "
+                    "rerun of a discarded start)"}
 
 
 def run_media(args):
