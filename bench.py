@@ -51,7 +51,8 @@ def parse():
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-warm", action="store_true", help="skip the learned warm-start leg")
     p.add_argument("--batch", type=int, default=4, help="right-hand sides of the batched leg (0: skip)")
-    p.add_argument("--media", type=int, default=8, help="media of mixed sizes in the concurrent leg (0: skip)")
+    p.add_argument("--media", type=int, default=48, help="media of mixed sizes in the concurrent leg (0: skip)")
+    p.add_argument("--angles", type=int, default=128, help="plane-wave angles on the 1024^2 medium (0: skip)")
     return p.parse_args()
 
 
@@ -389,6 +390,8 @@ def run_ours(args):
             legs["start_quality"] = run_start_quality(sim, h, s, blocks, opts, torch, dev, n_iter)
         if args.media > 0:
             legs["mixed_media"] = run_media(args)
+        if args.angles > 0:
+            legs["angles_1024"] = run_angles(args)
 
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
@@ -633,11 +636,15 @@ def run_start_quality(sim, h, s, blocks, opts, torch, dev, plain_it):
 def run_media(args):
     """args.media seeded media of mixed sizes (2-D 256^2-1024^2 Gaussian
     random media with a Gaussian-beam edge source, 3-D 64^3-192^3 cubes of the
-    sphere distribution with a plane wave), set up on the device, solved one
-    at a time and then concurrently (wavesim_b200.batch.solve_many, one
-    solver stream per medium, 4 host threads); solves/s of both."""
+    sphere distribution with a plane wave), set up on the device, solved
+    (1) one at a time, (2) concurrently (wavesim_b200.batch.solve_many, one
+    solver stream per medium, 4 host threads) and (3) grouped
+    (wavesim_b200.batch.solve_media: the media of each size in one batched
+    solve, one launch per kernel for the whole group, the groups on 4 host
+    threads); solves/s of each, and the largest difference of a grouped field
+    from the medium's own solve."""
     import wavesim_b200 as ws
-    from wavesim_b200.batch import solve_many
+    from wavesim_b200.batch import group_media, solve_many, solve_media
     from wavesim_b200.workloads import PPW, gaussian_random_field, sphere_medium
     rng = np.random.default_rng(48)
     probs, sizes = [], []
@@ -661,13 +668,61 @@ def run_media(args):
         probs.append((ws.WaveSim(n, opt), src))
     setup_s = time.perf_counter() - t0
     solve_many(probs, workers=1)  # warm-up: solvers, graphs
-    _, st_seq, t_seq = solve_many(probs, workers=1)
+    E_seq, st_seq, t_seq = solve_many(probs, workers=1)
     _, st_par, t_par = solve_many(probs, workers=4)
+    _, _, _, batches = solve_media(probs, workers=4)  # warm-up: media solvers, graphs
+    E_grp, st_grp, t_grp, _ = solve_media(probs, workers=4, batches=batches)
+    diff = max(float(np.max(np.abs(a - b))) for a, b in zip(E_grp, E_seq))
+    same_it = all(a.it == b.it for a, b in zip(st_grp, st_seq))
+    groups = group_media(probs)
+    for b in batches:
+        if b is not None:
+            b.close()
     for sim, _ in probs:
         sim.close()
-    return {"media": sizes, "host_setup_s": setup_s, "iterations": [s.it - 1 for s in st_seq],
+    return {"media": sizes, "groups": [len(g) for g in groups], "host_setup_s": setup_s,
+            "iterations": [s.it - 1 for s in st_seq],
             "sequential_solves_per_s": len(probs) / t_seq, "concurrent_solves_per_s": len(probs) / t_par,
-            "speedup": t_seq / t_par, "timing": "host wall clock around the solves (set-up excluded)"}
+            "grouped_solves_per_s": len(probs) / t_grp, "speedup": t_seq / t_par,
+            "grouped_speedup": t_seq / t_grp, "grouped_max_abs_diff": diff, "grouped_same_iterations": same_it,
+            "timing": "host wall clock around the solves (set-up excluded)"}
+
+
+def run_angles(args):
+    """C5's angle sweep: args.angles plane waves at incidence angles uniform in
+    +-30 degrees on the c2 medium (2-D 1024^2, Gaussian random field), one
+    batched solve (sources generated on the device) against single solves of
+    a sample of 8 of the angles; solves/s of both."""
+    import torch
+    import wavesim_b200 as ws
+    n, opt, _, _, _ = load_workloads().CONFIGS["c2"]()
+    sim = ws.WaveSim(n, dict(opt, device_setup=True))
+    r = sim.roi
+    ny = int(r[1, 0] - r[0, 0] + 1)
+    k = 2 * np.pi / sim.lambda_ * float(opt["pixel_size"])
+    angles = np.linspace(-30, 30, args.angles)
+    waves = [ws.PlaneWave((ny, 1), [1, 1], amplitude=1.0, phase=(k * np.sin(np.radians(a)), 0.0)) for a in angles]
+    sim.exec_batch(waves[:2])  # warm-up
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    Eb, sb = sim.exec_batch(waves)
+    torch.cuda.synchronize()
+    t_b = time.perf_counter() - t0
+    sample = waves[:: max(1, len(waves) // 8)][:8]
+    sim.exec_batch(sample[:1])
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    its = []
+    for w in sample:
+        _, st = sim.exec_batch([w])
+        its.append(st[0].it - 1)
+    torch.cuda.synchronize()
+    t_s = (time.perf_counter() - t0) / len(sample)
+    sim.close()
+    return {"angles": len(waves), "grid": [int(v) for v in sim.N[:2]], "ms_batch": t_b * 1e3,
+            "ms_per_solve_batched": t_b * 1e3 / len(waves), "ms_per_solve_single": t_s * 1e3,
+            "speedup": t_s * len(waves) / t_b, "iterations": [s.it - 1 for s in sb][:: max(1, len(waves) // 8)],
+            "single_iterations": its, "timing": "host wall clock, fields copied to the host included"}
 
 
 def run_e2e(args, sim, s, keep, torch, dev):

@@ -192,6 +192,18 @@ int ws_solver_create(const int64_t N[4], const ws_complex* gamma, int64_t n_wigg
                      float epsilon, ws_complex k02e, const int64_t roi[8], int memory, int device,
                      ws_solver* out);
 
+/* ws_solver_create_media - a solver for n_media media of one grid: gammas
+ * holds n_media gamma arrays of Ny*Nx*Nz elements back to back (in
+ * `memory`); everything else - wiggles, epsilon, k02e, roi - is shared, as it
+ * is for media of one size whose refractive indices span the same range
+ * (epsilon and k0c depend only on the extremes of n^2).  It is solved with
+ * ws_solver_solve_batch, one right-hand side per medium (right-hand side r
+ * on medium r), so every kernel launch covers all the media.  No counterpart
+ * in the reference, whose callers run exec once per medium. */
+int ws_solver_create_media(const int64_t N[4], int64_t n_media, const ws_complex* gammas, int64_t n_wiggles,
+                           const ws_wiggle* wiggles, float epsilon, ws_complex k02e, const int64_t roi[8],
+                           int memory, int device, ws_solver* out);
+
 /* ws_solver_solve - runs the loop for one source.  source values live in
  * source_memory; E_out in out_memory.  diff_energy_out (host) may be NULL.
  * converged (may be NULL) receives 1 if the energy test stopped the loop. */

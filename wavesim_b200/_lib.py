@@ -68,7 +68,7 @@ class ws_solve_options(C.Structure):
 EXPORTS = [
     "ws_default_options", "ws_version", "ws_last_error", "ws_size_supported", "ws_run_algorithm",
     "ws_run_algorithm_release",
-    "ws_solver_create", "ws_solver_solve", "ws_solver_solve_batch", "ws_solver_solve_plane_waves", "ws_solver_buffers",
+    "ws_solver_create", "ws_solver_create_media", "ws_solver_solve", "ws_solver_solve_batch", "ws_solver_solve_plane_waves", "ws_solver_buffers",
     "ws_solver_time_kernels", "ws_solver_time_split",
     "ws_solver_launches_per_iteration", "ws_solver_set_wait_limit", "ws_solver_time_fused", "ws_solver_warm_report", "ws_solver_warm_residual", "ws_solver_autotune", "ws_solver_destroy",
     "ws_run_algorithm_noalloc", "ws_medium_reduce", "ws_build_gamma", "ws_setup_last_error",
@@ -112,6 +112,9 @@ def _load():
     lib.ws_solver_create.argtypes = [i64p, P, C.c_int64, C.POINTER(ws_wiggle), C.c_float, ws_complex, i64p,
                                      C.c_int, C.c_int, C.POINTER(C.c_void_p)]
     lib.ws_solver_create.restype = C.c_int
+    lib.ws_solver_create_media.argtypes = [i64p, C.c_int64, P, C.c_int64, C.POINTER(ws_wiggle), C.c_float, ws_complex,
+                                           i64p, C.c_int, C.c_int, C.POINTER(C.c_void_p)]
+    lib.ws_solver_create_media.restype = C.c_int
     lib.ws_solver_solve.argtypes = [P, C.c_int64, C.POINTER(ws_source_block), C.c_int,
                                     C.POINTER(ws_solve_options), P, C.c_int, C.POINTER(C.c_double), i64p,
                                     C.POINTER(C.c_int)]

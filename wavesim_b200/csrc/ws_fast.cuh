@@ -504,6 +504,7 @@ __global__ void __launch_bounds__(kThreads, C >= 16 ? 3 : 2)
   dE += rhs * a.fstride;
   E += rhs * a.fstride;
   partials += (long long)rhs * a.bpr;
+  gamma += rhs * a.gstride;  // a batch of media: each right-hand side has its own gamma
   extern __shared__ float2 sm[];
   __shared__ float red[kThreads / 32];
   const int tid = threadIdx.x;
@@ -704,6 +705,7 @@ __global__ void __launch_bounds__(kThreads, 2)
   E += rhs * a.fstride;
   if (src1) src1 += rhs * a.fstride;
   partials += (long long)rhs * a.bpr;
+  gamma += rhs * a.gstride;  // a batch of media: each right-hand side has its own gamma
   extern __shared__ float2 sm[];
   __shared__ float red[kThreads / 32];
   const int tid = threadIdx.x;
@@ -884,6 +886,7 @@ __global__ void __launch_bounds__(kThreads, 2)
   E += rhs * a.fstride;
   if (src1) src1 += rhs * a.fstride;
   partials += (long long)rhs * a.bpr;
+  gamma += rhs * a.gstride;  // a batch of media: each right-hand side has its own gamma
   extern __shared__ float2 sm[];
   __shared__ float red[kThreads / 32];
   const int tid = threadIdx.x;
@@ -1121,6 +1124,7 @@ __global__ void __launch_bounds__(kThreads, 2)
   E += rhs * a.fstride;
   if (src1) src1 += rhs * a.fstride;
   partials += (long long)rhs * a.bpr;
+  gamma += rhs * a.gstride;  // a batch of media: each right-hand side has its own gamma
   __shared__ float2 sm[LPR * G::CS];  // one round of lines: the transforms' exchanges
   __shared__ float red[kThreads / 32];
   const int tid = threadIdx.x;
@@ -1252,6 +1256,7 @@ __global__ void __launch_bounds__(kThreads, 2)
   E += rhs * a.fstride;
   if (src1) src1 += rhs * a.fstride;
   partials += (long long)rhs * a.bpr;
+  gamma += rhs * a.gstride;  // a batch of media: each right-hand side has its own gamma
   extern __shared__ float2 sm[];
   float2* const ct = sm;                                       // columns [x0, x0 + M), stride CS
   float2* const rt = sm + F::col_bytes / sizeof(float2);       // rows: K3's, then the pushed ones; stride CS2

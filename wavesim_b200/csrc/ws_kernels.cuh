@@ -99,6 +99,7 @@ struct InnerArgs {
   int pf;       // fast kernels: block b pulls the inputs of block b + pf into L2 (0: off)
   int acc2;     // K3: E' += dE' in pairs, every second iteration (Nw even; 0: every iteration)
   int* err;     // fast kernels: set to 1 when a cluster exchange wait gives up (may be null)
+  long long gstride;  // elements between the gammas of consecutive right-hand sides (0: one shared gamma)
 };
 
 struct OuterArgs {
@@ -344,6 +345,7 @@ __global__ void __launch_bounds__(512, 1) k_inv_inner(InnerArgs a, const float2*
   dE += rhs * a.fstride;
   E += rhs * a.fstride;
   partials += (long long)rhs * a.bpr;
+  gamma += rhs * a.gstride;  // a batch of media: each right-hand side has its own gamma
   extern __shared__ float2 sm[];
   __shared__ float red[32];
   const int tid = threadIdx.x, nthr = blockDim.x;
@@ -484,9 +486,9 @@ static __global__ void k_reset_state(DevState* st, int n) {
 // v <- gamma .* psi0 / Nw (or E'/Nw when the start is already primed); gamma
 // is shared by the components and right-hand sides (npts points each).
 static __global__ void k_warm_scale(float2* __restrict__ v, const float2* __restrict__ gamma, long long n,
-                                    long long npts, float inv_nw, int primed) {
+                                    long long npts, float inv_nw, int primed, long long fe, long long gstride) {
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
-    const float2 u = primed ? v[i] : cmul(v[i], gamma[i % npts]);
+    const float2 u = primed ? v[i] : cmul(v[i], gamma[(i / fe) * gstride + (i % fe) % npts]);
     v[i] = make_float2(u.x * inv_nw, u.y * inv_nw);
   }
 }

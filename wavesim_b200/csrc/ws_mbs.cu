@@ -421,7 +421,8 @@ struct Solver {
   std::vector<Wig> wig;
   float* d_wigf = nullptr;   // all pxe/pye/pze
   float2* d_wigc = nullptr;  // all gx/gy/gz
-  float2* d_gamma = nullptr;
+  float2* d_gamma = nullptr;      // n_media gammas of npts elements each
+  int n_media = 1;                // > 1: a batch of media, right-hand side r on gamma r
   // per right-hand side (batch of nrhs, capacity batch_cap): fields at r * field elements
   float2 *d_E = nullptr, *d_dE = nullptr, *d_T = nullptr, *d_src = nullptr;
   int batch_cap = 0;
@@ -796,6 +797,7 @@ static InnerArgs inner_args(const Solver* s, int w) {
   a.bpr = (int)s->lay.grid_inner;
   a.fstride = (long long)field_elems(s);
   a.err = s->d_err;
+  a.gstride = s->n_media > 1 ? (long long)s->g.npts : 0;
   a.pf = 0;  // K3 (and the generic kernels) measured slower with it
   // E' += dE' in pairs when every stop (a multiple of Nw) falls after an even iteration
   a.acc2 = (s->nw % 2 == 0) ? 1 : 0;
@@ -1428,6 +1430,8 @@ static int solve_batch(Solver* s, int nrhs, const int64_t* counts, const ws_sour
   ws_default_options(&opt);
   if (o) opt = *o;
   if (nrhs < 1 || nrhs > 65536) return fail(WS_ERR_INVALID_ARGUMENT, "number of right-hand sides must be in [1, 65536]");
+  if (s->n_media > 1 && nrhs != s->n_media)
+    return fail(WS_ERR_INVALID_ARGUMENT, "a solver of several media takes one right-hand side per medium");
   if (opt.max_iterations < 1 || opt.max_iterations > 100000000LL)
     return fail(WS_ERR_INVALID_ARGUMENT, "max_iterations must be in [1, 1e8]");
   if (opt.energy_interval < 1) return fail(WS_ERR_INVALID_ARGUMENT, "energy_interval must be >= 1");
@@ -1476,7 +1480,8 @@ static int solve_batch(Solver* s, int nrhs, const int64_t* counts, const ws_sour
                             s->stream));
     const long long n = fe * nrhs;
     k_warm_scale<<<(unsigned)std::min<long long>((n + 255) / 256, 8 * kNumSms), 256, 0, s->stream>>>(
-        s->d_init, s->d_gamma, n, s->g.npts, 1.0f / (float)s->nw, opt.initial_is_eprime ? 1 : 0);
+        s->d_init, s->d_gamma, n, s->g.npts, 1.0f / (float)s->nw, opt.initial_is_eprime ? 1 : 0,
+        (long long)field_elems(s), s->n_media > 1 ? (long long)s->g.npts : 0LL);
     WS_CUDA(cudaGetLastError());
   }
   if (opt.use_graph && !want_cb) {
@@ -1557,7 +1562,8 @@ static int solve_batch(Solver* s, int nrhs, const int64_t* counts, const ws_sour
           dst = s->d_out;
         }
         const long long blocks = std::min<long long>(((long long)n + 255) / 256, 8 * kNumSms);
-        k_finalize<<<(unsigned)blocks, 256, 0, s->stream>>>(s->d_E + F * r, s->d_gamma, g, dst);
+        k_finalize<<<(unsigned)blocks, 256, 0, s->stream>>>(
+            s->d_E + F * r, s->d_gamma + (s->n_media > 1 ? (long long)r * s->g.npts : 0LL), g, dst);
         WS_CUDA(cudaGetLastError());
         if (out_memory != WS_DEVICE)
           WS_CUDA(cudaMemcpyAsync((float2*)E_out + n * r, s->d_out, n * sizeof(float2), k, s->stream));
@@ -1632,6 +1638,35 @@ int ws_solver_create(const int64_t N[4], const ws_complex* gamma, int64_t n_wigg
   Solver* s = nullptr;
   const int rc = create_solver(N, gamma, n_wiggles, wiggles, epsilon, k02e, roi, memory, device, &s);
   if (rc) return rc;
+  *out = reinterpret_cast<ws_solver>(s);
+  return WS_OK;
+}
+
+int ws_solver_create_media(const int64_t N[4], int64_t n_media, const ws_complex* gammas, int64_t n_wiggles,
+                           const ws_wiggle* wiggles, float epsilon, ws_complex k02e, const int64_t roi[8], int memory,
+                           int device, ws_solver* out) {
+  if (!out) return fail(WS_ERR_INVALID_ARGUMENT, "null output handle");
+  *out = nullptr;
+  if (n_media < 1 || n_media > 65536) return fail(WS_ERR_INVALID_ARGUMENT, "n_media must be in [1, 65536]");
+  if (!gammas) return fail(WS_ERR_INVALID_ARGUMENT, "null gammas");
+  Solver* s = nullptr;
+  const int rc = create_solver(N, gammas, n_wiggles, wiggles, epsilon, k02e, roi, memory, device, &s);
+  if (rc) return rc;
+  if (n_media > 1) {
+    const size_t bytes = (size_t)s->g.npts * sizeof(float2);
+    cudaFree(s->d_gamma);
+    s->d_gamma = nullptr;
+    cudaError_t e = cudaMalloc(&s->d_gamma, bytes * (size_t)n_media);
+    if (e == cudaSuccess)
+      e = cudaMemcpy(s->d_gamma, gammas, bytes * (size_t)n_media,
+                     memory == WS_DEVICE ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) {
+      destroy_solver(s);
+      return fail(e == cudaErrorMemoryAllocation ? WS_ERR_OUT_OF_MEMORY : WS_ERR_CUDA,
+                  std::string("media gammas: ") + cudaGetErrorString(e));
+    }
+    s->n_media = (int)n_media;
+  }
   *out = reinterpret_cast<ws_solver>(s);
   return WS_OK;
 }

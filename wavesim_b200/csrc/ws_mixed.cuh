@@ -281,6 +281,7 @@ __global__ void __launch_bounds__(kThreads, 2)
   dE += rhs * a.fstride;
   E += rhs * a.fstride;
   partials += (long long)rhs * a.bpr;
+  gamma += rhs * a.gstride;  // a batch of media: each right-hand side has its own gamma
   extern __shared__ float2 sm[];
   __shared__ float red[kThreads / 32];
   const int tid = threadIdx.x;
@@ -402,6 +403,7 @@ __global__ void __launch_bounds__(kThreads, 2)
   E += rhs * a.fstride;
   if (src1) src1 += rhs * a.fstride;
   partials += (long long)rhs * a.bpr;
+  gamma += rhs * a.gstride;  // a batch of media: each right-hand side has its own gamma
   extern __shared__ float2 sm[];
   __shared__ float red[kThreads / 32];
   const int tid = threadIdx.x;
@@ -560,6 +562,7 @@ __global__ void __launch_bounds__(kThreads, 2)
   E += rhs * a.fstride;
   if (src1) src1 += rhs * a.fstride;
   partials += (long long)rhs * a.bpr;
+  gamma += rhs * a.gstride;  // a batch of media: each right-hand side has its own gamma
   extern __shared__ float2 sm[];
   __shared__ float red[kThreads / 32];
   const int tid = threadIdx.x;
@@ -762,6 +765,7 @@ __global__ void __launch_bounds__(kThreads, 2)
   E += rhs * a.fstride;
   if (src1) src1 += rhs * a.fstride;
   partials += (long long)rhs * a.bpr;
+  gamma += rhs * a.gstride;  // a batch of media: each right-hand side has its own gamma
   __shared__ float2 sm[LPR * G::CS];
   __shared__ float2 sgy[2 * N];
   __shared__ float red[kThreads / 32];
