@@ -1,7 +1,7 @@
-"""The fused loop (K3 of each iteration and K1 of the next: on power-of-two
-planes the split step - x pencils, the column pass, x pencils - and with
-WAVESIM_B200_STEP=cluster, or on 192- and 96-point planes, one kernel on a
-cluster) against the three separate kernels (WAVESIM_B200_FUSE=0).  Both do
+"""The fused loop (K3 of each iteration and K1 of the next: on 3-D planes the
+split step - x pencils, the column pass, x pencils - or with
+WAVESIM_B200_STEP=cluster one kernel on a cluster; on 2-D grids the column
+pass alone) against the three separate kernels (WAVESIM_B200_FUSE=0).  Both do
 the same arithmetic in the same order, so the fields must agree bit for bit:
 cold, warm, batched, with the host loop and with the CUDA graph."""
 import os
@@ -45,6 +45,10 @@ CASES = {
     "256_split": ((224, 224, 16), [16, 16, 8], None),
     "256_split_x16": ((224, 224, 16), [16, 16, 8], {"WAVESIM_B200_XTY": "16"}),
     "256_split_vector": ((224, 224, 8), [16, 16, 4], "vector"),
+    # 2-D: K2 and the column pass (kc_col_step2d)
+    "2d_256": ((224, 224), [16, 16], None),
+    "2d_1024": ((960, 960), [32, 32], None),
+    "2d_512x120": ((448, 100), [32, 10], None),
     # the one-kernel step with the cluster exchange
     "128_cluster2": ((96, 96, 96), [16, 16, 16], CLUSTER),
     "256_cluster8": ((224, 224, 16), [16, 16, 8], CLUSTER),

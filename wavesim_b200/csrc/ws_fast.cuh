@@ -1221,6 +1221,135 @@ __global__ void __launch_bounds__(kThreads, 2)
   }
 }
 
+// The 2-D form: K2 already transforms along x, so K3 of iteration k and K1
+// of iteration k + 1 meet in one column pass, and an iteration is K2 plus
+// this kernel.  Block bid covers the 2-D column kernels' columns bid ncols
+// ... bid ncols + ncols - 1 (column col = x + Nx c), the same lines and
+// arithmetic as kf_plane_inv / kf_plane_fwd on a column (so the same
+// fields bit for bit) and their energy partial.  Idle lanes of a partial
+// last block work on a scratch column.  Dynamic shared memory:
+// (LPR + 1) columns and the two y ramps (smem_col_step2d).
+template <int N>
+__host__ __device__ constexpr size_t smem_col_step2d() {
+  return ((size_t)(kThreads / (N / 16) + 1) * PlaneGeom<N, 1, false>::CS + 2 * N) * sizeof(float2);
+}
+template <int N>
+__global__ void __launch_bounds__(kThreads, 2)
+    kc_col_step2d(InnerArgs a, Wig w1, const float2* __restrict__ src1, float2 A, float2* __restrict__ T,
+                  float2* __restrict__ dE, float2* __restrict__ E, const float2* __restrict__ gamma,
+                  const DevState* __restrict__ st, double* __restrict__ partials) {
+  using G = PlaneGeom<N, 1, false>;
+  constexpr int P = G::P, LPR = G::LPR;
+  const int rhs = blockIdx.x / a.bpr, bid = blockIdx.x - rhs * a.bpr;
+  st += rhs;
+  if (load_done(st)) return;
+  const bool acc_now = !a.acc2 || (__ldcg(&st->it) & 1) == 0;
+  T += rhs * a.fstride;
+  dE += rhs * a.fstride;
+  E += rhs * a.fstride;
+  if (src1) src1 += rhs * a.fstride;
+  partials += (long long)rhs * a.bpr;
+  gamma += rhs * a.gstride;  // a batch of media: each right-hand side has its own gamma
+  extern __shared__ float2 sm[];
+  float2* const sgy = sm + (LPR + 1) * G::CS;
+  __shared__ float red[kThreads / 32];
+  const int tid = threadIdx.x;
+  for (int i = tid; i < N; i += kThreads) {
+    sgy[i] = a.w.gy[i];
+    sgy[N + i] = w1.gy[i];
+  }
+  __syncthreads();
+  const Geom& g = a.g;
+  const int nx = g.nx;
+  const int M = a.ncols;
+  const long long colbase = (long long)bid * M;
+  const int ncol = (int)min((long long)M, (long long)nx * g.nc - colbase);
+  const int z = 0;
+  const float2 gzz = a.w.gz[z];
+  const float2 gzz1 = w1.gz[z];
+  float esum = 0.f;
+  for (int c0 = 0; c0 < ncol; c0 += LPR) {
+    const int cl = tid / P, cc = c0 + cl, p = tid % P;
+    const bool live = cc < ncol;
+    const long long col = colbase + cc;
+    const long long gcol = col * N;
+    ColLine L{sm + (live ? cl : LPR) * G::CS};
+    float2 v[16];
+    if (live) {
+#pragma unroll
+      for (int r = 0; r < 16; ++r) v[r] = T[gcol + p + P * r];
+    } else {
+#pragma unroll
+      for (int r = 0; r < 16; ++r) v[r] = make_float2(0.f, 0.f);
+    }
+    if constexpr (P <= 32) {
+      line_fft<N, true>(v, L, p, a.py.tw, SyncWarp{});
+    } else {
+      line_fft<N, true>(v, L, p, a.py.tw, SyncBlock{});
+    }
+    if (live) {
+      const int x = (int)(col % nx), c = (int)(col / nx);
+      const float2 gxz = cmul(a.w.gx[x], gzz);
+      const bool in_xzc = x >= g.r0[1] && x < g.r1[1] && z >= g.r0[2] && z < g.r1[2] && c >= g.r0[3] && c < g.r1[3];
+      const float2* __restrict__ gmc = gamma + (gcol - (long long)c * g.npts);
+      float2* __restrict__ dEc = dE + gcol;
+      float2* __restrict__ Ec = E + gcol;
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        float2 gm[8], d0[8], e0[8];
+#pragma unroll
+        for (int i = 0; i < 8; ++i) {
+          const int y = p + P * (8 * h + i);
+          gm[i] = gmc[y];
+          d0[i] = dEc[y];
+          e0[i] = acc_now ? Ec[y] : make_float2(0.f, 0.f);
+        }
+#pragma unroll
+        for (int i = 0; i < 8; ++i) {
+          const int m = 8 * h + i;
+          const int y = p + P * m;
+          const float2 ep = cmul_conj(cmul_conj(v[m], gxz), sgy[y]);
+          const float2 one_m = make_float2(1.f - kAlpha * gm[i].x, -kAlpha * gm[i].y);
+          const float2 t = cmul(cmul(gm[i], gm[i]), ep);
+          const float2 dn = cadd(cmul(one_m, d0[i]), make_float2(kAlpha * t.y, -kAlpha * t.x));
+          dEc[y] = dn;
+          if (acc_now) Ec[y] = cadd(e0[i], a.acc2 ? cadd(d0[i], dn) : dn);
+          if (in_xzc && y >= g.r0[0] && y < g.r1[0]) esum = fmaf(dn.x, dn.x, fmaf(dn.y, dn.y, esum));
+          v[m] = dn;
+        }
+      }
+      const float2 gxz1 = cmul(w1.gx[x], gzz1);
+      const float2* __restrict__ sr = src1 ? src1 + gcol : nullptr;
+#pragma unroll
+      for (int m = 0; m < 16; ++m) {
+        const int y = p + P * m;
+        float2 e = v[m];
+        if (sr) e = cadd(e, cmul(A, sr[y]));
+        v[m] = cmul(cmul(e, gxz1), sgy[N + y]);
+      }
+    }
+    if constexpr (P <= 32) {
+      line_fft<N, false>(v, L, p, a.py.tw, SyncWarp{});
+    } else {
+      line_fft<N, false>(v, L, p, a.py.tw, SyncBlock{});
+    }
+    if (live) {
+#pragma unroll
+      for (int m = 0; m < 16; ++m) T[gcol + p + P * m] = v[m];
+    }
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) esum += __shfl_xor_sync(0xffffffffu, esum, o);
+  if ((tid & 31) == 0) red[tid >> 5] = esum;
+  __syncthreads();
+  if (tid < 32) {
+    float v = tid < kThreads / 32 ? red[tid] : 0.f;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    if (tid == 0) partials[bid] = (double)v;
+  }
+}
+
 // The same fused step with K1's half of the plane exchange pushed: each block
 // sends its transformed columns to the row owners with st.async, completion
 // counted in bytes on the receiver's mbarrier (as in kf_plane_fwd), instead of

@@ -84,6 +84,7 @@ struct FastInner {
   size_t smem_fused = 0;
   const void* fused_tma = nullptr;  // the same with K3's rows loaded by a tensor copy (first argument: the map)
   const void* col_step = nullptr;   // the column pass of the split fused step (kc_col_step), or null
+  size_t smem_col = 0;              // its dynamic shared memory (2-D: kc_col_step2d)
 };
 struct FastPencil {
   int no, ty;
@@ -100,7 +101,12 @@ static FastInner fast_inner() {
   FastInner f{N, C, DX ? 1 : 0, (const void*)fast::kf_plane_fwd<N, C, DX>,
               (const void*)fast::kf_plane_inv<N, C, DX>, DX ? G::smem : (size_t)G::CS * sizeof(float2),
               DX ? (G::PUSH ? G::smem_push : G::smem_a) : 0, DX ? G::smem_max_ab : 0};
-  if constexpr (DX) f.col_step = (const void*)fast::kc_col_step<N, C>;
+  if constexpr (DX) {
+    f.col_step = (const void*)fast::kc_col_step<N, C>;
+  } else {
+    f.col_step = (const void*)fast::kc_col_step2d<N>;
+    f.smem_col = fast::smem_col_step2d<N>();
+  }
   if constexpr (DX && C > 1) {
     if constexpr (C >= 16) {  // small tiles: the column tile and the row tile fit side by side
       f.fused = (const void*)fast::kf_plane_fused_push<N, C>;
@@ -481,9 +487,9 @@ static void free_graph(Solver* s) {
 // a cluster); WAVESIM_B200_FUSE=0 keeps the three kernels separate.
 static void update_fuse(Solver* s) {
   const char* e = std::getenv("WAVESIM_B200_FUSE");
-  const int f = (s->lay.fi && (s->lay.fi->fused || s->lay.xp) && s->lay.mode3d && !s->pstd &&
-                 !(e && std::strcmp(e, "0") == 0))
-                    ? 1 : 0;
+  const bool on3 = s->lay.fi && (s->lay.fi->fused || s->lay.xp) && s->lay.mode3d;
+  const bool on2 = s->lay.fi && !s->lay.mode3d && s->lay.fi->col_step;  // 2-D: K2 + the column pass
+  const int f = ((on3 || on2) && !s->pstd && !(e && std::strcmp(e, "0") == 0)) ? 1 : 0;
   if (f != s->fuse) free_graph(s);
   s->fuse = f;
 }
@@ -559,6 +565,7 @@ static int set_kernel_attributes() {
       WS_CUDA(allow_dynamic_smem(f.fused, optin));
       WS_CUDA(cudaFuncSetAttribute(f.fused, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
     }
+    if (f.col_step) WS_CUDA(allow_dynamic_smem(f.col_step, optin));
     if (f.fused_tma) {
       WS_CUDA(allow_dynamic_smem(f.fused_tma, optin));
       WS_CUDA(cudaFuncSetAttribute(f.fused_tma, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
@@ -1143,12 +1150,13 @@ static cudaError_t launch_colstep(const Solver* s, int w, int w1, bool src_next)
   double* partials = s->d_partials;
   void* args[] = {&a, &W1, &src1, &A, &T, &dE, &E, &gamma, &st, &partials};
   return cudaLaunchKernel(s->lay.fi->col_step, dim3((unsigned)(s->lay.grid_inner * s->nrhs)), dim3(fast::kThreads),
-                          args, 0, s->stream);
+                          args, s->lay.fi->smem_col, s->stream);
 }
 
 // K3 of an iteration and K1 of the next: one kernel on a cluster, or the
 // split step (inverse x pencils, column pass, forward x pencils).
 static cudaError_t launch_step(const Solver* s, int w, int w1, bool src_next) {
+  if (!s->lay.mode3d) return launch_colstep(s, w, w1, src_next);  // 2-D: K2 already transformed along x
   if (!s->lay.xp) return launch_k3k1(s, w, w1, src_next);
   cudaError_t e = launch_xpencil(s, true);
   if (e != cudaSuccess) return e;
