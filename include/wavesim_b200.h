@@ -295,14 +295,26 @@ int ws_solver_warm_residual(ws_solver s, int64_t rhs, double* cold_residual_ener
 
 /* Autotuner (no counterpart in the reference): times the kernel layouts the
  * solver's grid supports - the power-of-two fast kernels or the generic
- * mixed-radix ones for the inner and the outer pass, the generic outer
- * pass's y tile, the 2-D columns per block - over n_iterations iterations
- * each, keeps the fastest inner and outer pass, and uses them from the next
- * solve on.  A candidate must first reproduce one iteration of the current
+ * mixed-radix ones for the inner and the outer pass, the generic kernels'
+ * radix schedules, the split step's x pencils (y tile, stages), the TMA
+ * pencil's stages, the generic outer pass's y tile, the 2-D columns per
+ * block - over n_iterations iterations of the loop as it runs (the fused
+ * step where there is one) each, keeps the fastest inner and outer pass,
+ * and uses them from the next solve on.  A candidate must first reproduce one iteration of the current
  * layout to 1e-4.  Outputs (may be NULL): candidates tried, and the time of
  * one iteration (K1 + K2 + K3, ms) before and after.  Overwrites the solver's
  * fields; call it between solves. */
 int ws_solver_autotune(ws_solver s, int n_iterations, int* n_tried, float* ms_before, float* ms_after);
+
+/* The solver's layout choice as 7 integers (the autotuner's pick, or zeros
+ * for the heuristics): inner kernels, outer kernel, cluster size, columns per
+ * block, y per outer block, radix schedule of the generic kernels, x pencil
+ * of the split step.  ws_solver_set_layout applies such a choice (e.g. one
+ * cached from an earlier autotune of the same grid) without timing anything;
+ * WS_ERR_UNSUPPORTED if this grid does not take it.  No counterpart in the
+ * reference. */
+int ws_solver_get_layout(ws_solver s, int32_t choice[7]);
+int ws_solver_set_layout(ws_solver s, const int32_t choice[7]);
 
 int ws_solver_destroy(ws_solver s);
 

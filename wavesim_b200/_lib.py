@@ -70,7 +70,7 @@ EXPORTS = [
     "ws_run_algorithm_release",
     "ws_solver_create", "ws_solver_create_media", "ws_solver_solve", "ws_solver_solve_batch", "ws_solver_solve_plane_waves", "ws_solver_buffers",
     "ws_solver_time_kernels", "ws_solver_time_split",
-    "ws_solver_launches_per_iteration", "ws_solver_set_wait_limit", "ws_solver_time_fused", "ws_solver_warm_report", "ws_solver_warm_residual", "ws_solver_autotune", "ws_solver_destroy",
+    "ws_solver_launches_per_iteration", "ws_solver_set_wait_limit", "ws_solver_time_fused", "ws_solver_warm_report", "ws_solver_warm_residual", "ws_solver_autotune", "ws_solver_get_layout", "ws_solver_set_layout", "ws_solver_destroy",
     "ws_run_algorithm_noalloc", "ws_medium_reduce", "ws_build_gamma", "ws_setup_last_error",
     "ws_noalloc_scratch_bytes", "ws_noalloc_last_error",
     "ws_pstd_default_options", "ws_pstd_create", "ws_pstd_run", "ws_pstd_destroy",
@@ -145,6 +145,10 @@ def _load():
     lib.ws_solver_warm_residual.restype = C.c_int
     lib.ws_solver_autotune.argtypes = [P, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_float), C.POINTER(C.c_float)]
     lib.ws_solver_autotune.restype = C.c_int
+    lib.ws_solver_get_layout.argtypes = [P, C.POINTER(C.c_int32)]
+    lib.ws_solver_get_layout.restype = C.c_int
+    lib.ws_solver_set_layout.argtypes = [P, C.POINTER(C.c_int32)]
+    lib.ws_solver_set_layout.restype = C.c_int
     i64a = C.POINTER(C.c_int64)
     lib.ws_medium_reduce.argtypes = [P, C.c_int, C.c_int64, C.c_double, C.c_double, C.POINTER(C.c_double), P]
     lib.ws_medium_reduce.restype = C.c_int

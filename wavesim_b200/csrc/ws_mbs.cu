@@ -50,12 +50,20 @@ static int fail(int code, const std::string& msg) {
 // ---------------------------------------------------------------------------
 // planning
 // ---------------------------------------------------------------------------
-static bool plan_radices(int n, std::vector<int>& out) {
+// Radix schedules of the generic kernels: 0 the largest radices first (the
+// default), 1 radices of at most 8 first (more, lighter stages), 2 the
+// default radices in reverse order.  Any order is a valid Stockham schedule;
+// the autotuner picks one by time.
+constexpr int kNumSchedules = 3;
+static bool plan_radices(int n, std::vector<int>& out, int sched = 0) {
   out.clear();
-  static const int pref[] = {16, 12, 13, 11, 10, 9, 8, 7, 6, 5, 4, 3, 2};
+  static const int pref0[] = {16, 12, 13, 11, 10, 9, 8, 7, 6, 5, 4, 3, 2};
+  static const int pref1[] = {8, 7, 6, 5, 4, 3, 9, 10, 11, 12, 13, 16, 2};
+  const int* pref = sched == 1 ? pref1 : pref0;
   while (n > 1) {
     bool found = false;
-    for (int r : pref) {
+    for (int i = 0; i < 13; ++i) {
+      const int r = pref[i];
       if (n % r == 0) {
         out.push_back(r);
         n /= r;
@@ -65,6 +73,7 @@ static bool plan_radices(int n, std::vector<int>& out) {
     }
     if (!found) return false;
   }
+  if (sched == 2) std::reverse(out.begin(), out.end());
   return (int)out.size() <= kMaxStages;
 }
 
@@ -255,8 +264,11 @@ struct LayoutChoice {
   int csize = 0;  // 3-D generic: smallest blocks per plane to try
   int ncols = 0;  // 2-D generic: columns per block
   int ty = 0;     // generic outer: consecutive y per block
+  int sched = 0;  // radix schedule of the generic kernels' plans (plan_radices)
+  int xp = 0;     // split step: 1 + index of the x pencil in x_pencil_table (0: the default)
   bool operator==(const LayoutChoice& o) const {
-    return inner == o.inner && outer == o.outer && csize == o.csize && ncols == o.ncols && ty == o.ty;
+    return inner == o.inner && outer == o.outer && csize == o.csize && ncols == o.ncols && ty == o.ty &&
+           sched == o.sched && xp == o.xp;
   }
 };
 
@@ -392,12 +404,23 @@ static int make_layout(const Geom& g, Layout& L, std::string& why, const LayoutC
   int want_xty = 0, want_xs = 0;  // WAVESIM_B200_XTY / _XSTAGES: the y tile and stages of the x pencils
   if (const char* e = std::getenv("WAVESIM_B200_XTY")) want_xty = std::atoi(e);
   if (const char* e = std::getenv("WAVESIM_B200_XSTAGES")) want_xs = std::atoi(e);
-  if (L.mode3d && L.fi && L.fi->col_step && !(step && std::strcmp(step, "cluster") == 0))
-    for (const XPencil& f : x_pencil_table())
-      if (f.no == g.nx && g.ny % f.ty == 0 && (!want_xty || f.ty == want_xty) && (!want_xs || f.stages == want_xs)) {
-        L.xp = &f;
-        break;
+  if (L.mode3d && L.fi && L.fi->col_step && !(step && std::strcmp(step, "cluster") == 0)) {
+    const auto& xt = x_pencil_table();
+    if (ch.xp > 0 && ch.xp <= (int)xt.size()) {
+      const XPencil& f = xt[ch.xp - 1];
+      if (f.no != g.nx || g.ny % f.ty) {
+        why = "the x pencil asked for does not fit the grid";
+        return WS_ERR_UNSUPPORTED;
       }
+      L.xp = &f;
+    } else {
+      for (const XPencil& f : xt)
+        if (f.no == g.nx && g.ny % f.ty == 0 && (!want_xty || f.ty == want_xty) && (!want_xs || f.stages == want_xs)) {
+          L.xp = &f;
+          break;
+        }
+    }
+  }
   return WS_OK;
 }
 
@@ -509,10 +532,10 @@ static void destroy_solver(Solver* s) {
   delete s;
 }
 
-static int build_plan(int n, const std::vector<float2>& tw_all_offset_dummy, FftPlan& p) {
+static int build_plan(int n, const std::vector<float2>& tw_all_offset_dummy, FftPlan& p, int sched = 0) {
   (void)tw_all_offset_dummy;
   std::vector<int> r;
-  if (!plan_radices(n, r)) return WS_ERR_UNSUPPORTED;
+  if (!plan_radices(n, r, sched)) return WS_ERR_UNSUPPORTED;
   p.n = n;
   p.nst = (int)r.size();
   for (int i = 0; i < kMaxStages; ++i) p.radix[i] = i < (int)r.size() ? r[i] : 1;
@@ -1916,6 +1939,9 @@ static __global__ void k_max_diff(const float2* __restrict__ a, const float2* __
 }
 
 // One iteration (wiggle 0, no source) from the fixed pattern; dE' -> out.
+// One iteration of the loop as it runs with the solver's current layout
+// (the fused step where there is one), from a fixed pattern; the new
+// increment dE' into `out`.
 static int tune_probe(Solver* s, const StopRule& rule, const Hist& hh, float2* out) {
   const long long n = (long long)field_elems(s);
   const unsigned blocks = (unsigned)std::min<long long>((n + 255) / 256, 8 * kNumSms);
@@ -1924,16 +1950,42 @@ static int tune_probe(Solver* s, const StopRule& rule, const Hist& hh, float2* o
   WS_CUDA(cudaGetLastError());
   WS_CUDA(launch_k1(s, 0, false));
   WS_CUDA(launch_k2(s, 0));
-  WS_CUDA(launch_k3_only(s, 0));
+  if (s->fuse) {
+    WS_CUDA(launch_step(s, 0, 1 % s->nw, false));
+  } else {
+    WS_CUDA(launch_k3_only(s, 0));
+  }
   WS_CUDA(launch_finish(s, rule, hh));
   WS_CUDA(cudaMemcpyAsync(out, s->d_dE, n * sizeof(float2), cudaMemcpyDeviceToDevice, s->stream));
   WS_CUDA(cudaStreamSynchronize(s->stream));
   return WS_OK;
 }
 
+// Mean device time of the loop's kernels: K1, K2, K3, or (fused) 0, K2 and
+// the step.
 static int tune_time(Solver* s, const StopRule& rule, const Hist& hh, int iters, float ms[3]) {
   k_resume_state<<<1, 32, 0, s->stream>>>(s->d_state);
   float acc[3] = {0, 0, 0};
+  if (s->fuse) {
+    WS_CUDA(launch_k1(s, 0, false));
+    for (int i = 0; i < iters; ++i) {
+      const int w = i % s->nw;
+      WS_CUDA(cudaEventRecord(s->ev[0], s->stream));
+      WS_CUDA(launch_k2(s, w));
+      WS_CUDA(cudaEventRecord(s->ev[1], s->stream));
+      WS_CUDA(launch_step(s, w, (i + 1) % s->nw, false));
+      WS_CUDA(cudaEventRecord(s->ev[2], s->stream));
+      WS_CUDA(launch_finish(s, rule, hh));
+      WS_CUDA(cudaEventSynchronize(s->ev[2]));
+      float t;
+      WS_CUDA(cudaEventElapsedTime(&t, s->ev[0], s->ev[1]));
+      acc[1] += t;
+      WS_CUDA(cudaEventElapsedTime(&t, s->ev[1], s->ev[2]));
+      acc[2] += t;
+    }
+    for (int k = 0; k < 3; ++k) ms[k] = acc[k] / iters;
+    return WS_OK;
+  }
   for (int i = 0; i < iters; ++i) {
     const int w = i % s->nw;
     WS_CUDA(cudaEventRecord(s->ev[0], s->stream));
@@ -1953,6 +2005,35 @@ static int tune_time(Solver* s, const StopRule& rule, const Hist& hh, int iters,
   }
   for (int k = 0; k < 3; ++k) ms[k] = acc[k] / iters;
   return WS_OK;
+}
+// The generic kernels' plans with radix schedule `sched` (same lengths and
+// twiddle tables).
+static void apply_sched(Solver* s, int sched) {
+  std::vector<float2> none;
+  FftPlan* plans[3] = {&s->py, &s->pxl, &s->po};
+  for (FftPlan* p : plans) {
+    const float2* tw = p->tw;
+    if (p->n >= 1) build_plan(p->n, none, *p, sched);
+    p->tw = tw;
+  }
+}
+
+// Makes `c` the solver's layout (kernels, plans, fused loop); false if the
+// grid does not allow it.
+static bool apply_choice(Solver* s, const LayoutChoice& c) {
+  Layout L;
+  std::string why;
+  if (make_layout(s->g, L, why, c) != WS_OK) return false;
+  // the generic 3-D kernels transform x-local lines of Nx / csize points with
+  // the plan and twiddles made for the solver's first layout: a layout with
+  // another cluster size would run them on lines of another length
+  if (L.mode3d && !L.fi && s->g.nx / L.csize != s->pxl.n) return false;
+  if (ensure_partials(s, L.grid_inner * std::max(1, s->batch_cap)) != WS_OK) return false;
+  s->lay = L;
+  apply_sched(s, c.sched);
+  update_fuse(s);
+  free_graph(s);
+  return true;
 }
 }  // namespace ws
 
@@ -2001,6 +2082,20 @@ int ws_solver_autotune(ws_solver h, int n_iterations, int* n_tried, float* ms_be
   if (!base.mode3d)
     for (int f : {4, 2, -2})
       inner_c.push_back(LayoutChoice{2, 0, 0, f > 0 ? std::max(1, base.ncols / f) : base.ncols * 2, 0});
+  for (int k = 1; k < kNumSchedules; ++k) {  // the generic kernels' radix schedules
+    LayoutChoice c{2, 0, 0, 0, 0};
+    c.sched = k;
+    inner_c.push_back(c);
+  }
+  if (base.mode3d) {  // the split step's x pencils
+    const auto& xt = x_pencil_table();
+    for (int i = 0; i < (int)xt.size(); ++i)
+      if (xt[i].no == s->g.nx && s->g.ny % xt[i].ty == 0) {
+        LayoutChoice c{1, 0, 0, 0, 0};
+        c.xp = i + 1;
+        inner_c.push_back(c);
+      }
+  }
   outer_c.push_back(LayoutChoice{0, 1, 0, 0, 0});
   outer_c.push_back(LayoutChoice{0, 1, 0, 0, 8});  // fast pencil with 8 y per block, where one exists
   for (int k : {2, 3}) outer_c.push_back(LayoutChoice{0, 3 + k, 0, 0, 0});
@@ -2008,12 +2103,12 @@ int ws_solver_autotune(ws_solver h, int n_iterations, int* n_tried, float* ms_be
   int tried = 0;
   LayoutChoice best_in{}, best_out{};
   float t_in = base_ms[0] + base_ms[2], t_out = base_ms[1];
+  const LayoutChoice base_choice = s->tuned;
   auto evaluate = [&](const LayoutChoice& c, float ms[3]) -> bool {
-    Layout L;
-    std::string why;
-    if (make_layout(s->g, L, why, c) != WS_OK) return false;
-    if (ensure_partials(s, L.grid_inner * std::max(1, s->batch_cap)) != WS_OK) return false;
-    s->lay = L;
+    if (!apply_choice(s, c)) {
+      apply_choice(s, base_choice);
+      return false;
+    }
     bool ok = tune_probe(s, rule, hh, got) == WS_OK;
     if (ok) {
       unsigned hmax[2] = {0, 0};
@@ -2028,7 +2123,7 @@ int ws_solver_autotune(ws_solver h, int n_iterations, int* n_tried, float* ms_be
       ok = ok && d <= 1e-4f * m;
     }
     if (ok) ok = tune_time(s, rule, hh, n_iterations, ms) == WS_OK;
-    s->lay = base;
+    apply_choice(s, base_choice);
     cudaGetLastError();  // a launch refused for a candidate must not leak into later calls
     ++tried;
     return ok;
@@ -2051,23 +2146,44 @@ int ws_solver_autotune(ws_solver h, int n_iterations, int* n_tried, float* ms_be
   fin.outer = best_out.outer;
   fin.ty = best_out.ty;
   float fin_ms[3] = {base_ms[0], base_ms[1], base_ms[2]};
-  if (!(fin == LayoutChoice{})) {
+  if (!(fin == base_choice)) {
     if (!evaluate(fin, fin_ms)) {
-      fin = LayoutChoice{};
+      fin = base_choice;
       std::memcpy(fin_ms, base_ms, sizeof(fin_ms));
-    } else {
-      Layout L;
-      std::string why;
-      make_layout(s->g, L, why, fin);
-      s->lay = L;
     }
   }
+  apply_choice(s, fin);
   s->tuned = fin;
-  update_fuse(s);
   cleanup();
   if (n_tried) *n_tried = tried;
   if (ms_before) *ms_before = base_ms[0] + base_ms[1] + base_ms[2];
   if (ms_after) *ms_after = fin_ms[0] + fin_ms[1] + fin_ms[2];
+  return WS_OK;
+}
+
+int ws_solver_get_layout(ws_solver h, int32_t choice[7]) {
+  if (!h || !choice) return fail(WS_ERR_INVALID_ARGUMENT, "bad argument");
+  const LayoutChoice& c = reinterpret_cast<Solver*>(h)->tuned;
+  const int32_t v[7] = {c.inner, c.outer, c.csize, c.ncols, c.ty, c.sched, c.xp};
+  std::memcpy(choice, v, sizeof(v));
+  return WS_OK;
+}
+
+int ws_solver_set_layout(ws_solver h, const int32_t choice[7]) {
+  if (!h || !choice) return fail(WS_ERR_INVALID_ARGUMENT, "bad argument");
+  Solver* s = reinterpret_cast<Solver*>(h);
+  LayoutChoice c{choice[0], choice[1], choice[2], choice[3], choice[4]};
+  c.sched = choice[5];
+  c.xp = choice[6];
+  if (c.inner < 0 || c.inner > 2 || c.outer < 0 || c.outer > 9 || c.csize < 0 || c.csize > 16 || c.ncols < 0 ||
+      c.ty < 0 || c.sched < 0 || c.sched >= kNumSchedules || c.xp < 0 || c.xp > (int)x_pencil_table().size())
+    return fail(WS_ERR_INVALID_ARGUMENT, "layout choice out of range");
+  WS_CUDA(cudaSetDevice(s->device));
+  if (!apply_choice(s, c)) {
+    apply_choice(s, s->tuned);
+    return fail(WS_ERR_UNSUPPORTED, "this grid does not take that layout");
+  }
+  s->tuned = c;
   return WS_OK;
 }
 
