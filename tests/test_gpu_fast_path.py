@@ -1,6 +1,7 @@
-"""The power-of-two fast kernels agree with the generic kernels and with the
-oracle on every shape they are instantiated for (plane kernels with and
-without a thread-block cluster, 2-D column kernels, pencil kernels)."""
+"""The fast kernels (power-of-two and register-resident mixed-radix) agree
+with the generic kernels and with the oracle on every shape they are
+instantiated for (plane kernels with and without a thread-block cluster, 2-D
+column kernels, pencil kernels)."""
 import os
 
 import numpy as np
@@ -59,6 +60,13 @@ CASES = {
     # 96-point lines (12 x 4 x 2): a whole 96^2 plane on one block
     "3d_96": ((64, 64, 64), [16, 16, 16], 16, False),
     "3d_96_vector": ((64, 64, 64), [16, 16, 16], 8, True),
+    # four-stage plans with more elements per thread than the first radix:
+    # 160 = 10 x 4 x 4 (20 per thread), 224 = 14 x 4 x 4 (28 per thread);
+    # planes on clusters of 5 and 7 blocks, z pencils
+    "3d_160_cluster5": ((128, 128, 8), [16, 16, 4], 16, False),
+    "3d_224_cluster7": ((192, 192, 8), [16, 16, 4], 16, False),
+    "3d_pencil_160": ((16, 16, 128), [8, 8, 16], 16, False),
+    "3d_pencil_224": ((16, 16, 192), [8, 8, 16], 16, False),
     # layout variants the autotuner may choose
     "3d_256_cluster16": ((224, 224, 16), [16, 16, 8], 16, False, {"WAVESIM_B200_CLUSTER": "16"}),
     "3d_pencil_192_vector_ty8": ((16, 16, 160), [8, 8, 16], 16, True, {"WAVESIM_B200_PENCIL_TY": "8"}),

@@ -59,9 +59,14 @@ CASES = {
     "192_split_vector": ((160, 160, 4), [16, 16, 2], "vector"),
     "192_split_x16": ((160, 160, 8), [16, 16, 4], {"WAVESIM_B200_XTY": "16"}),
     "96_split": ((64, 64, 32), [16, 16, 16], None),
+    "160_split": ((128, 128, 8), [16, 16, 4], None),
+    "224_split": ((192, 192, 8), [16, 16, 4], None),
     # 192-point planes on 6 blocks (km_plane_fused), scalar
     "192_cluster6": ((160, 160, 8), [16, 16, 4], CLUSTER),
     "192_cluster6_vector": ((160, 160, 4), [16, 16, 2], ("vector", CLUSTER)),
+    # 160- and 224-point planes on clusters of 5 and 7 blocks
+    "160_cluster5": ((128, 128, 8), [16, 16, 4], CLUSTER),
+    "224_cluster7": ((192, 192, 8), [16, 16, 4], CLUSTER),
     # K3's rows by per-thread loads instead of one tensor copy (kf_plane_fused)
     "128_cluster2_loads": ((96, 96, 96), [16, 16, 16], dict(CLUSTER, WAVESIM_B200_FUSED_TMA="0")),
     "256_cluster8_loads": ((224, 224, 16), [16, 16, 8], dict(CLUSTER, WAVESIM_B200_FUSED_TMA="0")),

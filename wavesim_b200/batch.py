@@ -141,7 +141,7 @@ class MediaBatch:
         del keep
         outs, states = [], []
         for i in range(R):
-            Ei = np.ascontiguousarray(E[i].transpose(3, 2, 1, 0))
+            Ei = E[i].transpose(3, 2, 1, 0)  # [y, x, z, c], column-major in memory
             if not first.vector:
                 Ei = Ei[..., 0]
             outs.append(Ei)

@@ -14,7 +14,7 @@ Run:  python gen_codelets.py > ws_codelets.cuh
 """
 import math
 
-RADICES = [2, 3, 4, 5, 6, 7, 8, 9, 10, 11, 12, 13, 16]
+RADICES = [2, 3, 4, 5, 6, 7, 8, 9, 10, 11, 12, 13, 14, 16]
 
 
 class Gen:

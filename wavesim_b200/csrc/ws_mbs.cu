@@ -93,7 +93,7 @@ struct FastInner {
   size_t smem_fused = 0;
   const void* fused_tma = nullptr;  // the same with K3's rows loaded by a tensor copy (first argument: the map)
   const void* col_step = nullptr;   // the column pass of the split fused step (kc_col_step), or null
-  size_t smem_col = 0;              // its dynamic shared memory (2-D: kc_col_step2d)
+  size_t smem_col = 0;              // its dynamic shared memory (kc_col_step2d, kmc_col_step)
 };
 struct FastPencil {
   int no, ty;
@@ -136,6 +136,8 @@ static FastPencil fast_pencil() {
 // mixed-radix / vector kernels (ws_mixed.cuh)
 using Plan192 = mixed::Plan<192, 12, 12, 4, 4>;
 using Plan96 = mixed::Plan<96, 12, 12, 4, 2>;
+using Plan160 = mixed::Plan<160, 20, 10, 4, 4>;
+using Plan224 = mixed::Plan<224, 28, 14, 4, 4>;
 template <class PL, int C>
 static FastInner mixed_inner() {
   using G = mixed::MGeom<PL, C>;
@@ -144,6 +146,7 @@ static FastInner mixed_inner() {
   f.fused = (const void*)mixed::km_plane_fused<PL, C>;
   f.fused_tma = (const void*)mixed::km_plane_fused_tma<PL, C>;
   f.col_step = (const void*)mixed::kmc_col_step<PL, C>;
+  f.smem_col = mixed::smem_col_step<PL, C>();
   f.smem_fused = G::smem;
   static_assert((size_t)PL::N * G::LR * sizeof(float2) + 128 <= G::smem, "the dense row tile fits");
   return f;
@@ -160,7 +163,8 @@ static const std::vector<FastInner>& fast_inner_table() {
       fast_inner<256, 16, true>(),
       fast_inner<64, 1, false>(),    fast_inner<128, 1, false>(),   fast_inner<256, 1, false>(),
       fast_inner<512, 1, false>(),   fast_inner<1024, 1, false>(),  fast_inner<2048, 1, false>(),
-      mixed_inner<Plan192, 6>(),     mixed_inner<Plan96, 1>()};
+      mixed_inner<Plan192, 6>(),     mixed_inner<Plan96, 1>(),      mixed_inner<Plan160, 5>(),
+      mixed_inner<Plan224, 7>()};
   return t;
 }
 // Persistent TMA-pipelined K2 (ws_tma.cuh) for z pencils of a 3-D grid.
@@ -204,8 +208,10 @@ static XPencil x_pencil_m() {
 static const std::vector<XPencil>& x_pencil_table() {
   // the first match of (no, ty) is the default
   static const std::vector<XPencil> t = {x_pencil<64, 16, 3>(), x_pencil<128, 16, 3>(), x_pencil<256, 8, 3>(),
-                                         x_pencil<256, 8, 4>(), x_pencil<256, 16, 3>(), x_pencil_m<Plan192, 8, 4>(),
-                                         x_pencil_m<Plan192, 16, 3>(), x_pencil_m<Plan96, 16, 3>()};
+                                         x_pencil<256, 8, 4>(), x_pencil<256, 16, 3>(), x_pencil<256, 8, 2>(),
+                                         x_pencil_m<Plan192, 8, 4>(),
+                                         x_pencil_m<Plan192, 16, 3>(), x_pencil_m<Plan96, 16, 3>(),
+                                         x_pencil_m<Plan160, 16, 3>(), x_pencil_m<Plan224, 16, 3>()};
   return t;
 }
 using Plan192t = mixed::Plan<192, 12, 12, 4, 4>;
@@ -216,7 +222,7 @@ static const std::vector<TmaPencil>& tma_pencil_table() {
   // 0.070 for 16 x 3, 0.081 for 4 x 4 and 0.096 for 8 x 6)
   static const std::vector<TmaPencil> t = {tma_pencil<64, 16, 3>(), tma_pencil<128, 16, 3>(),
                                            tma_pencil<256, 8, 3>(),  tma_pencil<256, 8, 4>(),
-                                           tma_pencil<256, 16, 3>(),
+                                           tma_pencil<256, 8, 2>(),  tma_pencil<256, 16, 3>(),
                                            tma_pencil<256, 16, 2>(), tma_pencil<256, 8, 6>(),
                                            tma_pencil<256, 4, 4>(),
                                            // 192 x 3 components: 8 y x 3 stages measured 0.131 ms against
@@ -234,6 +240,8 @@ static const std::vector<FastPencil>& fast_pencil_table() {
       mixed_pencil<Plan192, 16, 3>(),
       mixed_pencil<Plan96, 16, 1>(),
       mixed_pencil<Plan96, 16, 3>(),
+      mixed_pencil<Plan160, 16, 1>(),
+      mixed_pencil<Plan224, 16, 1>(),
       mixed_pencil<mixed::Plan<64, 16, 16, 4>, 16, 3>(),
       mixed_pencil<mixed::Plan<128, 16, 16, 8>, 16, 3>(),
       mixed_pencil<mixed::Plan<256, 16, 16, 16>, 16, 3>()};

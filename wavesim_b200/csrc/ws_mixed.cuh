@@ -3,13 +3,16 @@
 // a WaveSimVector problem with a 16-pixel boundary.
 //
 // A line of N points is held by P = N / E threads with E elements each, and
-// transformed by a Stockham schedule fixed at compile time: radices
-// R0 = E, R1, R2 with R0 R1 R2 = N and R1, R2 dividing E (192 = 12 x 4 x 4,
-// E = 12).  Thread p enters with v[r] = x[p + P r] and leaves with
-// v[m] = X[p + P m], as in the power-of-two kernels; stage s > 0 reads the
-// R inputs x[j + r N/R] of its butterflies j = p + P q, multiplies them by
-// W_{Ns R}^{(j mod Ns) r} (Ns = product of the earlier radices), applies the
-// radix-R DFT and writes output r to (j - j mod Ns) R + j mod Ns + r Ns.
+// transformed by a Stockham schedule fixed at compile time: up to four
+// radices R0 R1 R2 R3 = N, each dividing E (192 = 12 x 4 x 4 with E = 12;
+// 160 = 10 x 4 x 4 with E = 20; 224 = 14 x 4 x 4 with E = 28).  Thread p
+// enters with v[r] = x[p + P r] and leaves with v[m] = X[p + P m], as in the
+// power-of-two kernels.  Each stage runs E / R butterflies j = p + P q per
+// thread; stage 0 takes their inputs x[j + r N/R0] = v[q + (E/R0) r] from
+// registers, a later stage reads the R inputs x[j + r N/R] from shared
+// memory and multiplies them by W_{Ns R}^{(j mod Ns) r} (Ns = product of the
+// earlier radices); every stage but the last writes output r of butterfly j
+// to (j - j mod Ns) R + j mod Ns + r Ns.
 //
 //   km_plane_fwd<PL, C>  K1: (y, x) planes on a cluster of C blocks; y
 //                        transforms of N / C columns per block, then each
@@ -27,14 +30,25 @@ namespace mixed {
 
 constexpr int kThreads = 256;
 
-template <int N_, int E_, int R0, int R1, int R2 = 1>
+// The epilogues issue their loads (gamma, dE', E') in NH groups of H = E / NH
+// elements: halves up to 12 elements per thread, quarters beyond, so that
+// fewer loads are in flight in registers at once.
+template <int E>
+constexpr int kEpilogueParts = E > 12 && E % 4 == 0 ? 4 : 2;
+
+template <int N_, int E_, int R0, int R1, int R2 = 1, int R3 = 1>
 struct Plan {
   static constexpr int N = N_, E = E_, P = N_ / E_;
-  static constexpr int NST = R2 > 1 ? 3 : (R1 > 1 ? 2 : 1);
-  __host__ __device__ static constexpr int radix(int s) { return s == 0 ? R0 : (s == 1 ? R1 : R2); }
-  __host__ __device__ static constexpr int span(int s) { return s == 0 ? 1 : (s == 1 ? R0 : R0 * R1); }
-  static_assert(R0 * R1 * R2 == N_, "the radices multiply to N");
-  static_assert(R0 == E_ && E_ % R1 == 0 && E_ % R2 == 0, "first radix = elements per thread, the others divide it");
+  static constexpr int NST = R3 > 1 ? 4 : (R2 > 1 ? 3 : (R1 > 1 ? 2 : 1));
+  __host__ __device__ static constexpr int radix(int s) {
+    return s == 0 ? R0 : (s == 1 ? R1 : (s == 2 ? R2 : R3));
+  }
+  __host__ __device__ static constexpr int span(int s) {
+    return s == 0 ? 1 : (s == 1 ? R0 : (s == 2 ? R0 * R1 : R0 * R1 * R2));
+  }
+  static_assert(R0 * R1 * R2 * R3 == N_ && N_ % E_ == 0, "the radices multiply to N, E divides N");
+  static_assert(E_ % R0 == 0 && E_ % R1 == 0 && E_ % R2 == 0 && E_ % R3 == 0, "every radix divides E");
+  static_assert(NST > 1 || R0 == E_, "a one-stage line is one butterfly per thread");
 };
 
 template <int R, bool INV, int E>
@@ -52,6 +66,16 @@ __device__ __forceinline__ void stage(float2 (&v)[PL::E], const Line& L, int p, 
                                       Sync sync) {
   constexpr int E = PL::E, N = PL::N, P = PL::P;
   constexpr int R = PL::radix(S), Ns = PL::span(S), B = E / R, NR = N / R, TS = N / (Ns * R);
+  if constexpr (S == 0 && B > 1) {
+    // butterfly q takes v[q + B r]; gather it to v[q R + r]
+    float2 t[E];
+#pragma unroll
+    for (int m = 0; m < E; ++m) t[m] = v[m];
+#pragma unroll
+    for (int q = 0; q < B; ++q)
+#pragma unroll
+      for (int r = 0; r < R; ++r) v[q * R + r] = t[q + B * r];
+  }
   if constexpr (S > 0) {
 #pragma unroll
     for (int q = 0; q < B; ++q) {
@@ -98,6 +122,7 @@ __device__ __forceinline__ void line_fft(float2 (&v)[PL::E], const Line& L, int 
   stage<PL, INV, 0>(v, L, p, tw, sync);
   if constexpr (PL::NST > 1) stage<PL, INV, 1>(v, L, p, tw, sync);
   if constexpr (PL::NST > 2) stage<PL, INV, 2>(v, L, p, tw, sync);
+  if constexpr (PL::NST > 3) stage<PL, INV, 3>(v, L, p, tw, sync);
 }
 
 // Shared-memory tiles of the plane kernels (one buffer, used twice):
@@ -341,9 +366,9 @@ __global__ void __launch_bounds__(kThreads, 2)
     float2* __restrict__ Ec = E + gcol;
     // Eprop after the conjugate ramps (WaveSim.m:55), then f_mix (f_mix.m:3-4)
     // and E += dE; the loads of a half are issued together.
-    constexpr int H = EL / 2;
+    constexpr int NH = kEpilogueParts<EL>, H = EL / NH;
 #pragma unroll
-    for (int h = 0; h < 2; ++h) {
+    for (int h = 0; h < NH; ++h) {
       float2 gm[H], d0[H], e0[H];
 #pragma unroll
       for (int i = 0; i < H; ++i) {
@@ -462,9 +487,9 @@ __global__ void __launch_bounds__(kThreads, 2)
     float2* __restrict__ dEc = dE + gcol;
     float2* __restrict__ Ec = E + gcol;
     // K3's epilogue; v[m] becomes dE'_k(y = p + P m)
-    constexpr int H = EL / 2;
+    constexpr int NH = kEpilogueParts<EL>, H = EL / NH;
 #pragma unroll
-    for (int h = 0; h < 2; ++h) {
+    for (int h = 0; h < NH; ++h) {
       float2 gm[H], d0[H], e0[H];
 #pragma unroll
       for (int i = 0; i < H; ++i) {
@@ -664,9 +689,9 @@ __global__ void __launch_bounds__(kThreads, 2)
     float2* __restrict__ dEc = dE + gcol;
     float2* __restrict__ Ec = E + gcol;
     // K3's epilogue; v[m] becomes dE'_k(y = p + P m)
-    constexpr int H = EL / 2;
+    constexpr int NH = kEpilogueParts<EL>, H = EL / NH;
 #pragma unroll
-    for (int h = 0; h < 2; ++h) {
+    for (int h = 0; h < NH; ++h) {
       float2 gm[H], d0[H], e0[H];
 #pragma unroll
       for (int i = 0; i < H; ++i) {
@@ -748,7 +773,13 @@ __global__ void __launch_bounds__(kThreads, 2)
 // The column pass of the split fused step (see fast::kc_col_step) for the
 // mixed-radix planes: the columns of block (plane, rank) of km_plane_fused,
 // the same arithmetic in the same order and the same energy partial, with
-// the y ramps of both wiggles read from shared memory.
+// the y ramps of both wiggles read from shared memory (dynamic: LPR column
+// lines, then the 2 N ramps; smem_col_step bytes).
+template <class PL, int C>
+constexpr size_t smem_col_step() {
+  return sizeof(float2) * ((size_t)MGeom<PL, C>::LPR * MGeom<PL, C>::CS + 2 * PL::N);
+}
+
 template <class PL, int C>
 __global__ void __launch_bounds__(kThreads, 2)
     kmc_col_step(InnerArgs a, Wig w1, const float2* __restrict__ src1, float2 A, float2* __restrict__ T,
@@ -766,8 +797,9 @@ __global__ void __launch_bounds__(kThreads, 2)
   if (src1) src1 += rhs * a.fstride;
   partials += (long long)rhs * a.bpr;
   gamma += rhs * a.gstride;  // a batch of media: each right-hand side has its own gamma
-  __shared__ float2 sm[LPR * G::CS];
-  __shared__ float2 sgy[2 * N];
+  extern __shared__ float2 smc[];
+  float2* const sm = smc;
+  float2* const sgy = smc + LPR * G::CS;
   __shared__ float red[kThreads / 32];
   const int tid = threadIdx.x;
   for (int i = tid; i < N; i += kThreads) {
@@ -799,9 +831,9 @@ __global__ void __launch_bounds__(kThreads, 2)
     const float2* __restrict__ gmc = gamma + (gcol - (long long)comp * g.npts);
     float2* __restrict__ dEc = dE + gcol;
     float2* __restrict__ Ec = E + gcol;
-    constexpr int H = EL / 2;
+    constexpr int NH = kEpilogueParts<EL>, H = EL / NH;
 #pragma unroll
-    for (int h = 0; h < 2; ++h) {
+    for (int h = 0; h < NH; ++h) {
       float2 gm[H], d0[H], e0[H];
 #pragma unroll
       for (int i = 0; i < H; ++i) {

@@ -164,4 +164,4 @@ class PSTD:
         state.diff_energy = hist[:min(n_it.value, cap)].copy()
         state.converged = bool(conv.value)
         state.time = time.perf_counter() - t0
-        return np.ascontiguousarray(E), state
+        return E, state  # column-major in memory, as WaveSim.exec

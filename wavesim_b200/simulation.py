@@ -351,8 +351,9 @@ class WaveSim:
         """Simulation.exec (Simulation.m:138-190) with the loop on the GPU.
         Returns (E, state): E = E'/gamma on the ROI, indexed [y, x, z] (scalar)
         or [y, x, z, c] (vector), or with output="eprime" the full-grid E'
-        that the MEX call returns (WaveSimBase.m:146); state.it,
-        state.diff_energy, state.converged, state.time.
+        that the MEX call returns (WaveSimBase.m:146); column-major in memory
+        as the C ABI writes it and as MATLAB holds it (no reordering copy on
+        the host); state.it, state.diff_energy, state.converged, state.time.
 
         warm_start (no counterpart in the reference): an estimate psi0 of the
         field - a host array on the ROI or the full grid, a flat complex64
@@ -426,7 +427,7 @@ class WaveSim:
         state.time = time.perf_counter() - t0
         if not self.vector:
             E = E[..., 0]
-        return (np.ascontiguousarray(E) if output == "field" else E), state
+        return E, state
 
     def exec_batch(self, sources, warm_starts=None):
         """Many sources on this medium in one batched solve (ws_solver_solve_batch).
@@ -481,7 +482,7 @@ class WaveSim:
         dt = time.perf_counter() - t0
         outs, states = [], []
         for i in range(R):
-            Ei = np.ascontiguousarray(E[i].transpose(3, 2, 1, 0))  # back to [y, x, z, c]
+            Ei = E[i].transpose(3, 2, 1, 0)  # [y, x, z, c], column-major in memory
             if not self.vector:
                 Ei = Ei[..., 0]
             outs.append(Ei)
@@ -538,7 +539,7 @@ class WaveSim:
         dt = time.perf_counter() - t0
         outs, states = [], []
         for i in range(R):
-            Ei = np.ascontiguousarray(E[i].transpose(3, 2, 1, 0))
+            Ei = E[i].transpose(3, 2, 1, 0)
             if not self.vector:
                 Ei = Ei[..., 0]
             outs.append(Ei)
