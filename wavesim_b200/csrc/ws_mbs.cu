@@ -225,9 +225,12 @@ static const std::vector<TmaPencil>& tma_pencil_table() {
                                            tma_pencil<256, 8, 2>(),  tma_pencil<256, 16, 3>(),
                                            tma_pencil<256, 16, 2>(), tma_pencil<256, 8, 6>(),
                                            tma_pencil<256, 4, 4>(),
-                                           // 192 x 3 components: 8 y x 3 stages measured 0.131 ms against
-                                           // 0.132 (8 x 2), 0.137 (16 x 2), 0.163 (4 x 4)
-                                           tma_pencil_vec<Plan192t, 8, 3>()};
+                                           // 192 x 3 components, one at a time in registers: 8 y x 2 stages
+                                           // (3 blocks per SM) measured 0.120 ms at 192^3 against 0.143
+                                           // (8 x 3), 0.154 (4 x 3) and 0.145 (16 x 2); all three lines in
+                                           // registers took 0.131 at best
+                                           tma_pencil_vec<Plan192t, 8, 2>(), tma_pencil_vec<Plan192t, 8, 3>(),
+                                           tma_pencil_vec<Plan192t, 4, 3>(), tma_pencil_vec<Plan192t, 16, 2>()};
   return t;
 }
 

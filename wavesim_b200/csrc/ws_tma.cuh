@@ -405,9 +405,10 @@ __global__ void __launch_bounds__(MixedXTile<PL, TY, S>::kThreads, 2)
 // The vector form (WaveSimVector, 3 components): a tile is the three
 // component boxes of the same (x, y tile), at z offsets c Nz of the map
 // {2 Ny floats, Nx, Nz Nc nrhs}; each line is transformed with the
-// register-resident mixed-radix schedule (ws_mixed.cuh), the dyadic Green's
-// function (f_g0_vector.m) applied at every k point in registers, and the
-// three boxes stored back.  The rest is kt_pencil.
+// register-resident mixed-radix schedule (ws_mixed.cuh) one component at a
+// time, the dyadic Green's function (f_g0_vector.m) applied at every k point
+// of the three transformed boxes, the inverse transforms, and the three
+// boxes stored back.  The rest is kt_pencil.
 template <class PL, int TY, int S>
 struct VecPencilTile {
   static constexpr int NO = PL::N, P = PL::P, E = PL::E;
@@ -417,10 +418,14 @@ struct VecPencilTile {
   static constexpr unsigned kBoxBytes = NO * TY * sizeof(float2);
   static constexpr unsigned kTileBytes = 3 * kBoxBytes;
   static constexpr size_t smem = S * (size_t)kTileBytes + 128;
+  // blocks per SM the tiles leave room for (228 KB, 1 KB reserved per block,
+  // at most 4): the register bound of the kernel
+  static constexpr int kFit = (int)(228 * 1024 / (smem + 3 * 1024));
+  static constexpr int kMinBlocks = kFit >= 4 ? 4 : (kFit >= 1 ? kFit : 1);
 };
 
 template <class PL, int TY, int S>
-__global__ void __launch_bounds__(VecPencilTile<PL, TY, S>::kThreads, 1)
+__global__ void __launch_bounds__(VecPencilTile<PL, TY, S>::kThreads, VecPencilTile<PL, TY, S>::kMinBlocks)
     kt_pencil_vec(const __grid_constant__ CUtensorMap tmap, OuterArgs a, const DevState* __restrict__ st, int ntiles,
                   int* __restrict__ err) {
   using PT = VecPencilTile<PL, TY, S>;
@@ -482,39 +487,48 @@ __global__ void __launch_bounds__(VecPencilTile<PL, TY, S>::kThreads, 1)
     const bool live = !load_done(st + rhs);
     if (!live) refill();
     if (live) {
-      float2 v[3][E];
+      // one component at a time: each line's spectrum goes back to its own
+      // box (thread (p, yl) writes exactly the elements it read in the last
+      // stage, so no other thread still needs them), which keeps a single
+      // line in registers instead of three
+#pragma unroll 1
+      for (int c = 0; c < 3; ++c) {
+        float2 v[E];
 #pragma unroll
-      for (int c = 0; c < 3; ++c)
+        for (int r = 0; r < E; ++r) v[r] = box(b, c)[(p + P * r) * TY + yl];
+        mixed::line_fft<PL, false>(v, fast::RowLine{box(b, c) + yl, TY}, p, a.po.tw, fast::SyncBlock{});
 #pragma unroll
-        for (int r = 0; r < E; ++r) v[c][r] = box(b, c)[(p + P * r) * TY + yl];
-#pragma unroll
-      for (int c = 0; c < 3; ++c)
-        mixed::line_fft<PL, false>(v[c], fast::RowLine{box(b, c) + yl, TY}, p, a.po.tw, fast::SyncBlock{});
-      // f_g0_vector with the 1/N of ifftn: div = (p . E) / k02e; E_i <- (E_i - p_i div) / (|p|^2 - k02e)
+        for (int m = 0; m < E; ++m) box(b, c)[(p + P * m) * TY + yl] = v[m];
+      }
+      // f_g0_vector with the 1/N of ifftn: div = (p . E) / k02e; E_i <- (E_i - p_i div) / (|p|^2 - k02e),
+      // on this thread's own k points of the three boxes
       const float px = a.w.pxe[mid], py = a.w.pye[yt * TY + yl];
-#pragma unroll
+#pragma unroll 4
       for (int m = 0; m < E; ++m) {
+        const int k = (p + P * m) * TY + yl;
         const float pz = a.w.pze[p + P * m];
         const float dr = fmaf(px, px, fmaf(py, py, pz * pz)) - a.k02e.x;
         const float inv = __fdividef(a.norm, fmaf(dr, dr, di * di));
         const float2 g0 = make_float2(dr * inv, -di * inv);
-        const float2 ex = v[0][m], ey = v[1][m], ez = v[2][m];
+        const float2 ex = box(b, 0)[k], ey = box(b, 1)[k], ez = box(b, 2)[k];
         const float2 pe =
             make_float2(fmaf(px, ex.x, fmaf(py, ey.x, pz * ez.x)), fmaf(px, ex.y, fmaf(py, ey.y, pz * ez.y)));
         const float2 dv =
             make_float2((pe.x * a.k02e.x + pe.y * a.k02e.y) / kk, (pe.y * a.k02e.x - pe.x * a.k02e.y) / kk);
-        v[0][m] = cmul(g0, make_float2(ex.x - px * dv.x, ex.y - px * dv.y));
-        v[1][m] = cmul(g0, make_float2(ey.x - py * dv.x, ey.y - py * dv.y));
-        v[2][m] = cmul(g0, make_float2(ez.x - pz * dv.x, ez.y - pz * dv.y));
+        box(b, 0)[k] = cmul(g0, make_float2(ex.x - px * dv.x, ex.y - px * dv.y));
+        box(b, 1)[k] = cmul(g0, make_float2(ey.x - py * dv.x, ey.y - py * dv.y));
+        box(b, 2)[k] = cmul(g0, make_float2(ez.x - pz * dv.x, ez.y - pz * dv.y));
       }
       refill();
+#pragma unroll 1
+      for (int c = 0; c < 3; ++c) {
+        float2 v[E];
 #pragma unroll
-      for (int c = 0; c < 3; ++c)
-        mixed::line_fft<PL, true>(v[c], fast::RowLine{box(b, c) + yl, TY}, p, a.po.tw, fast::SyncBlock{});
+        for (int r = 0; r < E; ++r) v[r] = box(b, c)[(p + P * r) * TY + yl];
+        mixed::line_fft<PL, true>(v, fast::RowLine{box(b, c) + yl, TY}, p, a.po.tw, fast::SyncBlock{});
 #pragma unroll
-      for (int c = 0; c < 3; ++c)
-#pragma unroll
-        for (int m = 0; m < E; ++m) box(b, c)[(p + P * m) * TY + yl] = v[c][m];
+        for (int m = 0; m < E; ++m) box(b, c)[(p + P * m) * TY + yl] = v[m];
+      }
       asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
     }
     __syncthreads();
