@@ -67,6 +67,16 @@ CASES = {
     "3d_224_cluster7": ((192, 192, 8), [16, 16, 4], 16, False),
     "3d_pencil_160": ((16, 16, 128), [8, 8, 16], 16, False),
     "3d_pencil_224": ((16, 16, 192), [8, 8, 16], 16, False),
+    # 2-D grids on mixed-radix lines: columns (kmc_col_*2d) and x pencils
+    # (km_pencil along x); 320 = 4 x 4 x 4 x 5, 448 = 14 x 4 x 4 x 2,
+    # 576 = 12 x 12 x 4; a partial last block of columns (Nx = 100); a
+    # power-of-two column with mixed-radix x pencils
+    "2d_320": ((256, 256), [32, 32], 16, False),
+    "2d_448": ((384, 384), [32, 32], 16, False),
+    "2d_576": ((512, 512), [32, 32], 16, False),
+    "2d_192": ((160, 160), [16, 16], 16, False),
+    "2d_320x100": ((256, 68), [32, 16], 16, False),
+    "2d_256x192": ((224, 160), [16, 16], 16, False),
     # layout variants the autotuner may choose
     "3d_256_cluster16": ((224, 224, 16), [16, 16, 8], 16, False, {"WAVESIM_B200_CLUSTER": "16"}),
     "3d_pencil_192_vector_ty8": ((16, 16, 160), [8, 8, 16], 16, True, {"WAVESIM_B200_PENCIL_TY": "8"}),

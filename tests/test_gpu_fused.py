@@ -49,6 +49,10 @@ CASES = {
     "2d_256": ((224, 224), [16, 16], None),
     "2d_1024": ((960, 960), [32, 32], None),
     "2d_512x120": ((448, 100), [32, 10], None),
+    # 2-D on mixed-radix lines (kmc_col_step2d), with a partial last block
+    "2d_320": ((256, 256), [32, 32], None),
+    "2d_576": ((512, 512), [32, 32], None),
+    "2d_320x100": ((256, 68), [32, 16], None),
     # the one-kernel step with the cluster exchange
     "128_cluster2": ((96, 96, 96), [16, 16, 16], CLUSTER),
     "256_cluster8": ((224, 224, 16), [16, 16, 8], CLUSTER),

@@ -94,6 +94,7 @@ struct FastInner {
   const void* fused_tma = nullptr;  // the same with K3's rows loaded by a tensor copy (first argument: the map)
   const void* col_step = nullptr;   // the column pass of the split fused step (kc_col_step), or null
   size_t smem_col = 0;              // its dynamic shared memory (kc_col_step2d, kmc_col_step)
+  int lines = 0;                    // 2-D: columns per block (0: 4096 / N, 16 elements per thread)
 };
 struct FastPencil {
   int no, ty;
@@ -138,6 +139,11 @@ using Plan192 = mixed::Plan<192, 12, 12, 4, 4>;
 using Plan96 = mixed::Plan<96, 12, 12, 4, 2>;
 using Plan160 = mixed::Plan<160, 20, 10, 4, 4>;
 using Plan224 = mixed::Plan<224, 28, 14, 4, 4>;
+// (radix orders by register use: 5 x 4 x 4 x 4 spilled 416 bytes a thread in
+// the 2-D column pass, 4 x 4 x 4 x 5 16; 7 x 4 x 4 x 4 84, 14 x 4 x 4 x 2 40)
+using Plan320 = mixed::Plan<320, 20, 4, 4, 4, 5>;
+using Plan448 = mixed::Plan<448, 28, 14, 4, 4, 2>;
+using Plan576 = mixed::Plan<576, 36, 12, 12, 4>;
 template <class PL, int C>
 static FastInner mixed_inner() {
   using G = mixed::MGeom<PL, C>;
@@ -151,10 +157,22 @@ static FastInner mixed_inner() {
   static_assert((size_t)PL::N * G::LR * sizeof(float2) + 128 <= G::smem, "the dense row tile fits");
   return f;
 }
+// 2-D columns on the mixed-radix lines (kmc_col_*2d), one round of lines per block
+template <class PL>
+static FastInner mixed_inner2d() {
+  using G = mixed::MGeom2d<PL>;
+  FastInner f{PL::N, 1, 0, (const void*)mixed::kmc_col_fwd2d<PL>, (const void*)mixed::kmc_col_inv2d<PL>,
+              (size_t)G::CS * sizeof(float2), 0, 0};
+  f.col_step = (const void*)mixed::kmc_col_step2d<PL>;
+  f.smem_col = mixed::smem_col_step2d<PL>();
+  f.lines = G::LPR;
+  return f;
+}
+// one component: z pencils of 3-D grids and x pencils of 2-D grids; three: z pencils only
 template <class PL, int TY, int NC>
 static FastPencil mixed_pencil() {
   return FastPencil{PL::N, TY, (const void*)mixed::km_pencil<PL, TY, NC>, NC, TY * PL::P,
-                    (size_t)(TY + 1) * PL::N * sizeof(float2), 1};
+                    (size_t)(TY + 1) * PL::N * sizeof(float2), NC == 1 ? 0 : 1};
 }
 
 static const std::vector<FastInner>& fast_inner_table() {
@@ -164,7 +182,9 @@ static const std::vector<FastInner>& fast_inner_table() {
       fast_inner<64, 1, false>(),    fast_inner<128, 1, false>(),   fast_inner<256, 1, false>(),
       fast_inner<512, 1, false>(),   fast_inner<1024, 1, false>(),  fast_inner<2048, 1, false>(),
       mixed_inner<Plan192, 6>(),     mixed_inner<Plan96, 1>(),      mixed_inner<Plan160, 5>(),
-      mixed_inner<Plan224, 7>()};
+      mixed_inner<Plan224, 7>(),
+      mixed_inner2d<Plan192>(),      mixed_inner2d<Plan320>(),      mixed_inner2d<Plan448>(),
+      mixed_inner2d<Plan576>()};
   return t;
 }
 // Persistent TMA-pipelined K2 (ws_tma.cuh) for z pencils of a 3-D grid.
@@ -245,6 +265,9 @@ static const std::vector<FastPencil>& fast_pencil_table() {
       mixed_pencil<Plan96, 16, 3>(),
       mixed_pencil<Plan160, 16, 1>(),
       mixed_pencil<Plan224, 16, 1>(),
+      mixed_pencil<Plan320, 8, 1>(),
+      mixed_pencil<Plan448, 8, 1>(),
+      mixed_pencil<Plan576, 8, 1>(),
       mixed_pencil<mixed::Plan<64, 16, 16, 4>, 16, 3>(),
       mixed_pencil<mixed::Plan<128, 16, 16, 8>, 16, 3>(),
       mixed_pencil<mixed::Plan<256, 16, 16, 16>, 16, 3>()};
@@ -375,9 +398,9 @@ static int make_layout(const Geom& g, Layout& L, std::string& why, const LayoutC
   }
   if (L.mode3d) L.fi = pick3 ? pick3 : first3;
   if (L.fi && !L.mode3d) {
-    // one round of lines per block: 256 threads, 16 elements each
+    // one round of lines per block: 256 threads, 16 elements each (mixed-radix lines: E each)
     const long long total_cols = (long long)g.nx * g.nc;
-    const long long want = std::max(1, 4096 / g.ny);
+    const long long want = L.fi->lines ? L.fi->lines : std::max(1, 4096 / g.ny);
     L.ncols = (int)want;
     L.grid_inner = (total_cols + want - 1) / want;
   }

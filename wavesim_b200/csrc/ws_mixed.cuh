@@ -242,9 +242,10 @@ __global__ void __launch_bounds__(TY* PL::P, NC == 1 ? 2 : 1)
   const int tid = threadIdx.x;
   const int yl = tid % TY, p = tid / TY;
   const int nyt = g.ny / TY;
-  const int yt = bid % nyt, mid = bid / nyt;
+  // 3-D: z pencils of column x = mid; 2-D: x pencils (mid = 0)
+  const int yt = bid % nyt, mid = a.mode3d ? bid / nyt : 0;
   const int ky = yt * TY + yl;
-  const long long ps = (long long)g.ny * g.nx;
+  const long long ps = a.mode3d ? (long long)g.ny * g.nx : (long long)g.ny;
   float2* __restrict__ base = T + ky + (long long)g.ny * mid;
   float2 v[NC][E];
 #pragma unroll
@@ -254,11 +255,13 @@ __global__ void __launch_bounds__(TY* PL::P, NC == 1 ? 2 : 1)
   fast::RowLine L{sm + yl, TYS};
 #pragma unroll
   for (int c = 0; c < NC; ++c) line_fft<PL, false>(v[c], L, p, a.po.tw, fast::SyncBlock{});
-  const float px = a.w.pxe[mid], py = a.w.pye[ky];
+  const float pxm = a.w.pxe[mid], py = a.w.pye[ky], pz0 = a.w.pze[0];
   const float di = -a.k02e.y;
 #pragma unroll
   for (int m = 0; m < E; ++m) {
-    const float pz = a.w.pze[p + P * m];
+    // the pencil's own coordinate: z in 3-D, x in 2-D
+    const float px = a.mode3d ? pxm : a.w.pxe[p + P * m];
+    const float pz = a.mode3d ? a.w.pze[p + P * m] : pz0;
     const float dr = fmaf(px, px, fmaf(py, py, pz * pz)) - a.k02e.x;
     const float inv = __fdividef(a.norm, fmaf(dr, dr, di * di));
     const float2 g0 = make_float2(dr * inv, -di * inv);
@@ -879,6 +882,204 @@ __global__ void __launch_bounds__(kThreads, 2)
     for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
     if (tid == 0) partials[bid] = (double)v;
   }
+}
+
+// 2-D grids on the mixed-radix lines: the y transforms of whole columns, as
+// the power-of-two kf_plane_fwd / kf_plane_inv / kc_col_step2d do them for
+// 2-D (K2 transforms along x).  Block bid covers the columns bid M ... bid M
+// + M - 1 (M = a.ncols = LPR, column col = x + Nx c) in one round of lines;
+// idle lanes of a partial last block transform a scratch column.
+//   kmc_col_fwd2d<PL>   K1: source share, ramps, forward y transform
+//   kmc_col_inv2d<PL>   K3: inverse y transform, unwiggle, f_mix, E' += dE',
+//                       ROI energy
+//   kmc_col_step2d<PL>  K3 of an iteration and K1 of the next in one pass
+//                       (the ramps of both wiggles in shared memory), the
+//                       same arithmetic in the same order, so its fields
+//                       equal the separate kernels' bit for bit
+template <class PL>
+struct MGeom2d {
+  static constexpr int N = PL::N, P = PL::P;
+  static constexpr int CS = N + N / 16 + 1;
+  static constexpr int LPR = kThreads / P;
+  static_assert(kThreads % P == 0 && (P <= 32 ? 32 % P == 0 : true), "threads per line");
+};
+
+// dynamic shared memory of kmc_col_step2d: LPR + 1 columns and the two y ramps
+template <class PL>
+constexpr size_t smem_col_step2d() {
+  return sizeof(float2) * ((size_t)(MGeom2d<PL>::LPR + 1) * MGeom2d<PL>::CS + 2 * PL::N);
+}
+
+enum { kCol2dFwd = 0, kCol2dInv = 1, kCol2dStep = 2 };
+
+template <class PL, int MODE>
+__device__ __forceinline__ void col2d(const InnerArgs& a, const Wig& w1, const float2* __restrict__ din,
+                                      const float2* __restrict__ src, float2 A, float2* __restrict__ T,
+                                      float2* __restrict__ dE, float2* __restrict__ E,
+                                      const float2* __restrict__ gamma, const DevState* __restrict__ st,
+                                      double* __restrict__ partials) {
+  using G = MGeom2d<PL>;
+  constexpr int N = PL::N, EL = PL::E, P = PL::P, LPR = G::LPR;
+  using Sync = typename LineSync<P>::type;
+  const int rhs = blockIdx.x / a.bpr, bid = blockIdx.x - rhs * a.bpr;
+  st += rhs;
+  if (load_done(st)) return;
+  T += rhs * a.fstride;
+  if (src) src += rhs * a.fstride;
+  bool acc_now = false;
+  if constexpr (MODE == kCol2dFwd) {
+    din += rhs * a.fstride;
+  } else {
+    acc_now = !a.acc2 || (__ldcg(&st->it) & 1) == 0;
+    dE += rhs * a.fstride;
+    E += rhs * a.fstride;
+    partials += (long long)rhs * a.bpr;
+    gamma += rhs * a.gstride;  // a batch of media: each right-hand side has its own gamma
+  }
+  extern __shared__ float2 smx[];
+  float2* const sgy = smx + (LPR + 1) * G::CS;  // kCol2dStep only
+  __shared__ float red[kThreads / 32];
+  const int tid = threadIdx.x;
+  if constexpr (MODE == kCol2dStep) {
+    for (int i = tid; i < N; i += kThreads) {
+      sgy[i] = a.w.gy[i];
+      sgy[N + i] = w1.gy[i];
+    }
+    __syncthreads();
+  }
+  const Geom& g = a.g;
+  const int nx = g.nx;
+  const int M = a.ncols;
+  const long long colbase = (long long)bid * M;
+  const int ncol = (int)min((long long)M, (long long)nx * g.nc - colbase);
+  const float2 gzz = a.w.gz[0];
+  float esum = 0.f;
+  for (int c0 = 0; c0 < ncol; c0 += LPR) {
+    const int cl = tid / P, cc = c0 + cl, p = tid % P;
+    const bool live = cc < ncol;
+    const long long col = colbase + cc;
+    const long long gcol = col * N;
+    fast::ColLine L{smx + (live ? cl : LPR) * G::CS};
+    float2 v[EL];
+    if constexpr (MODE == kCol2dFwd) {
+      if (live) {
+        const int x = (int)(col % nx);
+        const float2 gxz = cmul(a.w.gx[x], gzz);
+#pragma unroll
+        for (int r = 0; r < EL; ++r) {
+          const int y = p + P * r;
+          float2 e = din[gcol + y];
+          if (src) e = cadd(e, cmul(A, src[gcol + y]));
+          v[r] = cmul(cmul(e, gxz), a.w.gy[y]);
+        }
+      } else {
+#pragma unroll
+        for (int r = 0; r < EL; ++r) v[r] = make_float2(0.f, 0.f);
+      }
+      line_fft<PL, false>(v, L, p, a.py.tw, Sync{});
+      if (live) {
+#pragma unroll
+        for (int m = 0; m < EL; ++m) T[gcol + p + P * m] = v[m];
+      }
+    } else {
+      if (live) {
+#pragma unroll
+        for (int r = 0; r < EL; ++r) v[r] = T[gcol + p + P * r];
+      } else {
+#pragma unroll
+        for (int r = 0; r < EL; ++r) v[r] = make_float2(0.f, 0.f);
+      }
+      line_fft<PL, true>(v, L, p, a.py.tw, Sync{});
+      if (live) {
+        const int x = (int)(col % nx), c = (int)(col / nx);
+        const float2 gxz = cmul(a.w.gx[x], gzz);
+        const bool in_xzc = x >= g.r0[1] && x < g.r1[1] && 0 >= g.r0[2] && 0 < g.r1[2] && c >= g.r0[3] && c < g.r1[3];
+        const float2* __restrict__ gmc = gamma + (gcol - (long long)c * g.npts);
+        float2* __restrict__ dEc = dE + gcol;
+        float2* __restrict__ Ec = E + gcol;
+        constexpr int NH = kEpilogueParts<EL>, H = EL / NH;
+#pragma unroll
+        for (int h = 0; h < NH; ++h) {
+          float2 gm[H], d0[H], e0[H];
+#pragma unroll
+          for (int i = 0; i < H; ++i) {
+            const int y = p + P * (H * h + i);
+            gm[i] = gmc[y];
+            d0[i] = dEc[y];
+            e0[i] = acc_now ? Ec[y] : make_float2(0.f, 0.f);
+          }
+#pragma unroll
+          for (int i = 0; i < H; ++i) {
+            const int m = H * h + i;
+            const int y = p + P * m;
+            const float2 gyy = MODE == kCol2dStep ? sgy[y] : a.w.gy[y];
+            const float2 ep = cmul_conj(cmul_conj(v[m], gxz), gyy);
+            const float2 one_m = make_float2(1.f - kAlpha * gm[i].x, -kAlpha * gm[i].y);
+            const float2 t = cmul(cmul(gm[i], gm[i]), ep);
+            const float2 dn = cadd(cmul(one_m, d0[i]), make_float2(kAlpha * t.y, -kAlpha * t.x));
+            dEc[y] = dn;
+            if (acc_now) Ec[y] = cadd(e0[i], a.acc2 ? cadd(d0[i], dn) : dn);
+            if (in_xzc && y >= g.r0[0] && y < g.r1[0]) esum = fmaf(dn.x, dn.x, fmaf(dn.y, dn.y, esum));
+            v[m] = dn;
+          }
+        }
+        if constexpr (MODE == kCol2dStep) {
+          // K1 of the next iteration on the same column: source, next ramps
+          const float2 gxz1 = cmul(w1.gx[x], w1.gz[0]);
+          const float2* __restrict__ sr = src ? src + gcol : nullptr;
+#pragma unroll
+          for (int m = 0; m < EL; ++m) {
+            const int y = p + P * m;
+            float2 e = v[m];
+            if (sr) e = cadd(e, cmul(A, sr[y]));
+            v[m] = cmul(cmul(e, gxz1), sgy[N + y]);
+          }
+        }
+      }
+      if constexpr (MODE == kCol2dStep) {
+        line_fft<PL, false>(v, L, p, a.py.tw, Sync{});
+        if (live) {
+#pragma unroll
+          for (int m = 0; m < EL; ++m) T[gcol + p + P * m] = v[m];
+        }
+      }
+    }
+  }
+  if constexpr (MODE != kCol2dFwd) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) esum += __shfl_xor_sync(0xffffffffu, esum, o);
+    if ((tid & 31) == 0) red[tid >> 5] = esum;
+    __syncthreads();
+    if (tid < 32) {
+      float v = tid < kThreads / 32 ? red[tid] : 0.f;
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+      if (tid == 0) partials[bid] = (double)v;
+    }
+  }
+}
+
+template <class PL>
+__global__ void __launch_bounds__(kThreads, 2)
+    kmc_col_fwd2d(InnerArgs a, const float2* __restrict__ dE, const float2* __restrict__ src, float2 A,
+                  float2* __restrict__ T, const DevState* __restrict__ st) {
+  col2d<PL, kCol2dFwd>(a, a.w, dE, src, A, T, nullptr, nullptr, nullptr, st, nullptr);
+}
+
+template <class PL>
+__global__ void __launch_bounds__(kThreads, 2)
+    kmc_col_inv2d(InnerArgs a, const float2* __restrict__ T, float2* __restrict__ dE, float2* __restrict__ E,
+                  const float2* __restrict__ gamma, const DevState* __restrict__ st, double* __restrict__ partials) {
+  col2d<PL, kCol2dInv>(a, a.w, nullptr, nullptr, make_float2(0.f, 0.f), const_cast<float2*>(T), dE, E, gamma,
+                       st, partials);
+}
+
+template <class PL>
+__global__ void __launch_bounds__(kThreads, 2)
+    kmc_col_step2d(InnerArgs a, Wig w1, const float2* __restrict__ src1, float2 A, float2* __restrict__ T,
+                   float2* __restrict__ dE, float2* __restrict__ E, const float2* __restrict__ gamma,
+                   const DevState* __restrict__ st, double* __restrict__ partials) {
+  col2d<PL, kCol2dStep>(a, w1, nullptr, src1, A, T, dE, E, gamma, st, partials);
 }
 
 }  // namespace mixed
