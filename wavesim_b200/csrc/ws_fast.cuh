@@ -1133,6 +1133,17 @@ __global__ void __launch_bounds__(kThreads, 2)
   const int rank = (int)(bid % C), plane = bid / C;
   const int x0 = rank * M, z = plane % g.nz, comp = plane / g.nz;
   const long long colbase = (long long)plane * nx + x0;
+  if (tid == 0) {
+    // the block's M columns of gamma, dE' (and E', the next source) are
+    // contiguous: pull them into L2 now, so that the epilogue's loads, which
+    // wait for the inverse transform, find them there
+    const long long off = colbase * N;
+    constexpr unsigned bytes = (unsigned)(M * N * sizeof(float2));
+    prefetch_l2(gamma + (off - (long long)comp * g.npts), bytes);
+    prefetch_l2(dE + off, bytes);
+    if (acc_now) prefetch_l2(E + off, bytes);
+    if (src1) prefetch_l2(src1 + off, bytes);
+  }
   // the y ramps of this and the next wiggle, read from shared memory: as
   // per-element global loads inside the epilogue they left the pass latency
   // bound (0.19 against 0.12 ms at 256^3)

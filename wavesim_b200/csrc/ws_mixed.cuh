@@ -805,16 +805,27 @@ __global__ void __launch_bounds__(kThreads, 2)
   float2* const sgy = smc + LPR * G::CS;
   __shared__ float red[kThreads / 32];
   const int tid = threadIdx.x;
-  for (int i = tid; i < N; i += kThreads) {
-    sgy[i] = a.w.gy[i];
-    sgy[N + i] = w1.gy[i];
-  }
-  __syncthreads();
   const Geom& g = a.g;
   const int nx = g.nx;
   const int rank = (int)(bid % C), plane = bid / C;
   const int x0 = rank * M, z = plane % g.nz, comp = plane / g.nz;
   const long long colbase = (long long)plane * nx + x0;
+  if (tid == 0) {
+    // the block's M columns of gamma, dE' (and E', the next source) are
+    // contiguous: pull them into L2 now, so that the epilogue's loads, which
+    // wait for the inverse transform, find them there
+    const long long off = colbase * N;
+    constexpr unsigned bytes = (unsigned)(M * N * sizeof(float2));
+    fast::prefetch_l2(gamma + (off - (long long)comp * g.npts), bytes);
+    fast::prefetch_l2(dE + off, bytes);
+    if (acc_now) fast::prefetch_l2(E + off, bytes);
+    if (src1) fast::prefetch_l2(src1 + off, bytes);
+  }
+  for (int i = tid; i < N; i += kThreads) {
+    sgy[i] = a.w.gy[i];
+    sgy[N + i] = w1.gy[i];
+  }
+  __syncthreads();
   const float2 gzz = a.w.gz[z];
   const float2 gzz1 = w1.gz[z];
   float esum = 0.f;
