@@ -790,7 +790,11 @@ __global__ void __launch_bounds__(kThreads, 2)
                  const DevState* __restrict__ st, double* __restrict__ partials) {
   using G = MGeom<PL, C>;
   constexpr int N = PL::N, EL = PL::E, P = PL::P, M = G::M, LPR = G::LPR;
-  const int rhs = blockIdx.x / a.bpr, bid = blockIdx.x - rhs * a.bpr;
+  // blocks in reverse order: the pass starts on the planes the inverse x
+  // pencils wrote last (still in L2), and ends on the planes the forward x
+  // pencils read first; a block's columns and energy partial do not change
+  const int rb = (int)gridDim.x - 1 - (int)blockIdx.x;
+  const int rhs = rb / a.bpr, bid = rb - rhs * a.bpr;
   st += rhs;
   if (load_done(st)) return;
   const bool acc_now = !a.acc2 || (__ldcg(&st->it) & 1) == 0;
