@@ -102,7 +102,7 @@ struct FastPencil {
   int nc;        // components it transforms together (1, or 3 with the dyadic Green's function)
   int threads;
   size_t smem;
-  int only3d;    // z pencils of a 3-D grid only
+  int dims;      // 3: z pencils of 3-D grids only; 2: x pencils of 2-D grids only; 0: both
 };
 
 template <int N, int C, bool DX>
@@ -168,11 +168,16 @@ static FastInner mixed_inner2d() {
   f.lines = G::LPR;
   return f;
 }
-// one component: z pencils of 3-D grids and x pencils of 2-D grids; three: z pencils only
+// z pencils of 3-D grids (one or three components), and x pencils of 2-D grids (one)
 template <class PL, int TY, int NC>
 static FastPencil mixed_pencil() {
-  return FastPencil{PL::N, TY, (const void*)mixed::km_pencil<PL, TY, NC>, NC, TY * PL::P,
-                    (size_t)(TY + 1) * PL::N * sizeof(float2), NC == 1 ? 0 : 1};
+  return FastPencil{PL::N, TY, (const void*)mixed::km_pencil<PL, TY, NC, true>, NC, TY * PL::P,
+                    (size_t)(TY + 1) * PL::N * sizeof(float2), 3};
+}
+template <class PL, int TY>
+static FastPencil mixed_pencil2d() {
+  return FastPencil{PL::N, TY, (const void*)mixed::km_pencil<PL, TY, 1, false>, 1, TY * PL::P,
+                    (size_t)(TY + 1) * PL::N * sizeof(float2), 2};
 }
 
 static const std::vector<FastInner>& fast_inner_table() {
@@ -265,9 +270,10 @@ static const std::vector<FastPencil>& fast_pencil_table() {
       mixed_pencil<Plan96, 16, 3>(),
       mixed_pencil<Plan160, 16, 1>(),
       mixed_pencil<Plan224, 16, 1>(),
-      mixed_pencil<Plan320, 8, 1>(),
-      mixed_pencil<Plan448, 8, 1>(),
-      mixed_pencil<Plan576, 8, 1>(),
+      mixed_pencil2d<Plan192, 16>(),
+      mixed_pencil2d<Plan320, 8>(),
+      mixed_pencil2d<Plan448, 8>(),
+      mixed_pencil2d<Plan576, 8>(),
       mixed_pencil<mixed::Plan<64, 16, 16, 4>, 16, 3>(),
       mixed_pencil<mixed::Plan<128, 16, 16, 8>, 16, 3>(),
       mixed_pencil<mixed::Plan<256, 16, 16, 16>, 16, 3>()};
@@ -412,7 +418,7 @@ static int make_layout(const Geom& g, Layout& L, std::string& why, const LayoutC
     if (!want_ty)
       if (const char* e = std::getenv("WAVESIM_B200_PENCIL_TY")) want_ty = std::atoi(e);
     for (const FastPencil& f : fast_pencil_table())
-      if (f.no == no && g.ny % f.ty == 0 && f.nc == g.nc && (L.mode3d || !f.only3d) && (!want_ty || f.ty == want_ty))
+      if (f.no == no && g.ny % f.ty == 0 && f.nc == g.nc && (f.dims == 0 || f.dims == (L.mode3d ? 3 : 2)) && (!want_ty || f.ty == want_ty))
         L.fp = &f;
   }
   if (L.fp) L.grid_outer = (long long)(g.ny / L.fp->ty) * mids;  // blocks of the fast pencil kernel

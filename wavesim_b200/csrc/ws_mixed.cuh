@@ -229,7 +229,10 @@ __global__ void __launch_bounds__(kThreads, 3)
 }
 
 // K2 --------------------------------------------------------------------------
-template <class PL, int TY, int NC>
+// D3: z pencils of a 3-D grid; otherwise x pencils of a 2-D grid (a
+// compile-time choice: the run-time branch cost the 3-D pencils registers
+// and 25-35% of their speed)
+template <class PL, int TY, int NC, bool D3 = true>
 __global__ void __launch_bounds__(TY* PL::P, NC == 1 ? 2 : 1)
     km_pencil(OuterArgs a, float2* __restrict__ T, const DevState* __restrict__ st) {
   constexpr int E = PL::E, P = PL::P, TYS = TY + 1;
@@ -243,9 +246,9 @@ __global__ void __launch_bounds__(TY* PL::P, NC == 1 ? 2 : 1)
   const int yl = tid % TY, p = tid / TY;
   const int nyt = g.ny / TY;
   // 3-D: z pencils of column x = mid; 2-D: x pencils (mid = 0)
-  const int yt = bid % nyt, mid = a.mode3d ? bid / nyt : 0;
+  const int yt = bid % nyt, mid = D3 ? bid / nyt : 0;
   const int ky = yt * TY + yl;
-  const long long ps = a.mode3d ? (long long)g.ny * g.nx : (long long)g.ny;
+  const long long ps = D3 ? (long long)g.ny * g.nx : (long long)g.ny;
   float2* __restrict__ base = T + ky + (long long)g.ny * mid;
   float2 v[NC][E];
 #pragma unroll
@@ -260,8 +263,8 @@ __global__ void __launch_bounds__(TY* PL::P, NC == 1 ? 2 : 1)
 #pragma unroll
   for (int m = 0; m < E; ++m) {
     // the pencil's own coordinate: z in 3-D, x in 2-D
-    const float px = a.mode3d ? pxm : a.w.pxe[p + P * m];
-    const float pz = a.mode3d ? a.w.pze[p + P * m] : pz0;
+    const float px = D3 ? pxm : a.w.pxe[p + P * m];
+    const float pz = D3 ? a.w.pze[p + P * m] : pz0;
     const float dr = fmaf(px, px, fmaf(py, py, pz * pz)) - a.k02e.x;
     const float inv = __fdividef(a.norm, fmaf(dr, dr, di * di));
     const float2 g0 = make_float2(dr * inv, -di * inv);
