@@ -53,6 +53,7 @@ def parse():
     p.add_argument("--batch", type=int, default=4, help="right-hand sides of the batched leg (0: skip)")
     p.add_argument("--media", type=int, default=48, help="media of mixed sizes in the concurrent leg (0: skip)")
     p.add_argument("--angles", type=int, default=128, help="plane-wave angles on the 1024^2 medium (0: skip)")
+    p.add_argument("--sweep-batch", type=int, default=8, help="angles per round of the continuation sweep")
     return p.parse_args()
 
 
@@ -692,7 +693,11 @@ def run_angles(args):
     """C5's angle sweep: args.angles plane waves at incidence angles uniform in
     +-30 degrees on the c2 medium (2-D 1024^2, Gaussian random field), one
     batched solve (sources generated on the device) against single solves of
-    a sample of 8 of the angles; solves/s of both."""
+    a sample of 8 of the angles; then the continuation sweep
+    (wavesim_b200.batch.solve_sweep: rounds of args.sweep_batch angles, each
+    later angle warm-started from its neighbour's tilted field) against the
+    same rounds cold, and the accuracy of cold and continued fields against
+    tight solves at three angles."""
     import torch
     import wavesim_b200 as ws
     n, opt, _, _, _ = load_workloads().CONFIGS["c2"]()
@@ -702,7 +707,7 @@ def run_angles(args):
     k = 2 * np.pi / sim.lambda_ * float(opt["pixel_size"])
     angles = np.linspace(-30, 30, args.angles)
     waves = [ws.PlaneWave((ny, 1), [1, 1], amplitude=1.0, phase=(k * np.sin(np.radians(a)), 0.0)) for a in angles]
-    sim.exec_batch(waves[:2])  # warm-up
+    sim.exec_batch(waves)  # warm-up: graph, and the pinned output staging at the batch's size
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     Eb, sb = sim.exec_batch(waves)
@@ -718,11 +723,53 @@ def run_angles(args):
         its.append(st[0].it - 1)
     torch.cuda.synchronize()
     t_s = (time.perf_counter() - t0) / len(sample)
+    # continuation: rounds of args.sweep_batch angles, each angle after the
+    # first round warm-started from its neighbour's field tilted to its angle
+    from wavesim_b200.batch import solve_sweep
+    solve_sweep(sim, waves[:2 * args.sweep_batch], batch=args.sweep_batch)  # warm-up: the warm graph
+    torch.cuda.synchronize()
+    # the same rounds cold, to separate the starts' gain from the batch size
+    rounds = -(-len(waves) // args.sweep_batch)
+    t0 = time.perf_counter()
+    cold_it = []
+    for j in range(rounds):
+        _, st = sim.exec_batch(waves[j::rounds])
+        cold_it += [x.it - 1 for x in st]
+    torch.cuda.synchronize()
+    t_rc = time.perf_counter() - t0
+    Ew, sw, t_w = solve_sweep(sim, waves, batch=args.sweep_batch)
+    torch.cuda.synchronize()
+    # accuracy of both against tight solves (threshold 1e-9) at a few angles
+    simt = ws.WaveSim(n, dict(opt, device_setup=True, energy_threshold=1e-9))
+    errs = []
+    for i in (len(waves) // 4 + 1, len(waves) // 2 + 1, 3 * len(waves) // 4 + 1):
+        Et, _ = simt.exec_batch([waves[i]])
+        ref = Et[0]
+        nr = float(np.linalg.norm(ref))
+        errs.append({"angle_deg": float(angles[i]), "cold": float(np.linalg.norm(Eb[i] - ref)) / nr,
+                     "continuation": float(np.linalg.norm(Ew[i] - ref)) / nr})
+    simt.close()
     sim.close()
+    warm_it = [x.it - 1 for x in sw]
+    round_max = [max(warm_it[j::rounds]) for j in range(rounds)]
     return {"angles": len(waves), "grid": [int(v) for v in sim.N[:2]], "ms_batch": t_b * 1e3,
             "ms_per_solve_batched": t_b * 1e3 / len(waves), "ms_per_solve_single": t_s * 1e3,
             "speedup": t_s * len(waves) / t_b, "iterations": [s.it - 1 for s in sb][:: max(1, len(waves) // 8)],
-            "single_iterations": its, "timing": "host wall clock, fields copied to the host included"}
+            "single_iterations": its,
+            "continuation": {"rounds": rounds, "batch": args.sweep_batch,
+                             "ms_per_solve": t_w * 1e3 / len(waves),
+                             "ms_per_solve_same_rounds_cold": t_rc * 1e3 / len(waves),
+                             "mean_iterations": float(np.mean(warm_it)),
+                             "mean_iterations_cold": float(np.mean(cold_it)),
+                             "round_max_iterations": round_max,
+                             "iterations_sample": warm_it[:: max(1, len(waves) // 16)],
+                             "discarded": int(sum(bool(getattr(x, "warm_discarded", False)) for x in sw)),
+                             "speedup_vs_single": t_s * len(waves) / t_w,
+                             "speedup_vs_batched_cold": t_b / t_w,
+                             "rel_l2_vs_tight_solve": errs,
+                             "note": "round 0 cold; every later angle starts from its neighbour's field "
+                                     "times the tilt between the two plane waves (wavesim_b200.batch.solve_sweep)"},
+            "timing": "host wall clock, fields copied to the host included"}
 
 
 def run_e2e(args, sim, s, keep, torch, dev):

@@ -10,6 +10,10 @@ No counterpart in the reference, whose ``exec`` runs one solve at a time
   ``solve_media``: one solver for all of them (``ws_solver_create_media``,
   one gamma per medium) and one batched solve, every kernel launch covering
   every medium of the group.
+* An ordered sweep of sources on one medium (incidence angles) goes through
+  ``solve_sweep``: batched solves in rounds, each source of a later round
+  warm-started from its neighbour's field of the round before
+  (``plane_wave_start`` tilts a plane wave's field to the next angle).
 * Groups of different sizes cannot share a launch (each size has its own FFT
   plan and kernel shapes); ``solve_media`` and ``solve_many`` run them
   concurrently instead: each solver has its own CUDA stream, and ``workers``
@@ -49,6 +53,129 @@ def solve_many(problems, workers=4, warm_starts=None):
             out = list(ex.map(run, range(len(problems))))
     dt = time.perf_counter() - t0
     return [o[0] for o in out], [o[1] for o in out], dt
+
+
+def plane_wave_tilt(sim, w_from, w_to):
+    """The ratio of plane wave w_to to plane wave w_from (blocks of the same
+    size and place) continued over the ROI, as three 1-D factors along y, x
+    and z (the amplitude ratio and the phase offset folded into the first).
+    Along the block's own axes the phase per pixel changes by dphase; along
+    an axis where the block is one pixel thick (its normal) the wave travels
+    away from the block with the phase per pixel kn = sqrt(kc^2 - |phase|^2),
+    kc = k0c times the pixel size (the loop's background wavenumber), so
+    the factor there is exp(i (kn_to - kn_from) |r - corner|)."""
+    r = sim.roi
+    n = [int(r[1, d] - r[0, d] + 1) for d in range(3)]
+    kc = float(np.real(sim.k0c)) * float(sim.options.get("pixel_size", 1.0))
+    ph_from = np.asarray(w_from.phase, float)
+    ph_to = np.asarray(w_to.phase, float)
+    f = []
+    for d in range(3):
+        a = np.arange(n[d]) - (int(w_from.position[d]) - 1)
+        if int(w_from.size[d]) > 1 or n[d] == 1:
+            f.append(np.exp(1j * (ph_to[d] - ph_from[d]) * a))
+        else:
+            kt_from = sum(ph_from[e] ** 2 for e in range(3) if e != d)
+            kt_to = sum(ph_to[e] ** 2 for e in range(3) if e != d)
+            kn = np.sqrt(max(kc * kc - kt_to, 0.0)) - np.sqrt(max(kc * kc - kt_from, 0.0))
+            f.append(np.exp(1j * kn * np.abs(a)))
+    f[0] = f[0] * (w_to.amplitude / w_from.amplitude) * np.exp(1j * (w_to.phase0 - w_from.phase0))
+    return f
+
+
+def plane_wave_start(sim, E_from, w_from, w_to):
+    """A start for plane wave w_to from the field E_from (on the ROI, [y, x],
+    [y, x, z] or [y, x, z, c]) that plane wave w_from produced: E_from times
+    plane_wave_tilt.  Exact in a homogeneous medium; in a scattering one it
+    holds for small tilts (the memory effect)."""
+    fy, fx, fz = plane_wave_tilt(sim, w_from, w_to)
+    E = np.asarray(E_from)
+    m = fy[:, None] * fx[None, :]
+    if E.ndim >= 3:
+        m = m[:, :, None] * fz[None, None, :]
+    if E.ndim == 4:
+        m = m[..., None]
+    return (E * m).astype(np.complex64)
+
+
+def _sweep_device(sim, sources, k):
+    """solve_sweep for PlaneWave sources with the fields kept on the device:
+    each round's starts are its predecessors' fields (rows of the round
+    before) times the tilt, continued over the grid by WaveSim.device_starts,
+    and passed to the solver as device memory."""
+    import torch
+    n = len(sources)
+    r = sim.roi
+    rs = [int(r[1, d] - r[0, d] + 1) for d in range(4)]
+    fields, states = [None] * n, [None] * n
+    prev = None
+    for j in range(k):
+        idx = list(range(j, n, k))
+        srcs = [sources[i] for i in idx]
+        starts = None
+        if j:
+            m = len(idx)
+            dev = prev.device
+            tl = [plane_wave_tilt(sim, sources[i - 1], sources[i]) for i in idx]
+            fy = torch.from_numpy(np.stack([t[0] for t in tl]).astype(np.complex64)).to(dev)
+            fx = torch.from_numpy(np.stack([t[1] for t in tl]).astype(np.complex64)).to(dev)
+            fz = torch.from_numpy(np.stack([t[2] for t in tl]).astype(np.complex64)).to(dev)
+            t = prev[:m].reshape(m, rs[3], rs[2], rs[1], rs[0])  # [rhs, c, z, x, y]
+            t = t * fy[:, None, None, None, :] * fx[:, None, None, :, None] * fz[:, None, :, None, None]
+            starts = sim.device_starts(t.reshape(m, -1))
+        outs, st, prev = sim._exec_plane_waves(srcs, starts, time.perf_counter(), keep_device=True)
+        for i, e, s_ in zip(idx, outs, st):
+            fields[i], states[i] = e, s_
+    return fields, states
+
+
+def solve_sweep(sim, sources, batch=8, start=None, device=None):
+    """An ordered sweep of sources on one medium (e.g. incidence angles in
+    order, neighbours giving similar fields), batched and warm-started by
+    continuation.  With k = ceil(len / batch) rounds, round 0 solves sources
+    0, k, 2k, ... cold in one batched solve; round j solves j, j + k, ...,
+    each started from the field of its predecessor (solved in round j - 1)
+    mapped by start(E_prev, i_prev, i) (default: plane_wave_start for
+    PlaneWave sources, the predecessor's field itself otherwise).  For
+    PlaneWave sources with the default start the fields stay on the device
+    between rounds (device=None: when CUDA is there; the host path does the
+    same arithmetic on host arrays).  Each solve runs to the usual
+    tolerance; a start whose initial residual is worse than a cold start's is
+    discarded and rerun cold.  Returns (fields, states, seconds) in the order
+    of `sources`.  No counterpart in the reference, whose sweeps call exec
+    once per source (examples/pulse2d.m:31-40)."""
+    from .problem import PlaneWave
+    n = len(sources)
+    if n == 0:
+        return [], [], 0.0
+    k = -(-n // max(1, int(batch)))
+    t0 = time.perf_counter()
+    waves = all(isinstance(s, PlaneWave) for s in sources)
+    if device is None:
+        try:
+            import torch
+            device = waves and start is None and torch.cuda.is_available()
+        except ImportError:
+            device = False
+    if device:
+        fields, states = _sweep_device(sim, sources, k)
+        return fields, states, time.perf_counter() - t0
+    if start is None:
+        if waves:
+            def start(E, i, j):
+                return plane_wave_start(sim, E, sources[i], sources[j])
+        else:
+            def start(E, i, j):
+                return E
+    fields, states = [None] * n, [None] * n
+    for j in range(k):
+        idx = list(range(j, n, k))
+        srcs = [sources[i] for i in idx]
+        warm = None if j == 0 else [start(fields[i - 1], i - 1, i) for i in idx]
+        E, st = sim.exec_batch(srcs, warm_starts=warm)
+        for i, e, s_ in zip(idx, E, st):
+            fields[i], states[i] = e, s_
+    return fields, states, time.perf_counter() - t0
 
 
 def media_key(sim):
@@ -127,16 +254,19 @@ class MediaBatch:
         o = first._options()
         r = first.roi
         shape = tuple(int(r[1, d] - r[0, d] + 1) for d in range(4))
-        E = np.empty((R,) + shape[::-1], dtype=np.complex64)
+        if getattr(self, "_hstage", None) is None:
+            self._hstage = _lib.HostStage()
+        buf = self._hstage.get(R * np.prod(shape))
         cap = o.max_iterations + len(first.wiggles) + 1
         hist = np.zeros((R, cap))
         n_it = np.zeros(R, dtype=np.int64)
         conv = np.zeros(R, dtype=np.int32)
         t0 = time.perf_counter()
         _lib.check(_lib.lib.ws_solver_solve_batch(
-            self.h, R, (C.c_int64 * R)(*counts), blocks, _lib.WS_HOST, C.byref(o), E.ctypes.data, _lib.WS_HOST,
+            self.h, R, (C.c_int64 * R)(*counts), blocks, _lib.WS_HOST, C.byref(o), buf.ctypes.data, _lib.WS_HOST,
             hist.ctypes.data_as(C.POINTER(C.c_double)), cap, n_it.ctypes.data_as(C.POINTER(C.c_int64)),
             conv.ctypes.data_as(C.POINTER(C.c_int))))
+        E = _lib.HostStage.take(buf, (R,) + shape[::-1])
         dt = time.perf_counter() - t0
         del keep
         outs, states = [], []

@@ -151,14 +151,17 @@ class PSTD:
             o.amplitude = amp_keep
         r = self.roi
         shape = tuple(int(r[1, d] - r[0, d] + 1) for d in range(3))
-        E = np.empty(shape, dtype=np.complex64, order="F")
+        if getattr(self, "_hstage", None) is None:
+            self._hstage = _lib.HostStage()
+        buf = self._hstage.get(np.prod(shape))
         cap = min(o.max_iterations, 10 ** 6) + 4096
         hist = np.zeros(cap)
         n_it = C.c_int64()
         conv = C.c_int()
-        _lib.check(_lib.lib.ws_pstd_run(h, len(s.values), blocks, _lib.WS_HOST, C.byref(o), E.ctypes.data,
+        _lib.check(_lib.lib.ws_pstd_run(h, len(s.values), blocks, _lib.WS_HOST, C.byref(o), buf.ctypes.data,
                                         hist.ctypes.data_as(C.POINTER(C.c_double)), cap, C.byref(n_it),
                                         C.byref(conv)))
+        E = _lib.HostStage.take(buf, shape, "F")
         del keep, amp_keep
         state.it = int(n_it.value) + 1
         state.diff_energy = hist[:min(n_it.value, cap)].copy()

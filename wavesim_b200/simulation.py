@@ -293,6 +293,12 @@ class WaveSim:
         n = n[..., 0] if n.ndim == 4 else n
         return np.real(n[lo[0]:hi[0], lo[1]:hi[1], lo[2]:hi[2]]).astype(np.float32)
 
+    def _stage(self):
+        """This simulation's pinned staging buffer for solver outputs."""
+        if getattr(self, "_hstage", None) is None:
+            self._hstage = _lib.HostStage()
+        return self._hstage
+
     def initial_field(self, psi0):
         """A starting field psi0 on the full grid (complex64, column-major, as
         the C ABI takes it).  psi0 is given on the full grid or on the ROI
@@ -397,13 +403,14 @@ class WaveSim:
             shape = tuple(int(r[1, d] - r[0, d] + 1) for d in range(4))
         else:
             shape = tuple(int(v) for v in self.N)
-        E = np.empty(shape, dtype=np.complex64, order="F")
+        buf = self._stage().get(np.prod(shape))
         hist = np.zeros(o.max_iterations + len(self.wiggles) + 1)
         n_it = C.c_int64()
         conv = C.c_int()
         _lib.check(_lib.lib.ws_solver_solve(
-            h, len(s.values), blocks, _lib.WS_HOST, C.byref(o), E.ctypes.data, _lib.WS_HOST,
+            h, len(s.values), blocks, _lib.WS_HOST, C.byref(o), buf.ctypes.data, _lib.WS_HOST,
             hist.ctypes.data_as(C.POINTER(C.c_double)), C.byref(n_it), C.byref(conv)))
+        E = _lib.HostStage.take(buf, shape, "F")
         del keep, cb_keep
         state.it = int(n_it.value) + 1  # Simulation.next leaves it one past the last iteration
         state.diff_energy = hist[:n_it.value].copy()
@@ -469,37 +476,45 @@ class WaveSim:
             o.initial_memory = _lib.WS_HOST
         r = self.roi
         shape = tuple(int(r[1, d] - r[0, d] + 1) for d in range(4))
-        E = np.empty((R,) + shape[::-1], dtype=np.complex64)  # each field column-major
+        buf = self._stage().get(R * np.prod(shape))
         cap = o.max_iterations + len(self.wiggles) + 1
         hist = np.zeros((R, cap))
         n_it = np.zeros(R, dtype=np.int64)
         conv = np.zeros(R, dtype=np.int32)
         _lib.check(_lib.lib.ws_solver_solve_batch(
-            h, R, (C.c_int64 * R)(*counts), blocks, _lib.WS_HOST, C.byref(o), E.ctypes.data, _lib.WS_HOST,
+            h, R, (C.c_int64 * R)(*counts), blocks, _lib.WS_HOST, C.byref(o), buf.ctypes.data, _lib.WS_HOST,
             hist.ctypes.data_as(C.POINTER(C.c_double)), cap, n_it.ctypes.data_as(C.POINTER(C.c_int64)),
             conv.ctypes.data_as(C.POINTER(C.c_int))))
+        E = _lib.HostStage.take(buf, (R,) + shape[::-1])  # each field column-major
         del keep
-        dt = time.perf_counter() - t0
+        return self._batch_results(h, E, hist, n_it, conv, groups, time.perf_counter() - t0, init is not None,
+                                   lambda i: self.exec(sources[i]))
+
+    def _batch_results(self, h, E, hist, n_it, conv, srcs, dt, warm, rerun):
+        """Fields and states of a batched solve; with warm starts, the warm
+        report of each right-hand side, and a cold rerun (rerun(i) -> (E, st))
+        of each discarded start."""
+        R = len(srcs)
         outs, states = [], []
         for i in range(R):
             Ei = E[i].transpose(3, 2, 1, 0)  # [y, x, z, c], column-major in memory
             if not self.vector:
                 Ei = Ei[..., 0]
             outs.append(Ei)
-            states.append(SimpleNamespace(source=groups[i], it=int(n_it[i]) + 1, converged=bool(conv[i]),
+            states.append(SimpleNamespace(source=srcs[i], it=int(n_it[i]) + 1, converged=bool(conv[i]),
                                           diff_energy=hist[i, :n_it[i]].copy(), time=dt))
-        if init is not None:
+        if warm:
             for i in range(R):
-                cold, warm, disc = C.c_double(), C.c_double(), C.c_int()
-                _lib.check(_lib.lib.ws_solver_warm_report(h, i, C.byref(cold), C.byref(warm), C.byref(disc)))
-                states[i].cold_first_energy, states[i].warm_cycle_energy = cold.value, warm.value
+                cold, wc, disc = C.c_double(), C.c_double(), C.c_int()
+                _lib.check(_lib.lib.ws_solver_warm_report(h, i, C.byref(cold), C.byref(wc), C.byref(disc)))
+                states[i].cold_first_energy, states[i].warm_cycle_energy = cold.value, wc.value
                 states[i].warm_discarded = bool(disc.value)
                 rc_, rw_ = C.c_double(), C.c_double()
                 _lib.check(_lib.lib.ws_solver_warm_residual(h, i, C.byref(rc_), C.byref(rw_)))
                 states[i].cold_residual_energy, states[i].warm_residual_energy = rc_.value, rw_.value
             for i in range(R):
                 if states[i].warm_discarded:
-                    outs[i], st = self.exec(sources[i])
+                    outs[i], st = rerun(i)
                     st.warm_discarded, st.warm_iterations = True, states[i].it - 1
                     for k in ("cold_first_energy", "warm_cycle_energy", "cold_residual_energy",
                               "warm_residual_energy"):
@@ -509,11 +524,57 @@ class WaveSim:
         return outs, states
 
 
-    def _exec_plane_waves(self, waves, warm_starts, t0):
+    def _start_windows(self):
+        """initial_field's cos^2 tapers (y, x, z) over the boundary layers."""
+        if getattr(self, "_swin", None) is None:
+            shape = [int(v) for v in self.N]
+            r = self.roi
+            out = []
+            for d in range(3):
+                lo, hi = int(r[0, d]) - 1, shape[d] - int(r[1, d])
+                w = np.ones(shape[d], np.float32)
+                if lo:
+                    w[:lo] = np.cos(0.5 * np.pi * np.arange(lo, 0, -1) / (lo + 1)) ** 2
+                if hi:
+                    w[shape[d] - hi:] = np.cos(0.5 * np.pi * np.arange(1, hi + 1) / (hi + 1)) ** 2
+                out.append(w)
+            self._swin = out
+        return self._swin
+
+    def device_starts(self, fields):
+        """initial_field on the device: `fields` is a complex64 CUDA tensor of
+        R ROI fields (one row each, column-major as the C ABI writes them);
+        returns R full-grid starting fields (rows, column-major), each
+        continued into the boundary layers by its edge values under the cos^2
+        taper of initial_field."""
+        import torch
+        shape = [int(v) for v in self.N]
+        r = self.roi
+        rs = [int(r[1, d] - r[0, d] + 1) for d in range(4)]
+        lo = [int(r[0, d]) - 1 for d in range(4)]
+        R = fields.shape[0]
+        dev = fields.device
+        t = fields.reshape(R, rs[3], rs[2], rs[1], rs[0])  # [rhs, c, z, x, y]
+        win = self._start_windows()
+        for d, axis in ((0, 4), (1, 3), (2, 2)):
+            if rs[d] != shape[d]:
+                idx = (torch.arange(shape[d], device=dev) - lo[d]).clamp(0, rs[d] - 1)
+                t = t.index_select(axis, idx)
+            if (win[d] != 1).any():
+                sh = [1, 1, 1, 1, 1]
+                sh[axis] = shape[d]
+                t = t * torch.from_numpy(win[d]).to(dev).view(sh)
+        if rs[3] != shape[3]:
+            full = torch.zeros((R, shape[3]) + tuple(t.shape[2:]), dtype=t.dtype, device=dev)
+            full[:, lo[3]:lo[3] + rs[3]] = t
+            t = full
+        return t.reshape(R, -1).contiguous()
+
+    def _exec_plane_waves(self, waves, warm_starts, t0, keep_device=False):
         """exec_batch for PlaneWave sources: the blocks are generated on the
-        device (ws_solver_solve_plane_waves)."""
-        if warm_starts is not None:
-            raise ValueError("warm starts with plane-wave descriptors: use Source blocks")
+        device (ws_solver_solve_plane_waves).  warm_starts may also be a CUDA
+        tensor of full-grid starts (device_starts); keep_device=True also
+        returns the fields as a CUDA tensor (one row each, column-major)."""
         R = len(waves)
         arr = (_lib.ws_plane_wave * R)()
         for i, w in enumerate(waves):
@@ -526,26 +587,54 @@ class WaveSim:
                                         (C.c_double * 3)(*[float(a) for a in pw.phase]), pw.phase0)
         h = self.solver()
         o = self._options()
+        init = None
+        if warm_starts is not None:
+            if len(warm_starts) != R:
+                raise ValueError("one warm start per source")
+            if hasattr(warm_starts, "data_ptr"):
+                if warm_starts.numel() != R * int(np.prod(self.N)):
+                    raise ValueError("device warm starts must hold the full grid for each source")
+                init = warm_starts
+                o.initial_field = init.data_ptr()
+                o.initial_memory = _lib.WS_DEVICE
+            else:
+                init = np.stack([np.ravel(self.initial_field(w), order="F") for w in warm_starts])
+                o.initial_field = init.ctypes.data
+                o.initial_memory = _lib.WS_HOST
         r = self.roi
         shape = tuple(int(r[1, d] - r[0, d] + 1) for d in range(4))
-        E = np.empty((R,) + shape[::-1], dtype=np.complex64)
         cap = o.max_iterations + len(self.wiggles) + 1
         hist = np.zeros((R, cap))
         n_it = np.zeros(R, dtype=np.int64)
         conv = np.zeros(R, dtype=np.int32)
+        Edev = None
+        if keep_device:
+            import torch
+            Edev = torch.empty((R, int(np.prod(shape))), dtype=torch.complex64,
+                               device=torch.device("cuda", self.device))
+            out, mem = Edev.data_ptr(), _lib.WS_DEVICE
+        else:
+            buf = self._stage().get(R * np.prod(shape))
+            out, mem = buf.ctypes.data, _lib.WS_HOST
         _lib.check(_lib.lib.ws_solver_solve_plane_waves(
-            h, R, arr, C.byref(o), E.ctypes.data, _lib.WS_HOST, hist.ctypes.data_as(C.POINTER(C.c_double)), cap,
+            h, R, arr, C.byref(o), out, mem, hist.ctypes.data_as(C.POINTER(C.c_double)), cap,
             n_it.ctypes.data_as(C.POINTER(C.c_int64)), conv.ctypes.data_as(C.POINTER(C.c_int))))
-        dt = time.perf_counter() - t0
-        outs, states = [], []
-        for i in range(R):
-            Ei = E[i].transpose(3, 2, 1, 0)
-            if not self.vector:
-                Ei = Ei[..., 0]
-            outs.append(Ei)
-            states.append(SimpleNamespace(source=waves[i], it=int(n_it[i]) + 1, converged=bool(conv[i]),
-                                          diff_energy=hist[i, :n_it[i]].copy(), time=dt))
-        return outs, states
+        del init
+        if keep_device:
+            import torch
+            buf = self._stage().get(Edev.numel())
+            torch.from_numpy(buf).copy_(Edev.reshape(-1))
+        E = _lib.HostStage.take(buf, (R,) + shape[::-1])
+        outs, states = self._batch_results(
+            h, E, hist, n_it, conv, list(waves), time.perf_counter() - t0, warm_starts is not None,
+            lambda i: [x[0] for x in self._exec_plane_waves([waves[i]], None, time.perf_counter())])
+        if not keep_device:
+            return outs, states
+        for i, st in enumerate(states):
+            if getattr(st, "warm_discarded", False):  # the cold rerun's field replaces the discarded run's
+                import torch
+                Edev[i] = torch.from_numpy(np.ravel(np.asarray(outs[i], np.complex64), order="F")).to(Edev.device)
+        return outs, states, Edev
 
 
 class WaveSimVector(WaveSim):
