@@ -442,9 +442,11 @@ class WaveSim:
         Equivalent to ``[self.exec(s) for s in sources]`` - every source runs
         the reference loop and stop rule on its own - but all of them share the
         medium's device data and each kernel launch covers the whole batch.
-        warm_starts: None, or one starting field per source (host arrays on
-        the ROI or the full grid), see exec; a discarded start is rerun cold
-        on its own.  Returns (list of E, list of state)."""
+        warm_starts: None, one starting field per source (host arrays on the
+        ROI or the full grid, see exec), or a CUDA tensor of the R full-grid
+        starts as column-major rows (device_starts, WarmStart.predict_grid);
+        the discarded starts are rerun cold together in one batched solve.
+        Returns (list of E, list of state)."""
         t0 = time.perf_counter()
         if sources and all(isinstance(s, PlaneWave) for s in sources):
             return self._exec_plane_waves(sources, warm_starts, t0)
@@ -467,13 +469,7 @@ class WaveSim:
         h = self.solver()
         o = self._options()
         R = len(sources)
-        init = None
-        if warm_starts is not None:
-            if len(warm_starts) != R:
-                raise ValueError("one warm start per source")
-            init = np.stack([np.ravel(self.initial_field(w), order="F") for w in warm_starts])
-            o.initial_field = init.ctypes.data
-            o.initial_memory = _lib.WS_HOST
+        init = self._batch_starts(o, warm_starts, R)
         r = self.roi
         shape = tuple(int(r[1, d] - r[0, d] + 1) for d in range(4))
         buf = self._stage().get(R * np.prod(shape))
@@ -486,14 +482,35 @@ class WaveSim:
             hist.ctypes.data_as(C.POINTER(C.c_double)), cap, n_it.ctypes.data_as(C.POINTER(C.c_int64)),
             conv.ctypes.data_as(C.POINTER(C.c_int))))
         E = _lib.HostStage.take(buf, (R,) + shape[::-1])  # each field column-major
-        del keep
-        return self._batch_results(h, E, hist, n_it, conv, groups, time.perf_counter() - t0, init is not None,
-                                   lambda i: self.exec(sources[i]))
+        del keep, init
+        return self._batch_results(h, E, hist, n_it, conv, groups, time.perf_counter() - t0,
+                                   warm_starts is not None, lambda idx: self.exec_batch([sources[i] for i in idx]))
+
+    def _batch_starts(self, o, warm_starts, R):
+        """Sets the options' starting fields for a batch of R: host arrays
+        (one per source, on the ROI or the full grid; see initial_field), or a
+        CUDA tensor of R full-grid starts, column-major rows (device_starts,
+        WarmStart.predict_grid), passed without a host round trip.  Returns
+        what must stay alive during the solve."""
+        if warm_starts is None:
+            return None
+        if len(warm_starts) != R:
+            raise ValueError("one warm start per source")
+        if hasattr(warm_starts, "data_ptr"):
+            if warm_starts.numel() != R * int(np.prod(self.N)) or not warm_starts.is_contiguous():
+                raise ValueError("device warm starts must be R contiguous full-grid fields")
+            o.initial_field = warm_starts.data_ptr()
+            o.initial_memory = _lib.WS_DEVICE
+            return warm_starts
+        init = np.stack([np.ravel(self.initial_field(w), order="F") for w in warm_starts])
+        o.initial_field = init.ctypes.data
+        o.initial_memory = _lib.WS_HOST
+        return init
 
     def _batch_results(self, h, E, hist, n_it, conv, srcs, dt, warm, rerun):
         """Fields and states of a batched solve; with warm starts, the warm
-        report of each right-hand side, and a cold rerun (rerun(i) -> (E, st))
-        of each discarded start."""
+        report of each right-hand side, and one batched cold rerun
+        (rerun(indices) -> (fields, states)) of the discarded starts."""
         R = len(srcs)
         outs, states = [], []
         for i in range(R):
@@ -512,9 +529,11 @@ class WaveSim:
                 rc_, rw_ = C.c_double(), C.c_double()
                 _lib.check(_lib.lib.ws_solver_warm_residual(h, i, C.byref(rc_), C.byref(rw_)))
                 states[i].cold_residual_energy, states[i].warm_residual_energy = rc_.value, rw_.value
-            for i in range(R):
-                if states[i].warm_discarded:
-                    outs[i], st = rerun(i)
+            idx = [i for i in range(R) if states[i].warm_discarded]
+            if idx:
+                re_E, re_st = rerun(idx)
+                for i, e, st in zip(idx, re_E, re_st):
+                    outs[i] = e
                     st.warm_discarded, st.warm_iterations = True, states[i].it - 1
                     for k in ("cold_first_energy", "warm_cycle_energy", "cold_residual_energy",
                               "warm_residual_energy"):
@@ -587,20 +606,7 @@ class WaveSim:
                                         (C.c_double * 3)(*[float(a) for a in pw.phase]), pw.phase0)
         h = self.solver()
         o = self._options()
-        init = None
-        if warm_starts is not None:
-            if len(warm_starts) != R:
-                raise ValueError("one warm start per source")
-            if hasattr(warm_starts, "data_ptr"):
-                if warm_starts.numel() != R * int(np.prod(self.N)):
-                    raise ValueError("device warm starts must hold the full grid for each source")
-                init = warm_starts
-                o.initial_field = init.data_ptr()
-                o.initial_memory = _lib.WS_DEVICE
-            else:
-                init = np.stack([np.ravel(self.initial_field(w), order="F") for w in warm_starts])
-                o.initial_field = init.ctypes.data
-                o.initial_memory = _lib.WS_HOST
+        init = self._batch_starts(o, warm_starts, R)
         r = self.roi
         shape = tuple(int(r[1, d] - r[0, d] + 1) for d in range(4))
         cap = o.max_iterations + len(self.wiggles) + 1
@@ -627,7 +633,7 @@ class WaveSim:
         E = _lib.HostStage.take(buf, (R,) + shape[::-1])
         outs, states = self._batch_results(
             h, E, hist, n_it, conv, list(waves), time.perf_counter() - t0, warm_starts is not None,
-            lambda i: [x[0] for x in self._exec_plane_waves([waves[i]], None, time.perf_counter())])
+            lambda idx: self._exec_plane_waves([waves[i] for i in idx], None, time.perf_counter()))
         if not keep_device:
             return outs, states
         for i, st in enumerate(states):
