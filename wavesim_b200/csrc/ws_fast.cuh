@@ -428,6 +428,7 @@ __global__ void __launch_bounds__(kThreads, 3)
 template <int NO, int TY>
 __global__ void __launch_bounds__(TY*(NO / 16) < 1024 ? TY*(NO / 16) : 1024, 3)
     kf_pencil(OuterArgs a, float2* __restrict__ T, const DevState* __restrict__ st) {
+  pdl_begin();
   constexpr int P = NO / 16;
   constexpr int TYS = TY + 1;
   const int rhs = blockIdx.x / a.bpr, bid = blockIdx.x - rhs * a.bpr;
@@ -1112,6 +1113,7 @@ __global__ void __launch_bounds__(kThreads, 2)
     kc_col_step(InnerArgs a, Wig w1, const float2* __restrict__ src1, float2 A, float2* __restrict__ T,
                 float2* __restrict__ dE, float2* __restrict__ E, const float2* __restrict__ gamma,
                 const DevState* __restrict__ st, double* __restrict__ partials) {
+  pdl_begin();
   using G = PlaneGeom<N, C, true>;
   constexpr int P = G::P, LPR = G::LPR, M = G::M;
   static_assert(M % LPR == 0, "whole rounds of lines");
@@ -1253,6 +1255,7 @@ __global__ void __launch_bounds__(kThreads, 2)
     kc_col_step2d(InnerArgs a, Wig w1, const float2* __restrict__ src1, float2 A, float2* __restrict__ T,
                   float2* __restrict__ dE, float2* __restrict__ E, const float2* __restrict__ gamma,
                   const DevState* __restrict__ st, double* __restrict__ partials) {
+  pdl_begin();
   using G = PlaneGeom<N, 1, false>;
   constexpr int P = G::P, LPR = G::LPR;
   const int rhs = blockIdx.x / a.bpr, bid = blockIdx.x - rhs * a.bpr;

@@ -121,6 +121,16 @@ struct OuterArgs {
 
 __device__ __forceinline__ int load_done(const DevState* st) { return __ldcg(&st->done); }
 
+// Programmatic dependent launch: the loop's kernels are launched so that the
+// next one may be scheduled while this one runs; each waits here, before it
+// touches global memory, until the kernel before it has completed and its
+// writes are visible (a no-op when launched without the attribute), then lets
+// the kernel after it be scheduled.
+__device__ __forceinline__ void pdl_begin() {
+  asm volatile("griddepcontrol.wait;" ::: "memory");
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
+
 // One radix-C step across the cluster (C = a.csize > 1), in place on the
 // shared tile.  Forward: out[x'] = sum_c u_c[x'] W_Nx^{rank (x' + c M)};
 // inverse: out[x'] = sum_c u_c[x'] conj(W_Nx^{c (x' + rank M)}), M = Nx / C.
@@ -433,6 +443,7 @@ __global__ void __launch_bounds__(512, 1) k_inv_inner(InnerArgs a, const float2*
 // Simulation.next (Simulation.m:193-217).  One block.
 static __global__ void __launch_bounds__(256) k_finish_iteration(DevState* st, StopRule rule, Hist h,
                                                           const double* __restrict__ partials, int nparts) {
+  pdl_begin();
   const int rhs = blockIdx.x;  // one block per right-hand side
   st += rhs;
   partials += (long long)rhs * nparts;

@@ -235,6 +235,7 @@ __global__ void __launch_bounds__(kThreads, 3)
 template <class PL, int TY, int NC, bool D3 = true>
 __global__ void __launch_bounds__(TY* PL::P, NC == 1 ? 2 : 1)
     km_pencil(OuterArgs a, float2* __restrict__ T, const DevState* __restrict__ st) {
+  pdl_begin();
   constexpr int E = PL::E, P = PL::P, TYS = TY + 1;
   const int rhs = blockIdx.x / a.bpr, bid = blockIdx.x - rhs * a.bpr;
   st += rhs;
@@ -791,6 +792,7 @@ __global__ void __launch_bounds__(kThreads, 2)
     kmc_col_step(InnerArgs a, Wig w1, const float2* __restrict__ src1, float2 A, float2* __restrict__ T,
                  float2* __restrict__ dE, float2* __restrict__ E, const float2* __restrict__ gamma,
                  const DevState* __restrict__ st, double* __restrict__ partials) {
+  pdl_begin();
   using G = MGeom<PL, C>;
   constexpr int N = PL::N, EL = PL::E, P = PL::P, M = G::M, LPR = G::LPR;
   // blocks in reverse order: the pass starts on the planes the inverse x
@@ -1081,6 +1083,7 @@ template <class PL>
 __global__ void __launch_bounds__(kThreads, 2)
     kmc_col_fwd2d(InnerArgs a, const float2* __restrict__ dE, const float2* __restrict__ src, float2 A,
                   float2* __restrict__ T, const DevState* __restrict__ st) {
+  pdl_begin();
   col2d<PL, kCol2dFwd>(a, a.w, dE, src, A, T, nullptr, nullptr, nullptr, st, nullptr);
 }
 
@@ -1088,6 +1091,7 @@ template <class PL>
 __global__ void __launch_bounds__(kThreads, 2)
     kmc_col_inv2d(InnerArgs a, const float2* __restrict__ T, float2* __restrict__ dE, float2* __restrict__ E,
                   const float2* __restrict__ gamma, const DevState* __restrict__ st, double* __restrict__ partials) {
+  pdl_begin();
   col2d<PL, kCol2dInv>(a, a.w, nullptr, nullptr, make_float2(0.f, 0.f), const_cast<float2*>(T), dE, E, gamma,
                        st, partials);
 }
@@ -1097,6 +1101,7 @@ __global__ void __launch_bounds__(kThreads, 2)
     kmc_col_step2d(InnerArgs a, Wig w1, const float2* __restrict__ src1, float2 A, float2* __restrict__ T,
                    float2* __restrict__ dE, float2* __restrict__ E, const float2* __restrict__ gamma,
                    const DevState* __restrict__ st, double* __restrict__ partials) {
+  pdl_begin();
   col2d<PL, kCol2dStep>(a, w1, nullptr, src1, A, T, dE, E, gamma, st, partials);
 }
 

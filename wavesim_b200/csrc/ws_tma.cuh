@@ -96,6 +96,7 @@ template <int NO, int TY, int S>
 __global__ void __launch_bounds__(PencilTile<NO, TY, S>::kThreads, PencilTile<NO, TY, S>::kMinBlocks)
     kt_pencil(const __grid_constant__ CUtensorMap tmap, OuterArgs a, const DevState* __restrict__ st, int ntiles,
               int* __restrict__ err) {
+  pdl_begin();
   using PT = PencilTile<NO, TY, S>;
   constexpr int P = PT::P;
   extern __shared__ uint8_t smem_raw[];
@@ -224,6 +225,7 @@ template <int NO, int TY, int S, bool INV>
 __global__ void __launch_bounds__(PencilTile<NO, TY, S>::kThreads, PencilTile<NO, TY, S>::kMinBlocks)
     kt_xpencil(const __grid_constant__ CUtensorMap tmap, Geom g, const float2* __restrict__ twx,
                const DevState* __restrict__ st, int ntiles, long long wait_clocks, int* __restrict__ err) {
+  pdl_begin();
   using PT = PencilTile<NO, TY, S>;
   constexpr int P = PT::P;
   extern __shared__ uint8_t smem_raw[];
@@ -323,6 +325,7 @@ template <class PL, int TY, int S, bool INV>
 __global__ void __launch_bounds__(MixedXTile<PL, TY, S>::kThreads, 2)
     kt_xpencil_m(const __grid_constant__ CUtensorMap tmap, Geom g, const float2* __restrict__ twx,
                  const DevState* __restrict__ st, int ntiles, long long wait_clocks, int* __restrict__ err) {
+  pdl_begin();
   using PT = MixedXTile<PL, TY, S>;
   constexpr int NO = PT::NO, P = PT::P, E = PT::E;
   extern __shared__ uint8_t smem_raw[];
@@ -428,6 +431,7 @@ template <class PL, int TY, int S>
 __global__ void __launch_bounds__(VecPencilTile<PL, TY, S>::kThreads, VecPencilTile<PL, TY, S>::kMinBlocks)
     kt_pencil_vec(const __grid_constant__ CUtensorMap tmap, OuterArgs a, const DevState* __restrict__ st, int ntiles,
                   int* __restrict__ err) {
+  pdl_begin();
   using PT = VecPencilTile<PL, TY, S>;
   constexpr int NO = PT::NO, P = PT::P, E = PT::E;
   extern __shared__ uint8_t smem_raw[];
