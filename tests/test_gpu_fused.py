@@ -132,3 +132,27 @@ def test_fused_warm_and_batched(gpu):
     for a, b in zip(Ebf, Ebu):
         np.testing.assert_array_equal(a, b)
     assert [s.it for s in sbf] == [s.it for s in sbu]
+
+
+@pytest.mark.parametrize("name", ["256_split", "192_split", "2d_1024", "2d_320"])
+def test_programmatic_launch_is_bit_identical(gpu, name):
+    """WAVESIM_B200_PDL=1 (the loop's kernels launched with programmatic
+    dependent launch, each waiting for the one before it) gives the same
+    fields as plain stream order."""
+    shape, bw, env = CASES[name]
+    n = medium(shape)
+    opt = {"lambda": 1.0, "pixel_size": 0.25, "boundary_widths": bw, "energy_threshold": 1e-3, "max_iterations": 48}
+    val = np.ones(shape[:2]) + 0.3j
+    pos = [1] * len(shape)
+
+    def run(ws):
+        sim = ws.WaveSim(n, opt)
+        E, st = sim.exec(ws.Source(val, pos))
+        sim.close()
+        return E, st
+
+    Ep, sp = solve(True, run, dict(env or {}, WAVESIM_B200_PDL="1"))
+    Eq, sq = solve(True, run, dict(env or {}, WAVESIM_B200_PDL="0"))
+    assert sp.it == sq.it
+    np.testing.assert_array_equal(sp.diff_energy, sq.diff_energy)
+    np.testing.assert_array_equal(Ep, Eq)
