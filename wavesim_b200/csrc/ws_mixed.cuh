@@ -30,6 +30,30 @@ namespace mixed {
 
 constexpr int kThreads = 256;
 
+// Column lines of the column passes (kmc_col_step, the 2-D kernels): element
+// i of a line at i + (i >> SH), lines CS elements apart.  The shift and
+// stride minimise the shared-memory wavefronts of the lines' exchanges (a
+// host model of every stage's accesses, half-warp by half-warp, 8-byte
+// banks): 224 points 2496 against 3968 with the planes' (i >> 4, N + N/16 + 1),
+// 160: 1824 against 3520, 96: 1024 against 1792, 192: 1152 against 1344,
+// 576: 3456 against 4032; the others keep the planes' layout.
+template <int N>
+struct ColPad {
+  static constexpr int SH = 4, CS = N + N / 16 + 1;
+};
+template <> struct ColPad<96> { static constexpr int SH = 5, CS = 104; };
+template <> struct ColPad<160> { static constexpr int SH = 5, CS = 168; };
+template <> struct ColPad<192> { static constexpr int SH = 5, CS = 197; };
+template <> struct ColPad<224> { static constexpr int SH = 5, CS = 232; };
+template <> struct ColPad<576> { static constexpr int SH = 5, CS = 593; };
+
+template <int N>
+struct ColLineP {
+  float2* base;
+  static_assert(ColPad<N>::CS >= (N - 1) + ((N - 1) >> ColPad<N>::SH) + 1, "a line fits its stride");
+  __device__ __forceinline__ float2& at(int i) const { return base[i + (i >> ColPad<N>::SH)]; }
+};
+
 // The epilogues issue their loads (gamma, dE', E') in NH groups of H = E / NH
 // elements: halves up to 12 elements per thread, quarters beyond, so that
 // fewer loads are in flight in registers at once.
@@ -784,7 +808,7 @@ __global__ void __launch_bounds__(kThreads, 2)
 // lines, then the 2 N ramps; smem_col_step bytes).
 template <class PL, int C>
 constexpr size_t smem_col_step() {
-  return sizeof(float2) * ((size_t)MGeom<PL, C>::LPR * MGeom<PL, C>::CS + 2 * PL::N);
+  return sizeof(float2) * ((size_t)MGeom<PL, C>::LPR * ColPad<PL::N>::CS + 2 * PL::N);
 }
 
 template <class PL, int C>
@@ -811,7 +835,7 @@ __global__ void __launch_bounds__(kThreads, 2)
   gamma += rhs * a.gstride;  // a batch of media: each right-hand side has its own gamma
   extern __shared__ float2 smc[];
   float2* const sm = smc;
-  float2* const sgy = smc + LPR * G::CS;
+  float2* const sgy = smc + LPR * ColPad<N>::CS;
   __shared__ float red[kThreads / 32];
   const int tid = threadIdx.x;
   const Geom& g = a.g;
@@ -843,7 +867,7 @@ __global__ void __launch_bounds__(kThreads, 2)
     const int x = x0 + cc;
     const long long gcol = (colbase + cc) * N;
     float2* __restrict__ Tc = T + gcol;
-    fast::ColLine L{sm + cl * G::CS};
+    ColLineP<N> L{sm + cl * ColPad<N>::CS};
     float2 v[EL];
 #pragma unroll
     for (int r = 0; r < EL; ++r) v[r] = Tc[p + P * r];
@@ -919,7 +943,7 @@ __global__ void __launch_bounds__(kThreads, 2)
 template <class PL>
 struct MGeom2d {
   static constexpr int N = PL::N, P = PL::P;
-  static constexpr int CS = N + N / 16 + 1;
+  static constexpr int CS = ColPad<N>::CS;
   static constexpr int LPR = kThreads / P;
   static_assert(kThreads % P == 0 && (P <= 32 ? 32 % P == 0 : true), "threads per line");
 };
@@ -979,7 +1003,7 @@ __device__ __forceinline__ void col2d(const InnerArgs& a, const Wig& w1, const f
     const bool live = cc < ncol;
     const long long col = colbase + cc;
     const long long gcol = col * N;
-    fast::ColLine L{smx + (live ? cl : LPR) * G::CS};
+    ColLineP<N> L{smx + (live ? cl : LPR) * G::CS};
     float2 v[EL];
     if constexpr (MODE == kCol2dFwd) {
       if (live) {
