@@ -74,3 +74,22 @@ def test_device_starts_equal_initial_field():
         rows = torch.from_numpy(np.stack([np.ravel(f, order="F") for f in (roi, 2 * roi)]))
         got = sim.device_starts(rows).numpy()
         np.testing.assert_allclose(got, want, rtol=1e-6, atol=1e-7)
+
+
+def test_host_stage_take():
+    """The output staging buffer: take() gives a new array in the requested
+    order with the buffer's values, also through its chunked threaded copy."""
+    from wavesim_b200._lib import HostStage
+    st = HostStage()
+    for shape in ((3, 4, 5), (256, 128, 9)):  # the second is above the 4 MB of the chunked copy
+        n = int(np.prod(shape))
+        buf = st.get(n)
+        buf[:] = (np.arange(n) + 1j * np.arange(n)[::-1]).astype(np.complex64)
+        f = HostStage.take(buf, shape, "F")
+        c = HostStage.take(buf, shape)
+        assert f.flags.f_contiguous and c.flags.c_contiguous
+        np.testing.assert_array_equal(np.ravel(f, order="F"), buf)
+        np.testing.assert_array_equal(np.ravel(c), buf)
+        buf[:] = 0  # the results are copies
+        assert np.ravel(c)[1] != 0
+    assert st.get(10).size == 10
