@@ -231,6 +231,7 @@ class HostStage:
         return self._a[:count]
 
     _pool = None
+    _pool_lock = __import__("threading").Lock()
 
     @classmethod
     def take(cls, buf, shape, order="C"):
@@ -242,9 +243,10 @@ class HostStage:
         out = np.empty(buf.size, np.complex64)
         n = buf.size
         if buf.nbytes > (4 << 20):
-            if cls._pool is None:
-                from concurrent.futures import ThreadPoolExecutor
-                cls._pool = ThreadPoolExecutor(max_workers=max(1, min(8, os.cpu_count() or 1)))
+            with cls._pool_lock:  # solvers on several host threads share one pool
+                if cls._pool is None:
+                    from concurrent.futures import ThreadPoolExecutor
+                    cls._pool = ThreadPoolExecutor(max_workers=max(1, min(8, os.cpu_count() or 1)))
             k = cls._pool._max_workers
             step = -(-n // k)
 
