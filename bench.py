@@ -324,7 +324,7 @@ def run_ours(args):
     # and the stop-rule kernel per iteration, the cycle guard per wiggle
     # cycle, state reset, source scatter, finalize
     per_it = _lib.lib.ws_solver_launches_per_iteration(h)
-    fused = per_it != 4
+    fused = _lib.lib.ws_solver_fused(h) == 1
     launches_per_solve = (per_it * n_iter + (n_iter // len(sim.wiggles)) + 1 + len(s.values) + 1
                           + (1 if fused else 0))
 

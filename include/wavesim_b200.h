@@ -262,6 +262,12 @@ int ws_solver_set_wait_limit(ws_solver s, int64_t clocks);
 /* Number of kernel launches one iteration makes. */
 int ws_solver_launches_per_iteration(ws_solver s);
 
+/* 1 if the solver's loop fuses K3 of an iteration with K1 of the next (the
+ * one-kernel step on a cluster, the split step of 3-D planes, the column
+ * pass of 2-D grids), 0 if it runs K1, K2 and K3 as separate kernels.  No
+ * counterpart in the reference. */
+int ws_solver_fused(ws_solver s);
+
 /* Where the loop fuses K3 of an iteration with K1 of the next (3-D fast
  * planes on a cluster), the mean CUDA-event time of that kernel and its
  * algorithmic bytes per launch (K3's plus the write of T); otherwise

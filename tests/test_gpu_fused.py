@@ -96,7 +96,7 @@ def test_fused_loop_is_bit_identical(gpu, name, use_graph):
     def run(ws):
         sim = (ws.WaveSimVector if vector else ws.WaveSim)(n, opt)
         from wavesim_b200 import _lib
-        fused = _lib.lib.ws_solver_launches_per_iteration(sim.solver()) != 4
+        fused = _lib.lib.ws_solver_fused(sim.solver()) == 1
         E, st = sim.exec(ws.Source(val, pos))
         sim.close()
         return E, st, fused
@@ -135,10 +135,12 @@ def test_fused_warm_and_batched(gpu):
 
 
 @pytest.mark.parametrize("name", ["256_split", "192_split", "2d_1024", "2d_320"])
-def test_programmatic_launch_is_bit_identical(gpu, name):
+@pytest.mark.parametrize("var", ["WAVESIM_B200_PDL", "WAVESIM_B200_FIN"])
+def test_loop_variants_are_bit_identical(gpu, name, var):
     """WAVESIM_B200_PDL=1 (the loop's kernels launched with programmatic
-    dependent launch, each waiting for the one before it) gives the same
-    fields as plain stream order."""
+    dependent launch, each waiting for the one before it) and
+    WAVESIM_B200_FIN=1 (the column pass's last block runs the stop rule, no
+    k_finish_iteration) give the same fields and histories as the default."""
     shape, bw, env = CASES[name]
     n = medium(shape)
     opt = {"lambda": 1.0, "pixel_size": 0.25, "boundary_widths": bw, "energy_threshold": 1e-3, "max_iterations": 48}
@@ -151,8 +153,8 @@ def test_programmatic_launch_is_bit_identical(gpu, name):
         sim.close()
         return E, st
 
-    Ep, sp = solve(True, run, dict(env or {}, WAVESIM_B200_PDL="1"))
-    Eq, sq = solve(True, run, dict(env or {}, WAVESIM_B200_PDL="0"))
+    Ep, sp = solve(True, run, dict(env or {}, **{var: "1"}))
+    Eq, sq = solve(True, run, dict(env or {}, **{var: "0"}))
     assert sp.it == sq.it
     np.testing.assert_array_equal(sp.diff_energy, sq.diff_energy)
     np.testing.assert_array_equal(Ep, Eq)

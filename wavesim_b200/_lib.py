@@ -70,7 +70,7 @@ EXPORTS = [
     "ws_run_algorithm_release",
     "ws_solver_create", "ws_solver_create_media", "ws_solver_solve", "ws_solver_solve_batch", "ws_solver_solve_plane_waves", "ws_solver_buffers",
     "ws_solver_time_kernels", "ws_solver_time_split",
-    "ws_solver_launches_per_iteration", "ws_solver_set_wait_limit", "ws_solver_time_fused", "ws_solver_warm_report", "ws_solver_warm_residual", "ws_solver_autotune", "ws_solver_get_layout", "ws_solver_set_layout", "ws_solver_destroy",
+    "ws_solver_launches_per_iteration", "ws_solver_fused", "ws_solver_set_wait_limit", "ws_solver_time_fused", "ws_solver_warm_report", "ws_solver_warm_residual", "ws_solver_autotune", "ws_solver_get_layout", "ws_solver_set_layout", "ws_solver_destroy",
     "ws_run_algorithm_noalloc", "ws_medium_reduce", "ws_build_gamma", "ws_setup_last_error",
     "ws_noalloc_scratch_bytes", "ws_noalloc_last_error",
     "ws_pstd_default_options", "ws_pstd_create", "ws_pstd_run", "ws_pstd_destroy",
@@ -134,6 +134,8 @@ def _load():
     lib.ws_solver_set_wait_limit.restype = C.c_int
     lib.ws_solver_launches_per_iteration.argtypes = [P]
     lib.ws_solver_launches_per_iteration.restype = C.c_int
+    lib.ws_solver_fused.argtypes = [P]
+    lib.ws_solver_fused.restype = C.c_int
     lib.ws_solver_time_fused.argtypes = [P, C.c_int, C.POINTER(C.c_float), C.POINTER(C.c_double)]
     lib.ws_solver_time_split.argtypes = [P, C.c_int, C.POINTER(C.c_float), C.POINTER(C.c_double)]
     lib.ws_solver_time_split.restype = C.c_int

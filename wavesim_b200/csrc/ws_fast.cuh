@@ -1236,6 +1236,7 @@ __global__ void __launch_bounds__(kThreads, 2)
     for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
     if (tid == 0) partials[bid] = (double)v;
   }
+  if (a.fin) finish_in_last_block(const_cast<DevState*>(st), a.rule, a.hist, partials, a.bpr, rhs);
 }
 
 // The 2-D form: K2 already transforms along x, so K3 of iteration k and K1
@@ -1366,6 +1367,7 @@ __global__ void __launch_bounds__(kThreads, 2)
     for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
     if (tid == 0) partials[bid] = (double)v;
   }
+  if (a.fin) finish_in_last_block(const_cast<DevState*>(st), a.rule, a.hist, partials, a.bpr, rhs);
 }
 
 // The same fused step with K1's half of the plane exchange pushed: each block

@@ -100,6 +100,9 @@ struct InnerArgs {
   int acc2;     // K3: E' += dE' in pairs, every second iteration (Nw even; 0: every iteration)
   int* err;     // fast kernels: set to 1 when a cluster exchange wait gives up (may be null)
   long long gstride;  // elements between the gammas of consecutive right-hand sides (0: one shared gamma)
+  int fin;            // column passes: the last block of a right-hand side runs the stop rule
+  StopRule rule;      //   (finish_in_last_block) with this rule and history
+  Hist hist;
 };
 
 struct OuterArgs {
@@ -339,6 +342,40 @@ __device__ __forceinline__ void finish_iteration(DevState* st, const StopRule& r
   st->calc_energy = ((it - 1) % rule.interval) == 0;
   st->it = it + 1;
   st->blocks_done = 0;
+}
+
+// The stop rule of an iteration run by the last block (of 256 threads) of
+// the pass that wrote the iteration's energy partials, instead of a separate
+// k_finish_iteration launch: each block counts itself in st->blocks_done
+// after its partial is visible; the block that completes the count (all
+// others have then finished, and read st->it before it changes) sums the
+// partials in k_finish_iteration's order (thread i takes i, i + 256, ...,
+// then the same tree) and runs finish_iteration, which clears the count.
+// st and partials are those of the block's right-hand side.
+__device__ __forceinline__ void finish_in_last_block(DevState* st, const StopRule& rule, Hist h,
+                                                    const double* partials, int nparts, int rhs) {
+  __shared__ unsigned s_last;
+  __shared__ double red[256];
+  __threadfence();
+  __syncthreads();
+  if (threadIdx.x == 0) s_last = atomicAdd(&st->blocks_done, 1u) == (unsigned)(nparts - 1) ? 1u : 0u;
+  __syncthreads();
+  if (!s_last) return;
+  __threadfence();
+  h.diff += rhs * h.stride;
+  if (h.fresh) h.fresh += rhs * h.stride;
+  double acc = 0.0;
+  for (int i = threadIdx.x; i < nparts; i += blockDim.x) acc += __ldcg(&partials[i]);
+  red[threadIdx.x] = acc;
+  __syncthreads();
+  for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+    if ((int)threadIdx.x < o) red[threadIdx.x] += red[threadIdx.x + o];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    st->e_acc = red[0];
+    finish_iteration(st, rule, h);
+  }
 }
 
 // K3 -------------------------------------------------------------------------

@@ -530,6 +530,9 @@ struct Solver {
   LayoutChoice tuned{};          // the autotuner's choice (all zero: the heuristics)
   double warm_ratio = 0.0;       // discard threshold of the current solve
   long long wait_clocks = 0;     // bound of the TMA pencils' tile waits (0: the default)
+  int fin_fuse = 0;              // WAVESIM_B200_FIN=1: the column pass's last block runs the stop rule instead
+                                 // of k_finish_iteration (measured: 256^3 46.05 against 45.63 ms, 1024^2
+                                 // 8.83 against 8.74 ms, 320^2 5.52 against 5.40 ms; off)
   int pdl = 0;                   // WAVESIM_B200_PDL=1: launch the loop's kernels with programmatic
                                  // dependent launch (measured: 256^3 solve 46.3 against 44.3 ms,
                                  // 96^3 3.38 against 2.80 ms, 1024^2 8.50 against 8.71 ms; off)
@@ -756,6 +759,7 @@ static int create_solver(const int64_t N[4], const ws_complex* gamma, int64_t n_
     s->pf_outer = per_sm * kNumSms;
     if (const char* e = std::getenv("WAVESIM_B200_FUSED_TMA")) s->fused_tma = std::atoi(e) ? 1 : 0;
     if (const char* e = std::getenv("WAVESIM_B200_PDL")) s->pdl = std::atoi(e) ? 1 : 0;
+    if (const char* e = std::getenv("WAVESIM_B200_FIN")) s->fin_fuse = std::atoi(e) ? 1 : 0;
   }
 #define WS_TRY(call)                 \
   do {                               \
@@ -1228,9 +1232,17 @@ static cudaError_t launch_xpencil(const Solver* cs, bool inv) {
 
 // The column pass of the split fused step (kc_col_step): the columns of every
 // plane kernel block, no cluster.
-static cudaError_t launch_colstep(const Solver* s, int w, int w1, bool src_next) {
+// With rule and h, the pass's last block per right-hand side also runs the
+// stop rule (finish_in_last_block), in place of k_finish_iteration.
+static cudaError_t launch_colstep(const Solver* s, int w, int w1, bool src_next, const StopRule* rule = nullptr,
+                                  const Hist* h = nullptr) {
   InnerArgs a = inner_args(s, w);
   a.ncols = s->lay.ncols;
+  if (rule && h) {
+    a.fin = 1;
+    a.rule = *rule;
+    a.hist = *h;
+  }
   Wig W1 = s->wig[w1];
   const float2* src1 = src_next ? s->d_src : nullptr;
   float2 A = make_float2(0.f, (float)(1.0f / s->eps / (float)s->nw));
@@ -1247,14 +1259,19 @@ static cudaError_t launch_colstep(const Solver* s, int w, int w1, bool src_next)
 
 // K3 of an iteration and K1 of the next: one kernel on a cluster, or the
 // split step (inverse x pencils, column pass, forward x pencils).
-static cudaError_t launch_step(const Solver* s, int w, int w1, bool src_next) {
-  if (!s->lay.mode3d) return launch_colstep(s, w, w1, src_next);  // 2-D: K2 already transformed along x
+static cudaError_t launch_step(const Solver* s, int w, int w1, bool src_next, const StopRule* rule = nullptr,
+                               const Hist* h = nullptr) {
+  if (!s->lay.mode3d) return launch_colstep(s, w, w1, src_next, rule, h);  // 2-D: K2 already transformed along x
   if (!s->lay.xp) return launch_k3k1(s, w, w1, src_next);
   cudaError_t e = launch_xpencil(s, true);
   if (e != cudaSuccess) return e;
-  if ((e = launch_colstep(s, w, w1, src_next)) != cudaSuccess) return e;
+  if ((e = launch_colstep(s, w, w1, src_next, rule, h)) != cudaSuccess) return e;
   return launch_xpencil(s, false);
 }
+
+// Whether the loop's column pass runs the stop rule itself (2-D, or the
+// split step of 3-D planes; WAVESIM_B200_FIN=1).
+static bool finish_in_step(const Solver* s) { return s->fin_fuse && (!s->lay.mode3d || s->lay.xp); }
 
 // One iteration of the fused loop: T already holds K1's output for it.
 static cudaError_t launch_iteration_fused(const Solver* s, int i, bool src_next, const StopRule& rule,
@@ -1262,6 +1279,7 @@ static cudaError_t launch_iteration_fused(const Solver* s, int i, bool src_next,
   const int w = i % s->nw, w1 = (i + 1) % s->nw;
   cudaError_t e = launch_k2(s, w);
   if (e != cudaSuccess) return e;
+  if (finish_in_step(s)) return launch_step(s, w, w1, src_next, &rule, &h);
   if ((e = launch_step(s, w, w1, src_next)) != cudaSuccess) return e;
   return launch_finish(s, rule, h);
 }
@@ -1817,7 +1835,15 @@ int ws_solver_launches_per_iteration(ws_solver h) {
   if (!h) return 0;
   const Solver* s = reinterpret_cast<Solver*>(h);
   // K2, K3 + next K1 (one kernel, or the split step's three), stop rule; or K1, K2, K3, stop rule
-  return s->fuse ? (s->lay.xp ? 5 : 3) : 4;
+  if (!s->fuse) return 4;                                   // K1, K2, K3, the stop rule
+  if (s->lay.mode3d && !s->lay.xp) return 3;                // K2, K3K1 on a cluster, the stop rule
+  const int step = s->lay.mode3d ? 4 : 2;                   // K2 (+ x pencils), the column pass (+ x pencils)
+  return finish_in_step(s) ? step : step + 1;
+}
+
+int ws_solver_fused(ws_solver h) {
+  if (!h) return 0;
+  return reinterpret_cast<Solver*>(h)->fuse ? 1 : 0;
 }
 
 int ws_solver_time_fused(ws_solver h, int n_iterations, float* ms_out, double* bytes_out) {

@@ -926,6 +926,7 @@ __global__ void __launch_bounds__(kThreads, 2)
     for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
     if (tid == 0) partials[bid] = (double)v;
   }
+  if (a.fin) finish_in_last_block(const_cast<DevState*>(st), a.rule, a.hist, partials, a.bpr, rhs);
 }
 
 // 2-D grids on the mixed-radix lines: the y transforms of whole columns, as
@@ -1100,6 +1101,8 @@ __device__ __forceinline__ void col2d(const InnerArgs& a, const Wig& w1, const f
       for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
       if (tid == 0) partials[bid] = (double)v;
     }
+    if (MODE == kCol2dStep && a.fin)
+      finish_in_last_block(const_cast<DevState*>(st), a.rule, a.hist, partials, a.bpr, rhs);
   }
 }
 
