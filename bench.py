@@ -384,6 +384,7 @@ def run_ours(args):
     if ws == 1 and args.config == "c3":
         if args.batch > 0:
             legs["batched"] = run_batched(args, sim, h, stream, torch, dev, value)
+            legs["sweep_256"] = run_sweep_256(args, sim, spec, torch, value)
         if not args.no_warm:
             legs["warm_start"] = run_warm(args, sim, h, s, blocks, opts, torch, dev, E_dev, value)
             if args.batch > 0:
@@ -541,6 +542,53 @@ def _tilt(sim, angle_deg, n_bg=1.33):
     k = 2 * np.pi / sim.lambda_ * n_bg * float(sim.options["pixel_size"])
     ph = np.exp(1j * k * np.sin(np.radians(angle_deg)) * np.arange(nx))
     return np.broadcast_to(ph[None, :, None], (ny, nx, nz)), ph
+
+
+def run_sweep_256(args, sim, spec, torch, plain_ms):
+    """The continuation start on the 256^3 medium: 16 plane waves on the z = 1
+    face at incidence angles 0.5 degrees apart (exp(i k n_bg sin(theta) x),
+    n_bg 1.33), solved by wavesim_b200.batch.solve_sweep in rounds of 2
+    (round 0 cold, every later angle started from its neighbour's field
+    tilted on the device) against the same rounds solved cold; both through
+    the Python API with the fields copied to the host.  Accuracy of one
+    continued field and its cold counterpart against a tight solve
+    (threshold 1e-7)."""
+    import wavesim_b200 as ws
+    from wavesim_b200.batch import solve_sweep
+    r = sim.roi
+    ny, nx = int(r[1, 0] - r[0, 0] + 1), int(r[1, 1] - r[0, 1] + 1)
+    k = 2 * np.pi / sim.lambda_ * 1.33 * float(sim.options["pixel_size"])
+    angles = -3.75 + 0.5 * np.arange(16)
+    waves = [ws.PlaneWave((ny, nx, 1), [1, 1, 1], phase=(0.0, k * np.sin(np.radians(a)), 0.0)) for a in angles]
+    B = 2
+    rounds = -(-len(waves) // B)
+    solve_sweep(sim, waves[:2 * B], batch=B)  # warm-up: graphs, staging
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    Ec, sc = [None] * len(waves), [None] * len(waves)
+    for j in range(rounds):
+        E, st = sim.exec_batch(waves[j::rounds])
+        for i, e, s_ in zip(range(j, len(waves), rounds), E, st):
+            Ec[i], sc[i] = e, s_
+    torch.cuda.synchronize()
+    t_cold = time.perf_counter() - t0
+    Ew, sw, t_w = solve_sweep(sim, waves, batch=B)
+    torch.cuda.synchronize()
+    i = len(waves) // 2 + 1
+    tight = ws.WaveSim(spec[0], dict(spec[1], device_setup=True, energy_threshold=1e-7))
+    Et, _ = tight.exec_batch([waves[i]])
+    tight.close()
+    ref = Et[0]
+    nr = float(np.linalg.norm(ref))
+    n = len(waves)
+    return {"angles_deg": [float(a) for a in angles], "batch": B, "rounds": rounds,
+            "ms_per_solve": t_w * 1e3 / n, "ms_per_solve_same_rounds_cold": t_cold * 1e3 / n,
+            "iterations": [s_.it - 1 for s_ in sw], "iterations_cold": [s_.it - 1 for s_ in sc],
+            "discarded": int(sum(bool(getattr(s_, "warm_discarded", False)) for s_ in sw)),
+            "speedup_vs_same_rounds_cold": t_cold / t_w,
+            "rel_l2_vs_tight_solve": {"angle_deg": float(angles[i]), "cold": float(np.linalg.norm(Ec[i] - ref)) / nr,
+                                      "continuation": float(np.linalg.norm(Ew[i] - ref)) / nr},
+            "timing": "host wall clock, fields copied to the host included (both sides)"}
 
 
 def run_warm_batched(args, sim, torch, dev, plain_ms):
