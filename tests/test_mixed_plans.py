@@ -100,3 +100,27 @@ def test_plan_schedule_matches_fft(name, N, E, radices):
     x = rng.standard_normal(N) + 1j * rng.standard_normal(N)
     np.testing.assert_allclose(replay(x, E, radices, False), np.fft.fft(x), rtol=0, atol=1e-9 * N)
     np.testing.assert_allclose(replay(x, E, radices, True), np.fft.ifft(x) * N, rtol=0, atol=1e-9 * N)
+
+
+def test_column_padding_is_the_models_choice():
+    """ColPad<N> (ws_mixed.cuh) gives the column passes' exchanges at most 6%
+    more shared-memory wavefronts than the best (shift, stride) of the host
+    model in wavesim_b200/csrc/colpad_model.py, for every plan it covers."""
+    import sys
+    csrc = os.path.join(ROOT, "wavesim_b200", "csrc")
+    sys.path.insert(0, csrc)
+    try:
+        import colpad_model as cm
+    finally:
+        sys.path.pop(0)
+    with open(os.path.join(csrc, "ws_mixed.cuh")) as f:
+        src = f.read()
+    table = {int(m.group(1)): (int(m.group(2)), int(m.group(3))) for m in re.finditer(
+        r"struct ColPad<(\d+)> \{ static constexpr int SH = (\d+), CS = (\d+); \};", src)}
+    assert table, "ColPad specialisations found"
+    for N, E, radices in cm.PLANS:
+        SH, CS = table.get(N, (4, N + N // 16 + 1))
+        assert CS >= (N - 1) + ((N - 1) >> SH) + 1
+        got = cm.wavefronts(N, E, radices, CS, SH)
+        best = cm.best(N, E, radices)[0][0]
+        assert got <= 1.06 * best, (N, got, best)
