@@ -32,8 +32,8 @@ constexpr int kThreads = 256;
 
 // Column lines of the column passes (kmc_col_step, the 2-D kernels): element
 // i of a line at i + (i >> SH), lines CS elements apart.  The shift and
-// stride minimise the shared-memory wavefronts of the lines' exchanges (a
-// host model of every stage's accesses, half-warp by half-warp, 8-byte
+// stride minimise the shared-memory wavefronts of the lines' exchanges
+// (colpad_model.py: every stage's accesses, half-warp by half-warp, 8-byte
 // banks): 224 points 2496 against 3968 with the planes' (i >> 4, N + N/16 + 1),
 // 160: 1824 against 3520, 96: 1024 against 1792, 192: 1152 against 1344,
 // 576: 3456 against 4032; the others keep the planes' layout.
