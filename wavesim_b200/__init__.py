@@ -11,5 +11,5 @@ from .problem import Medium, PlaneWave, SimulationGrid, Source, efficient_size, 
 from .simulation import WaveSim, WaveSimVector, nuttallwin, wiggle_perm  # noqa: F401
 from .pstd import PSTD  # noqa: F401
 
-__all__ = ["WaveSim", "WaveSimVector", "Source", "Medium", "SimulationGrid", "WaveSimError",
+__all__ = ["WaveSim", "WaveSimVector", "Source", "PlaneWave", "PSTD", "Medium", "SimulationGrid", "WaveSimError",
            "efficient_size", "symrange", "nuttallwin", "wiggle_perm"]
